@@ -1,0 +1,360 @@
+"""CPU oracle for the FFTLIB batched FFT hot path.
+
+TEST INFRASTRUCTURE ONLY. Imported by ``tests/``, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py`` as the checker, never by the product
+package ``c7x_fftlib_b200``.
+
+Three layers, all on the CPU:
+
+* ``liboracle.so`` -- this repository's C restatement of the reference
+  natural-C (``_cn``) kernels (``oracle/fftlib_oracle.c``), with the same
+  buffer layouts and twiddle tables as the reference.
+* ``_ref/libref_*.so`` -- the reference's own ``_cn`` sources, compiled by
+  ``oracle/Makefile`` from the reference tree (present only where that tree
+  was available at build time; the shared objects travel with the checkout).
+* FP64 references through numpy's ``pocketfft`` (``np.fft``), against which
+  every result reports relative L2 error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_i16p = np.ctypeslib.ndpointer(np.int16, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u32 = C.c_uint32
+
+
+def build(ref_root: str | None = None, with_ref: bool = True) -> None:
+    """Compile liboracle.so and, if the reference tree exists, oracle/_ref."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    ref_root = ref_root or "/root/reference"
+    if with_ref and os.path.isdir(os.path.join(ref_root, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_root}", "all"], check=True)
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build(with_ref=False)
+        L = C.CDLL(path)
+        L.orc_tw_gen_f32.argtypes = [_f32p, _u32]
+        L.orc_tw_gen_i16.argtypes = [_i16p, _u32]
+        L.orc_split_factor_r2c.argtypes = [_f32p, _u32]
+        L.orc_split_factor_c2r.argtypes = [_f32p, _u32]
+        L.orc_fft_c2c_f32.argtypes = [_f32p, _f32p, _f32p, _u32, _u32, C.c_int]
+        L.orc_fft_r2c_f32.argtypes = [_f32p, _f32p, _f32p, _f32p, _f32p, _u32, _u32, C.c_int]
+        L.orc_fft_c2r_f32.argtypes = [_f32p, _f32p, _f32p, _f32p, _f32p, _u32, _u32, C.c_int]
+        L.orc_fft_c2c_i16.argtypes = [_i16p, _i16p, _i16p, _u32p, _u32, _u32, _u32]
+        for fn in ("orc_fft_c2c_f32", "orc_fft_r2c_f32", "orc_fft_c2r_f32", "orc_fft_c2c_i16"):
+            getattr(L, fn).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+# --------------------------------------------------------------------------
+# Tables
+# --------------------------------------------------------------------------
+
+def tw_gen_f32(n: int) -> np.ndarray:
+    """FP32 twiddle table (2n floats) in the reference tw_gen layout."""
+    w = np.zeros(max(2 * n, 2), np.float32)
+    lib().orc_tw_gen_f32(w, n)
+    return w[: 2 * n] if n else w[:0]
+
+
+def tw_gen_i16(n: int) -> np.ndarray:
+    """Q15 radix-4 twiddle table (2n int16) in the reference layout."""
+    w = np.zeros(max(2 * n, 2), np.int16)
+    lib().orc_tw_gen_i16(w, n)
+    return w[: 2 * n]
+
+
+def split_factor_r2c(n: int) -> np.ndarray:
+    sf = np.zeros(2 * n, np.float32)
+    lib().orc_split_factor_r2c(sf, n)
+    return sf
+
+
+def split_factor_c2r(n: int) -> np.ndarray:
+    sf = np.zeros(2 * n, np.float32)
+    lib().orc_split_factor_c2r(sf, n)
+    return sf
+
+
+# --------------------------------------------------------------------------
+# Restated kernels (inputs are copied; the C code clobbers its input like
+# the reference does)
+# --------------------------------------------------------------------------
+
+def fft_c2c_f32(x: np.ndarray, n: int, channels: int, inverse: bool = False) -> np.ndarray:
+    xin = np.ascontiguousarray(x, np.float32).copy()
+    y = np.zeros(max(2 * n * channels, 1), np.float32)
+    w = tw_gen_f32(n) if n else np.zeros(2, np.float32)
+    rc = lib().orc_fft_c2c_f32(xin, np.ascontiguousarray(w), y, n, channels, int(inverse))
+    if rc:
+        raise ValueError(f"oracle c2c rejected N={n} (rc={rc})")
+    return y[: 2 * n * channels]
+
+
+def fft_r2c_f32(x: np.ndarray, n: int, channels: int, outmode: int = 0) -> np.ndarray:
+    xin = np.ascontiguousarray(x, np.float32).copy()
+    nout = n if outmode else n // 2 + 1
+    y = np.zeros(2 * nout * channels, np.float32)
+    xfft = np.zeros(n * channels, np.float32)
+    rc = lib().orc_fft_r2c_f32(xin, tw_gen_f32(n // 2), xfft, split_factor_r2c(n), y, n, channels, int(outmode))
+    if rc:
+        raise ValueError(f"oracle r2c rejected N={n}")
+    return y
+
+
+def fft_c2r_f32(x: np.ndarray, n: int, channels: int, inmode: int = 0) -> np.ndarray:
+    xin = np.ascontiguousarray(x, np.float32).copy()
+    y = np.zeros(n * channels, np.float32)
+    xfft = np.zeros(n * channels, np.float32)
+    rc = lib().orc_fft_c2r_f32(xin, tw_gen_f32(n // 2), xfft, split_factor_c2r(n), y, n, channels, int(inmode))
+    if rc:
+        raise ValueError(f"oracle c2r rejected N={n}")
+    return y
+
+
+def fft_c2c_i16(x: np.ndarray, n: int, channels: int, shifts) -> np.ndarray:
+    xin = np.ascontiguousarray(x, np.int16).copy()
+    y = np.zeros(2 * n * channels, np.int16)
+    sh = np.ascontiguousarray(shifts, np.uint32)
+    rc = lib().orc_fft_c2c_i16(xin, tw_gen_i16(n), y, sh, len(sh), n, channels)
+    if rc:
+        raise ValueError(f"oracle int16 rejected N={n} shifts={list(shifts)} (rc={rc})")
+    return y
+
+
+# --------------------------------------------------------------------------
+# FP64 references and error metric
+# --------------------------------------------------------------------------
+
+def as_complex(a: np.ndarray, n: int, channels: int) -> np.ndarray:
+    a = np.asarray(a, np.float64).reshape(channels, n, 2)
+    return a[..., 0] + 1j * a[..., 1]
+
+
+def fp64_c2c(x: np.ndarray, n: int, channels: int, inverse: bool = False) -> np.ndarray:
+    z = as_complex(x, n, channels)
+    return np.fft.ifft(z, axis=1) if inverse else np.fft.fft(z, axis=1)
+
+
+def fp64_r2c(x: np.ndarray, n: int, channels: int, outmode: int = 0) -> np.ndarray:
+    z = np.fft.fft(np.asarray(x, np.float64).reshape(channels, n), axis=1)
+    return z if outmode else z[:, : n // 2 + 1]
+
+
+def fp64_c2r(x: np.ndarray, n: int, channels: int, inmode: int = 0) -> np.ndarray:
+    """The reference c2r algorithm in exact arithmetic (FP64, exact pi):
+    Z[i] = X[i] A'[i] + b[i] B'[i] with A' = (1 - sin t)/2 + i cos t/2,
+    B' = (1 + sin t)/2 - i cos t/2, t = 2 pi i / N, b[i] = conj(X[N/2-i])
+    (inMode 0) or X[i+N/2] (inMode 1); then the N/2-point inverse DFT read as
+    N interleaved reals. For a Hermitian spectrum this is numpy's irfft."""
+    h = n // 2
+    nin = h + 1 if inmode == 0 else n
+    z = as_complex(x, nin, channels)
+    i = np.arange(h)
+    t = 2 * np.pi * i / n
+    a = 0.5 * (1 - np.sin(t)) + 0.5j * np.cos(t)
+    bb = 0.5 * (1 + np.sin(t)) - 0.5j * np.cos(t)
+    b = np.conj(z[:, h - i]) if inmode == 0 else z[:, i + h]
+    zz = z[:, :h] * a + b * bb
+    y = np.fft.ifft(zz, axis=1)
+    out = np.empty((channels, n))
+    out[:, 0::2] = y.real
+    out[:, 1::2] = y.imag
+    return out
+
+
+def rel_l2(got, ref) -> float:
+    got = np.asarray(got)
+    ref = np.asarray(ref)
+    if np.iscomplexobj(ref) and not np.iscomplexobj(got):
+        got = got.astype(np.float64).reshape(ref.shape + (2,))
+        got = got[..., 0] + 1j * got[..., 1]
+    den = np.linalg.norm(ref.ravel())
+    num = np.linalg.norm((np.asarray(got, np.complex128) - ref).ravel())
+    return float(num / den) if den > 0 else float(num)
+
+
+# --------------------------------------------------------------------------
+# The reference's own _cn code (oracle/_ref)
+# --------------------------------------------------------------------------
+
+class BufParams(C.Structure):
+    """FFTLIB_bufParams1D_t (src/common/FFTLIB_bufParams.h:62-67)."""
+    _fields_ = [("data_type", C.c_uint32), ("dim_x", C.c_uint32)]
+
+
+FFTLIB_INT16, FFTLIB_UINT32, FFTLIB_FLOAT32 = 1, 8, 12
+
+
+def ref_available() -> bool:
+    return all(os.path.exists(os.path.join(REF_DIR, f"libref_{k}.so"))
+               for k in ("c2c", "ifft", "r2c", "c2r", "i16", "twgen"))
+
+
+_ref = {}
+
+
+def ref_lib(kind: str) -> C.CDLL:
+    if kind not in _ref:
+        path = os.path.join(REF_DIR, f"libref_{kind}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (make -C oracle all)")
+        _ref[kind] = C.CDLL(path)
+    return _ref[kind]
+
+
+def _bp(dtype, dim):
+    return C.byref(BufParams(dtype, dim))
+
+
+def ref_tw_gen_c2c(n: int) -> np.ndarray:
+    w = np.zeros(max(2 * n, 2), np.float32)
+    ref_lib("twgen").ref_tw_gen_c2c(w.ctypes.data_as(C.c_void_p), _u32(n))
+    return w[: 2 * n]
+
+
+def ref_tw_gen_i16(n: int) -> np.ndarray:
+    w = np.zeros(max(2 * n, 2), np.int16)
+    ref_lib("twgen").ref_tw_gen_i16(w.ctypes.data_as(C.c_void_p), _u32(n))
+    return w[: 2 * n]
+
+
+def ref_tw_gen_r2c(n: int) -> np.ndarray:
+    w = np.zeros(max(n, 2), np.float32)
+    ref_lib("r2c").tw_gen_r2c(w.ctypes.data_as(C.c_void_p), C.c_int32(n))
+    return w[:n]
+
+
+def ref_tw_gen_c2r(n: int) -> np.ndarray:
+    w = np.zeros(max(n, 2), np.float32)
+    ref_lib("c2r").ifft_c2r_tw_gen(w.ctypes.data_as(C.c_void_p), C.c_int32(n))
+    return w[:n]
+
+
+def ref_split_factor_r2c(n: int) -> np.ndarray:
+    sf = np.zeros(2 * n, np.float32)
+    ref_lib("r2c").split_factor_gen_r2c(sf.ctypes.data_as(C.c_void_p), C.c_int32(n))
+    return sf
+
+
+def ref_split_factor_c2r(n: int) -> np.ndarray:
+    sf = np.zeros(2 * n, np.float32)
+    ref_lib("c2r").ifft_c2r_split_factor_gen(sf.ctypes.data_as(C.c_void_p), C.c_int32(n))
+    return sf
+
+
+def _vp(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def ref_c2c_f32(x, n, channels, inverse=False, w=None):
+    """Reference FFTLIB_{fft,ifft}1dBatched_i32fc_c32fc_o32fc_cn."""
+    xin = np.ascontiguousarray(x, np.float32).copy()
+    y = np.zeros(max(2 * n * channels, 2), np.float32)
+    w = ref_tw_gen_c2c(n) if w is None else np.ascontiguousarray(w, np.float32)
+    L = ref_lib("ifft" if inverse else "c2c")
+    fn = L.FFTLIB_ifft1dBatched_i32fc_c32fc_o32fc_cn if inverse else L.FFTLIB_fft1dBatched_i32fc_c32fc_o32fc_cn
+    dim = 2 * n * channels
+    rc = fn(_vp(xin), _bp(FFTLIB_FLOAT32, dim), _vp(w), _bp(FFTLIB_FLOAT32, 2 * n), _vp(y),
+            _bp(FFTLIB_FLOAT32, dim), _u32(n), _u32(channels))
+    if rc:
+        raise ValueError(f"reference c2c returned {rc}")
+    return y[: 2 * n * channels]
+
+
+def ref_r2c_f32(x, n, channels, outmode=0):
+    xin = np.ascontiguousarray(x, np.float32).copy()
+    nout = n if outmode else n // 2 + 1
+    y = np.zeros(2 * nout * channels, np.float32)
+    xfft = np.zeros(n * channels + 2, np.float32)
+    w = ref_tw_gen_r2c(n)
+    sf = ref_split_factor_r2c(n)
+    L = ref_lib("r2c")
+    dim = n * channels
+    rc = L.FFTLIB_fft1dBatched_i32f_c32fc_o32fc_cn(
+        _vp(xin), _bp(FFTLIB_FLOAT32, dim), _vp(w), _bp(FFTLIB_FLOAT32, dim), _vp(xfft),
+        _bp(FFTLIB_FLOAT32, dim), _vp(sf), _bp(FFTLIB_FLOAT32, 2 * n), _vp(y), _bp(FFTLIB_FLOAT32, dim),
+        _u32(n), _u32(channels), C.c_uint8(outmode))
+    if rc:
+        raise ValueError(f"reference r2c returned {rc}")
+    return y
+
+
+def ref_c2r_f32(x, n, channels, inmode=0):
+    xin = np.ascontiguousarray(x, np.float32).copy()
+    y = np.zeros(n * channels, np.float32)
+    xfft = np.zeros((n + 1) * 2 * channels, np.float32)
+    w = ref_tw_gen_c2r(n)
+    sf = ref_split_factor_c2r(n)
+    L = ref_lib("c2r")
+    dim = n * channels
+    rc = L.FFTLIB_ifft1dBatched_i32fc_c32fc_o32f_cn(
+        _vp(xin), _bp(FFTLIB_FLOAT32, dim), _vp(w), _bp(FFTLIB_FLOAT32, dim), _vp(xfft),
+        _bp(FFTLIB_FLOAT32, dim), _vp(sf), _bp(FFTLIB_FLOAT32, 2 * n), _vp(y), _bp(FFTLIB_FLOAT32, dim),
+        _u32(n), _u32(channels), C.c_uint8(inmode))
+    if rc:
+        raise ValueError(f"reference c2r returned {rc}")
+    return y
+
+
+def ref_c2c_i16(x, n, channels, shifts, w=None):
+    xin = np.ascontiguousarray(x, np.int16).copy()
+    y = np.zeros(2 * n * channels, np.int16)
+    w = ref_tw_gen_i16(n) if w is None else np.ascontiguousarray(w, np.int16)
+    sh = np.ascontiguousarray(shifts, np.uint32)
+    L = ref_lib("i16")
+    dim = 2 * n * channels
+    rc = L.FFTLIB_fft1dBatched_i16sc_c16sc_o16sc_cn(
+        _vp(xin), _bp(FFTLIB_INT16, dim), _vp(w), _bp(FFTLIB_INT16, 2 * n), _vp(y), _bp(FFTLIB_INT16, dim),
+        _vp(sh), _bp(FFTLIB_UINT32, len(sh)), _u32(n), _u32(channels))
+    if rc:
+        raise ValueError(f"reference int16 returned {rc}")
+    return y
+
+
+# --------------------------------------------------------------------------
+# Seeded synthetic inputs (splitmix64-free: numpy PCG64 with a fixed seed)
+# --------------------------------------------------------------------------
+
+def rng(seed: int) -> np.random.Generator:
+    return np.random.default_rng(seed)
+
+
+def uniform_c2c(n: int, channels: int, seed: int, lo=-1.0, hi=1.0) -> np.ndarray:
+    return rng(seed).uniform(lo, hi, 2 * n * channels).astype(np.float32)
+
+
+def real_signal(n: int, channels: int, seed: int) -> np.ndarray:
+    """N(0,1) noise plus 3 sinusoids per channel (amplitude U[1,10], integer
+    bins U{1..N/2-1}, phase U[0,2pi)), the real-input workload."""
+    g = rng(seed)
+    t = np.arange(n, dtype=np.float64)
+    x = g.standard_normal((channels, n))
+    for _ in range(3):
+        amp = g.uniform(1.0, 10.0, (channels, 1))
+        k = g.integers(1, max(n // 2, 2), (channels, 1))
+        ph = g.uniform(0.0, 2 * np.pi, (channels, 1))
+        x += amp * np.cos(2 * np.pi * k * t / n + ph)
+    return x.astype(np.float32).ravel()
+
+
+def int16_input(n: int, channels: int, seed: int, lo=-2048, hi=2047) -> np.ndarray:
+    return rng(seed).integers(lo, hi + 1, 2 * n * channels).astype(np.int16)

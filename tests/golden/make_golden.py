@@ -1,0 +1,210 @@
+"""Generate the committed golden fixtures in tests/golden/.
+
+Run in a checkout that has the reference FFTLIB tree (default
+/root/reference) and oracle/_ref built (``make -C oracle all``):
+
+    python tests/golden/make_golden.py [--ref /path/to/c7x_fftlib]
+
+Outputs (small .npz files; nothing here is read at run time except the
+fixtures themselves):
+
+* ``r2c_extended.npz`` / ``c2r_extended.npz`` -- the reference's committed
+  static test vectors for the batched real-input kernels
+  (test/fft_c7x/FFTLIB_fft1dBatched_i32f_c32fc_o32fc/test_data/extended_test_cases,
+  test/fft_c7x/FFTLIB_ifft1dBatched_i32fc_c32fc_o32f/test_data/extended_test_cases),
+  with their (numChannels, numPoints, mode) from the generator's
+  test_cases_list.csv; a size-bounded subset of the c2r cases.
+* ``i16_pymodel.npz`` -- outputs of the reference's bit-exact Python model of
+  the int16 kernel (test/fft_c7x/FFTLIB_idat_gen/FFTLIB_fft1dBatched_i16sc_c16sc_o16sc/
+  fft1dBatched_i16sc_c16sc_o16sc.py) on seeded inputs, with its twiddle table.
+* ``c2c_pymodel.npz`` -- outputs of the reference's Python golden generators
+  for c2c and ifft c2c (np.fft based, rounded to 6 decimals as the reference
+  does) on seeded inputs.
+* ``ref_cn.npz`` -- outputs of the reference's own ``_cn`` C code
+  (oracle/_ref) on seeded inputs, for every batched kernel.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import importlib.util
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle as O  # noqa: E402
+
+ARRAY_RE = re.compile(r"static\s+(?:float|int16_t)\s+(\w+)\[\]\s*=\s*\{([^}]*)\}", re.S)
+
+
+def parse_c_arrays(path):
+    with open(path) as f:
+        text = f.read()
+    out = {}
+    for name, body in ARRAY_RE.findall(text):
+        vals = [v for v in (t.strip() for t in body.replace("\n", " ").split(",")) if v]
+        out[name] = np.array([float(v.rstrip("f")) for v in vals], np.float64)
+    return out
+
+
+def read_cases(csv_path):
+    with open(csv_path) as f:
+        return {int(r["ID"]): r for r in csv.DictReader(f)}
+
+
+def _sizes(kind, nch, n, mode):
+    """(input floats, output floats) of one case of the real-input kernels."""
+    bins = n if mode else n // 2 + 1
+    return (nch * n, 2 * nch * bins) if kind == "r2c" else (2 * nch * bins, nch * n)
+
+
+def extended(ref, kernel, mode_key, byte_budget):
+    """The committed extended test vectors. Their file numbers do not follow
+    the generator's current test_cases_list.csv row for row, so each file's
+    (numChannels, numPoints, mode) is taken from the CSV rows whose buffer
+    sizes match the arrays, choosing among them the one the oracle reproduces
+    most closely; files no row explains are skipped."""
+    kind = "r2c" if "i32f_c32fc" in kernel else "c2r"
+    run = O.fft_r2c_f32 if kind == "r2c" else O.fft_c2r_f32
+    base = os.path.join(ref, "test", "fft_c7x", kernel, "test_data", "extended_test_cases")
+    cases = read_cases(os.path.join(ref, "test", "fft_c7x", "FFTLIB_idat_gen", kernel, "test_cases_list.csv"))
+    params = sorted({(int(r["numChannels"]), int(r["numPoints"]), int(r[mode_key])) for r in cases.values()})
+    files = os.listdir(base)
+    rows, used = [], 0
+    for fn in sorted(files, key=lambda s: os.path.getsize(os.path.join(base, s))):
+        cid = int(re.findall(r"\d+", fn)[0])
+        arr = parse_c_arrays(os.path.join(base, fn))
+        xin, yout = arr[f"staticRefIn{cid}"], arr[f"staticRefOut{cid}"]
+        size = (xin.size + yout.size) * 4
+        if used + size > byte_budget:
+            continue
+        best = None
+        for nch, n, mode in params:
+            if _sizes(kind, nch, n, mode) != (xin.size, yout.size):
+                continue
+            err = float(np.abs(run(xin.astype(np.float32), n, nch, mode) - yout).max())
+            if best is None or err < best[0]:
+                best = (err, nch, n, mode)
+        # reference tolerances: r2c 2^-3 (..._i32f_c32fc_o32fc_d.c:208-234),
+        # c2r 1e-3 (..._ifft1dBatched_i32fc_c32fc_o32f_d.c:196-201)
+        tol = 2.0 ** -3 if kind == "r2c" else 1e-3
+        if best is None or best[0] > tol:
+            print(f"skip {kind} extended case {cid}: no test_cases_list.csv row reproduces it")
+            continue
+        used += size
+        rows.append((cid, best[1], best[2], best[3], xin.astype(np.float32), yout.astype(np.float32)))
+    rows.sort()
+    d = {"ids": np.array([r[0] for r in rows]), "channels": np.array([r[1] for r in rows]),
+         "points": np.array([r[2] for r in rows]), "mode": np.array([r[3] for r in rows])}
+    for cid, _, _, _, xin, yout in rows:
+        d[f"in_{cid}"] = xin
+        d[f"out_{cid}"] = yout
+    return d
+
+
+def load_module(path, name):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def i16_pymodel(ref):
+    gen = os.path.join(ref, "test", "fft_c7x", "FFTLIB_idat_gen", "FFTLIB_fft1dBatched_i16sc_c16sc_o16sc")
+    mod = load_module(os.path.join(gen, "fft1dBatched_i16sc_c16sc_o16sc.py"), "ref_i16_model")
+    cls = mod.FFTLIB_fft1dBatched_i16sc_c16sc_o16sc
+    # (numChannels, numPoints, shiftVector) as in the reference test_cases_list.csv
+    cases = [(2, 16, [1, 1]), (2, 64, [0, 1, 1]), (3, 128, [0, 1, 1]), (2, 256, [0, 1, 1, 1]),
+             (2, 512, [1, 0, 1, 1]), (2, 1024, [2, 2, 2, 2, 2]), (1, 2048, [0, 1, 1, 1, 1]),
+             (2, 32, [0, 0]), (1, 8, [1]), (1, 4, [2])]
+    d = {"n_cases": np.array(len(cases))}
+    for i, (nch, n, sh) in enumerate(cases):
+        x = O.int16_input(n, nch, 1000 + i)
+        g = x.astype(np.float64).reshape(nch, n, 2)
+        model = cls(nch, n, list(sh))
+        out, _ = model.exec(g[..., 0] + 1j * g[..., 1])
+        y = np.stack([out.real, out.imag], -1).astype(np.int16).ravel()
+        d[f"case{i}_meta"] = np.array([nch, n])
+        d[f"case{i}_shift"] = np.array(sh, np.uint32)
+        d[f"case{i}_in"] = x
+        d[f"case{i}_out"] = y
+        d[f"case{i}_tw"] = np.array(model.pW, np.int16)
+    return d
+
+
+def c2c_pymodel(ref):
+    gen = os.path.join(ref, "test", "fft_c7x", "FFTLIB_idat_gen")
+    fwd = load_module(os.path.join(gen, "FFTLIB_fft1dBatched_i32fc_c32fc_o32fc", "fft1dBatched_i32fc_c32fc_o32fc.py"),
+                      "ref_c2c_model").FFTLIB_fft1dBatched_i32fc_c32fc_o32fc
+    inv = load_module(os.path.join(gen, "FFTLIB_ifft1dBatched_i32fc_c32fc_o32fc", "ifft1dBatched_i32fc_c32fc_o32fc.py"),
+                      "ref_ifft_model").FFTLIB_ifft1dBatched_i32fc_c32fc_o32fc
+    cases = [(4, 256), (2, 60), (1, 3000), (2, 125), (3, 96), (1, 4096), (8, 16), (2, 1536)]
+    d = {"n_cases": np.array(len(cases))}
+    for i, (nch, n) in enumerate(cases):
+        x = O.uniform_c2c(n, nch, 2000 + i)
+        z = O.as_complex(x, n, nch)
+        yf = fwd(nch, n).exec(z)
+        yi = inv(nch, n).exec(z)
+        d[f"case{i}_meta"] = np.array([nch, n])
+        d[f"case{i}_in"] = x
+        d[f"case{i}_fwd"] = np.stack([yf.real, yf.imag], -1).ravel()
+        d[f"case{i}_inv"] = np.stack([yi.real, yi.imag], -1).ravel()
+    return d
+
+
+def ref_cn():
+    d = {}
+    c2c = [(16, 256), (2, 4096), (3, 60), (2, 3000), (4, 125), (1, 6561), (5, 12), (2, 2), (1, 1), (3, 30)]
+    for i, (nch, n) in enumerate(c2c):
+        x = O.uniform_c2c(n, nch, 3000 + i, -256.0, 256.0)
+        d[f"c2c{i}_meta"] = np.array([nch, n])
+        d[f"c2c{i}_in"] = x
+        d[f"c2c{i}_fwd"] = O.ref_c2c_f32(x, n, nch, False)
+        d[f"c2c{i}_inv"] = O.ref_c2c_f32(x, n, nch, True)
+    d["c2c_n"] = np.array(len(c2c))
+    rc = [(2, 4096, 0), (2, 4096, 1), (3, 480, 0), (1, 250, 1), (4, 64, 0), (2, 6, 0)]
+    for i, (nch, n, mode) in enumerate(rc):
+        x = O.real_signal(n, nch, 4000 + i)
+        yr = O.ref_r2c_f32(x, n, nch, mode)
+        d[f"rc{i}_meta"] = np.array([nch, n, mode])
+        d[f"rc{i}_in"] = x
+        d[f"rc{i}_r2c"] = yr
+        d[f"rc{i}_c2r"] = O.ref_c2r_f32(yr, n, nch, mode)
+    d["rc_n"] = np.array(len(rc))
+    i16 = [(4, 1024, [2, 2, 2, 2, 2]), (3, 2048, [1, 1, 1, 1, 2]), (8, 64, [0, 1, 1]), (2, 256, [3, 3, 3, 3])]
+    for i, (nch, n, sh) in enumerate(i16):
+        x = O.int16_input(n, nch, 5000 + i, -32768, 32767) if i == 3 else O.int16_input(n, nch, 5000 + i)
+        d[f"i16{i}_meta"] = np.array([nch, n])
+        d[f"i16{i}_shift"] = np.array(sh, np.uint32)
+        d[f"i16{i}_in"] = x
+        d[f"i16{i}_out"] = O.ref_c2c_i16(x, n, nch, sh)
+    d["i16_n"] = np.array(len(i16))
+    return d
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    a = ap.parse_args()
+    if not O.ref_available():
+        O.build(a.ref)
+    np.savez_compressed(os.path.join(HERE, "r2c_extended.npz"),
+                        **extended(a.ref, "FFTLIB_fft1dBatched_i32f_c32fc_o32fc", "outmode", 1 << 20))
+    np.savez_compressed(os.path.join(HERE, "c2r_extended.npz"),
+                        **extended(a.ref, "FFTLIB_ifft1dBatched_i32fc_c32fc_o32f", "inMode", 1 << 20))
+    np.savez_compressed(os.path.join(HERE, "i16_pymodel.npz"), **i16_pymodel(a.ref))
+    np.savez_compressed(os.path.join(HERE, "c2c_pymodel.npz"), **c2c_pymodel(a.ref))
+    np.savez_compressed(os.path.join(HERE, "ref_cn.npz"), **ref_cn())
+    for fn in sorted(os.listdir(HERE)):
+        if fn.endswith(".npz"):
+            print(fn, os.path.getsize(os.path.join(HERE, fn)))
+
+
+if __name__ == "__main__":
+    main()
