@@ -1,0 +1,309 @@
+"""Benchmark of the B200 FFTLIB batched FFT hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the north-star headline): FFTLIB_fft1dBatched_i32fc_c32fc_o32fc,
+FP32 complex-to-complex forward FFT, N = 4096 points, 8192 channels per GPU,
+interleaved re/im, inputs iid U[-1, 1) from a fixed seed. A step is one
+batched transform of the whole batch. Metric: HBM throughput in GB/s of
+algorithmic bytes (16 bytes per point: read 8 + write 8), whole job.
+
+* value: device-resident buffers, one `_kernelAsync` launch per step, timed
+  with CUDA events on the launching stream (inputs 256 MiB > 126 MB L2).
+* e2e: the same transform through the synchronous FFTLIB `_kernel` call with
+  pinned host buffers, host->device and device->host copies inside the
+  timed region (wall clock).
+* roofline: achieved GB/s of the FFT kernel against the measured HBM copy
+  bandwidth in MEASURED_PEAKS.json; traffic per launch from the committed
+  ncu capture summary (profiles/).
+* cpu_baseline: the reference's own _cn code (oracle/_ref, built from the
+  reference sources with gcc -O3) on the host cores, on a bounded sample of
+  the same workload.
+* --impl reference: that reference CPU implementation alone, as the
+  reference arm.
+
+Multi-GPU (torchrun): every rank transforms its own 8192-channel batch
+(weak scaling, no collective on the data path); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_POINTS = 4096
+CHANNELS = 8192
+METRIC = "batched FFT HBM GB/s (% peak); TC-DFT vs FP32-FFT speedup at ≤2e-6 rel err"
+WORKLOAD = "fft1dBatched_i32fc_c32fc_o32fc c2c FP32 forward, N=4096 x 8192 channels"
+
+
+def algo_bytes(n, ch):
+    return 16.0 * n * ch
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profile(kernel_tag):
+    """Per-launch DRAM bytes of the kernel from the committed ncu summary
+    (lines 'traffic <tag> <bytes>'), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        for line in open(p):
+            f = line.split()
+            if len(f) >= 3 and f[0] == "traffic" and f[1] == kernel_tag:
+                return float(f[2])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_arm(args, world, rank):
+    """The reference's own CPU implementation (_cn compiled from its sources)
+    on all host threads: each step a bounded sample of the workload."""
+    if rank != 0:
+        return
+    import oracle as O
+
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference _cn build) is not present"}))
+        return
+    sample = 256  # channels per step: ~64 MiB of the 8192-channel workload
+    threads = O.host_threads()
+    for _ in range(args.warmup):
+        O.time_reference_c2c(N_POINTS, sample, threads, reps=1)
+    times = [O.time_reference_c2c(N_POINTS, sample, threads, reps=1, seed=s)[0] for s in range(args.steps)]
+    t = sum(times)
+    gbs = algo_bytes(N_POINTS, sample) * args.steps / t / 1e9
+    ms_full = (algo_bytes(N_POINTS, CHANNELS) / (gbs * 1e9)) * 1e3
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_full, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_channels_per_step": sample, "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "reference",
+                         "sample": f"{sample} channels of N={N_POINTS} per step, reference "
+                                   f"FFTLIB_fft1dBatched_i32fc_c32fc_o32fc_cn built with gcc -O3"},
+        "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def our_arm(args, world, rank, local):
+    import torch
+
+    import c7x_fftlib_b200 as F
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    n, ch = N_POINTS, CHANNELS
+    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    X = torch.rand(2 * n * ch, device="cuda", generator=g) * 2 - 1
+    Y = torch.empty_like(X)
+    W = torch.zeros(2 * n, device="cuda")
+    b, bw = F.bp(F.FFTLIB_FLOAT32, 2 * n * ch), F.bp(F.FFTLIB_FLOAT32, 2 * n)
+    base = F.KERNELS["c2c"]
+    pb = F.pblock("c2c")
+    F.check(F.fn(base + "_init")(F.ptr(X), b, F.ptr(W), bw, F.ptr(Y), b, n, ch, pb), "init")
+    stream = torch.cuda.Stream()
+    launch = F.fn("FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync")
+    sp = F.ptr(stream.cuda_stream)
+
+    def step():
+        st = launch(F.ptr(X), F.ptr(Y), n, ch, pb, sp)
+        if st:
+            F.check(st, "kernelAsync")
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    per_gpu_gbs = algo_bytes(n, ch) / (ms_step * 1e-3) / 1e9
+    value = per_gpu_gbs * world
+
+    # parity spot check of the timed output (a few channels against FP64)
+    import numpy as np
+
+    import oracle as O
+
+    idx = [0, ch // 3, ch - 1]
+    xs = X.view(ch, 2 * n)[idx].cpu().numpy().ravel()
+    ys = Y.view(ch, 2 * n)[idx].cpu().numpy().ravel()
+    rel = O.rel_l2(ys, O.fp64_c2c(xs, n, len(idx)))
+
+    # end to end through the synchronous FFTLIB call with pinned host buffers
+    e2e_steps = max(2, min(args.steps, 5))
+    Xh = X.cpu().pin_memory()
+    Yh = torch.empty_like(Xh).pin_memory()
+    kern = F.fn(base + "_kernel")
+    F.check(kern(F.ptr(Xh), b, F.ptr(W), bw, F.ptr(Yh), b, n, ch, pb), "kernel (host)")
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        F.check(kern(F.ptr(Xh), b, F.ptr(W), bw, F.ptr(Yh), b, n, ch, pb), "kernel (host)")
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_gbs = algo_bytes(n, ch) * e2e_steps * world / e2e_s / 1e9
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peak, peak_kind = measured_peak()
+    traffic = traffic_from_profile("c2c_4096")
+    out = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "numPoints": n, "numChannels_per_gpu": ch, "parallelism": f"replicas{world}",
+                   "plan": F.describe_plan(n), "l2": "inputs (256 MiB) larger than L2, no flush",
+                   "transforms_per_s": round(ch * world / (ms_step * 1e-3), 1)},
+        "roofline": {"bound": "hbm", "achieved": round(per_gpu_gbs, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(per_gpu_gbs / peak, 4), "peak_source": peak_kind,
+                     "traffic": traffic},
+        "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s", "h2d_bytes_per_step": int(8 * n * ch),
+                "d2h_bytes_per_step": int(8 * n * ch), "path": "FFTLIB _kernel, pinned host buffers"},
+        "gpu_launches": args.steps,
+        "parity": {"rel_l2_vs_fp64_sampled": rel, "bound": 2e-6},
+        "clocks": clk.summary(),
+    }
+    if world == 1:
+        out["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(out))
+
+
+def cpu_baseline():
+    import oracle as O
+
+    if not O.ref_available():
+        return None
+    sample = 512
+    threads = O.host_threads()
+    t, used = O.time_reference_c2c(N_POINTS, sample, threads, reps=3)
+    return {"value": round(algo_bytes(N_POINTS, sample) / t / 1e9, 4), "unit": "GB/s", "cores": used,
+            "kind": "reference",
+            "sample": f"{sample} channels of N={N_POINTS}, median of 3, reference _cn (gcc -O3), one thread per core"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+    else:
+        our_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

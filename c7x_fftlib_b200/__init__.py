@@ -1,0 +1,168 @@
+"""c7x_fftlib_b200 -- B200-native FFTLIB batched FFT hot path.
+
+The product is ``libfftlib_b200.so`` (hand-written sm_100a CUDA behind the
+FFTLIB C API, headers in ``include/``). This package builds it in-tree
+(``c7x_fftlib_b200._build``) and binds it with ctypes under the reference
+names, so Python callers (tests, benchmarks) drive exactly the C entry points
+a C caller would link against. There is no fallback: if the shared library
+is missing, ``lib()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+__all__ = ["lib", "BufParams", "pblock", "ptr", "check", "FftlibError"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfftlib_b200.so")
+
+# FFTLIB_STATUS (src/common/FFTLIB_types.h:168-211)
+FFTLIB_SUCCESS = 0
+FFTLIB_ERR_FAILURE = 1
+FFTLIB_ERR_INVALID_VALUE = 2
+FFTLIB_ERR_INVALID_TYPE = 3
+FFTLIB_ERR_INVALID_DIMENSION = 4
+FFTLIB_ERR_NULL_POINTER = 5
+FFTLIB_ERR_NOT_IMPLEMENTED = 6
+FFTLIB_ERR_NOT_ALIGNED_PTRS_STRIDES = 8
+FFTLIB_ERR_INVALID_OUTMODE = 14
+
+# FFTLIB_data_type_e (src/common/FFTLIB_bufParams.h:22-42)
+FFTLIB_INT16 = 1
+FFTLIB_INT32 = 2
+FFTLIB_UINT32 = 8
+FFTLIB_FLOAT32 = 12
+
+# FFTLIB_FUNCTION_STYLE
+FFTLIB_FUNCTION_NATC = 0
+FFTLIB_FUNCTION_OPTIMIZED = 1
+
+SE_PARAM_SIZE = 64
+PBLOCK_SIZE = {
+    "c2c": 31 * SE_PARAM_SIZE + 18 * 4,
+    "ifft": 31 * SE_PARAM_SIZE + 18 * 4,
+    "r2c": 41 * SE_PARAM_SIZE + 18 * 4,
+    "c2r": 41 * SE_PARAM_SIZE + 18 * 4,
+    "i16": 13 * SE_PARAM_SIZE,
+}
+
+
+class FftlibError(RuntimeError):
+    pass
+
+
+class BufParams(C.Structure):
+    """FFTLIB_bufParams1D_t (src/common/FFTLIB_bufParams.h:62-67)."""
+    _fields_ = [("data_type", C.c_uint32), ("dim_x", C.c_uint32)]
+
+
+_vp = C.c_void_p
+_bpp = C.POINTER(BufParams)
+_u32 = C.c_uint32
+_u8 = C.c_uint8
+
+_SIGS = {
+    # name suffix: argtypes (after the common prefix)
+    "c2c": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32, _vp],
+    "c2c_cn": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32],
+    "real": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32, _u8, _vp],
+    "real_cn": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32, _u8],
+    "real_check": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32, _u8, _vp],
+    "real_check_cn": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32, _u8],
+    "i16": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32, _vp],
+    "i16_cn": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32],
+}
+
+KERNELS = {
+    "c2c": "FFTLIB_fft1dBatched_i32fc_c32fc_o32fc",
+    "ifft": "FFTLIB_ifft1dBatched_i32fc_c32fc_o32fc",
+    "r2c": "FFTLIB_fft1dBatched_i32f_c32fc_o32fc",
+    "c2r": "FFTLIB_ifft1dBatched_i32fc_c32fc_o32f",
+    "i16": "FFTLIB_fft1dBatched_i16sc_c16sc_o16sc",
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libfftlib_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FftlibError(f"{LIB_PATH} is missing; build it with `python -m c7x_fftlib_b200._build`")
+    L = C.CDLL(LIB_PATH)
+    for kind, base in KERNELS.items():
+        if kind in ("c2c", "ifft"):
+            fam = {"_init": "c2c", "_kernel": "c2c", "_checkParams": "c2c", "_cn": "c2c_cn", "_checkParams_cn": "c2c_cn"}
+        elif kind in ("r2c", "c2r"):
+            fam = {"_init": "real", "_kernel": "real", "_checkParams": "real_check", "_cn": "real_cn",
+                   "_checkParams_cn": "real_check_cn"}
+        else:
+            fam = {"_init": "i16", "_kernel": "i16", "_checkParams": "i16", "_cn": "i16_cn", "_checkParams_cn": "i16_cn"}
+        for suffix, sig in fam.items():
+            fn = getattr(L, base + suffix)
+            fn.argtypes = _SIGS[sig]
+            fn.restype = C.c_int
+    L.FFTLIB_b200_lastError.restype = C.c_char_p
+    L.FFTLIB_b200_lastError.argtypes = []
+    L.FFTLIB_b200_version.restype = C.c_int
+    L.FFTLIB_b200_describePlan.argtypes = [_u32, C.c_char_p, _u32]
+    L.FFTLIB_b200_describePlan.restype = C.c_int
+    L.FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync.argtypes = [_vp, _vp, _u32, _u32, _vp, _vp]
+    L.FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32fc_kernelAsync.argtypes = [_vp, _vp, _u32, _u32, _vp, _vp]
+    L.FFTLIB_b200_fft1dBatched_i32f_c32fc_o32fc_kernelAsync.argtypes = [_vp, _vp, _vp, _u32, _u32, _u8, _vp, _vp]
+    L.FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32f_kernelAsync.argtypes = [_vp, _vp, _vp, _u32, _u32, _u8, _vp, _vp]
+    L.FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync.argtypes = [_vp, _vp, _vp, _vp, _u32, _u32, _u32, _vp,
+                                                                         _vp]
+    L.FFTLIB_b200_tw_gen_c2c.argtypes = [_vp, _u32]
+    L.FFTLIB_b200_tw_gen_i16.argtypes = [_vp, _u32]
+    for fn in ("tw_gen_r2c", "split_factor_gen_r2c", "ifft_c2r_tw_gen", "ifft_c2r_split_factor_gen"):
+        getattr(L, fn).argtypes = [_vp, C.c_int32]
+        getattr(L, fn).restype = None
+    _lib = L
+    return L
+
+
+def ptr(x) -> C.c_void_p | None:
+    """Address of a buffer: None, an int address, a numpy array, a torch
+    tensor (device or host) or a ctypes object."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return C.c_void_p(x)
+    if hasattr(x, "data_ptr"):
+        return C.c_void_p(x.data_ptr())
+    if hasattr(x, "ctypes"):
+        return C.c_void_p(x.ctypes.data)
+    return C.cast(x, C.c_void_p)
+
+
+def pblock(kind: str):
+    """A zeroed pBlock of the reference size for kernel kind."""
+    return C.create_string_buffer(PBLOCK_SIZE[kind])
+
+
+def bp(data_type: int, dim_x: int) -> BufParams:
+    return BufParams(data_type, dim_x)
+
+
+def last_error() -> str:
+    return lib().FFTLIB_b200_lastError().decode()
+
+
+def check(status: int, what: str = "FFTLIB call") -> None:
+    if status != FFTLIB_SUCCESS:
+        raise FftlibError(f"{what} returned {status}: {last_error()}")
+
+
+def describe_plan(n: int) -> str:
+    buf = C.create_string_buffer(256)
+    check(lib().FFTLIB_b200_describePlan(n, buf, 256), "describePlan")
+    return buf.value.decode()
+
+
+def fn(name: str):
+    """The exported C function `name` (reference name or FFTLIB_b200_*)."""
+    return getattr(lib(), name)

@@ -1,0 +1,80 @@
+// fft_args.h -- launch descriptors shared by host planning code and the
+// FP32 FFT kernels (plain C++ structs, no CUDA types beyond float2).
+#pragma once
+
+#include <stdint.h>
+#include <vector_types.h>
+
+#if defined(__CUDACC__)
+#define FFTB_HD __host__ __device__
+#else
+#define FFTB_HD
+#endif
+
+namespace fftb200 {
+
+constexpr int kMaxPasses = 8;
+
+// Magic multiplier for floor(j / d) = umulhi(j, m), m = floor(2^32 / d) + 1,
+// exact whenever j * d < 2^32 (all indices here are below 2^16).
+inline FFTB_HD uint32_t fastdiv_magic(uint32_t d)
+{
+    return d <= 1u ? 0u : (uint32_t)((0x100000000ull / d) + 1ull);
+}
+
+// Shared-memory length (complex values) of one length-n region with one pad
+// slot per 16 values.
+inline FFTB_HD constexpr uint32_t smem_len(uint32_t n) { return n + (n >> 4) + 1u; }
+
+// One Stockham pass of radix R: butterfly j reads in[j + q*N/R] (q < R),
+// multiplies input q by W_{Ns*R}^{q*(j mod Ns)} and writes output q to
+// out[(j/Ns)*Ns*R + (j mod Ns) + q*Ns]. Ns is the product of the radices of
+// the passes before it, so the last pass writes out[j + q*N/R] (natural order).
+struct PassInfo {
+    int32_t  R;
+    uint32_t Ns;
+    uint32_t nsMagic;   // fastdiv_magic(Ns)
+    uint32_t stride;    // N / R
+    uint32_t twStride;  // N / (Ns * R): index step into the W_N table
+};
+
+enum IoMode : int32_t {
+    IO_C2C = 0,        // complex in, complex out
+    IO_R2C_SPLIT = 1,  // packed reals in, split post-process epilogue
+    IO_C2R_SPLIT = 2,  // split pre-process prologue, packed reals out
+};
+
+struct FftArgs {
+    const float2* in;
+    float2*       out;
+    const float2* tw;        // W_N^m = exp(-2 pi i m / N), m < N
+    uint32_t N;              // complex transform length handled by the passes
+    uint32_t T;              // threads per transform (N / E)
+    uint32_t M;              // transforms per CTA
+    uint32_t P;              // number of passes
+    PassInfo pass[kMaxPasses];
+    int64_t  inBatch, inElem;    // strides in complex elements
+    int64_t  outBatch, outElem;
+    uint32_t batch;              // number of transforms
+    int32_t  conjIn;             // conjugate on load  (inverse DFT = conj(FFT(conj x)))
+    int32_t  conjOut;            // conjugate on store
+    float    scale;              // applied on store
+    int32_t  batchMinor;         // thread layout: transform index fastest
+    int32_t  staged;             // tile through shared memory on load/store
+    // four-step column step: output k of transform b is multiplied by
+    // twBig[b * k] = W_bigN^{b k}
+    const float2* twBig;
+    uint32_t bigN;
+    // real-input kernels (N = h = half the real length)
+    int32_t  ioMode;             // IoMode
+    int32_t  realMode;           // r2c outmode / c2r inMode
+    const float2* twSplit;       // W_{2h}^i, i < h
+    uint32_t nMagic;             // fastdiv_magic(N)
+    // shared memory: per-transform stride (complex values) and, for staged
+    // input, the input row length
+    uint32_t slen;
+    uint32_t inCount;
+    uint32_t inMagic;            // fastdiv_magic(inCount)
+};
+
+} // namespace fftb200

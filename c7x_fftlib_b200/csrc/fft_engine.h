@@ -1,0 +1,22 @@
+// fft_engine.h -- host-side entry points of the device kernels (internal to
+// libfftlib_b200.so; the exported C ABI lives in capi_*.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_args.h"
+
+namespace fftb200 {
+
+// Largest CTA size the engine instantiation with register capacity emax
+// (complex values per thread) accepts; 0 if emax is not instantiated.
+int engine_max_threads(int emax);
+
+// Launch the FP32 Stockham engine described by a (grid = ceil(batch / M)).
+cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s);
+
+// W[i] = exp(-2 pi i (i mod n) / n), i < count, computed in FP64.
+cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s);
+
+} // namespace fftb200

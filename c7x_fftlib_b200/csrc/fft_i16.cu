@@ -1,0 +1,216 @@
+// fft_i16.cu -- batched int16 complex FFT with per-stage shift (K5),
+// bit-exact with FFTLIB_fft1dBatched_i16sc_c16sc_o16sc_cn
+// (src/fft_c7x/FFTLIB_fft1dBatched_i16sc_c16sc_o16sc/..._cn.c:191-338).
+//
+// The result of the reference is defined by its exact integer sequence:
+// radix-4 decimation-in-frequency stages with int16 two's-complement
+// intermediates, the VCROT90H-style multiply by j, Q15 twiddle products
+// rounded and saturated like VCMPYR1HH, a rounding right shift per stage,
+// the 8-point stage special case and a final bit reversal. Butterflies within
+// a stage are independent, so a CTA keeps one transform (as packed short2) in
+// shared memory and runs each stage's butterflies across its threads; every
+// butterfly performs exactly the reference's operations, so the output is
+// identical bit for bit.
+//
+// Register-resident fusion: two consecutive radix-4 stages touch 16 points
+// {k0 + i*M/16} of one length-M block, so a thread loads those 16 points,
+// runs both stages in registers and stores once, halving shared-memory
+// traffic and barriers.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_i16.h"
+
+namespace fftb200 {
+
+__device__ __forceinline__ int16_t wrap16(int v) { return (int16_t)(uint16_t)(unsigned)v; }
+
+// ((x + 0x4000) << 1) clamped to [-2^31, 0x7FFF0000], then >> 16.
+__device__ __forceinline__ int16_t q15_scale(long long x)
+{
+    long long t = (x + 0x4000LL) * 2LL;
+    t = t > 0x7FFF0000LL ? 0x7FFF0000LL : t;
+    t = t < -0x80000000LL ? -0x80000000LL : t;
+    return (int16_t)(t >> 16);
+}
+
+// -im with the VCROT90H saturation of -(-32768) to 32767.
+__device__ __forceinline__ int16_t rot90_re(int16_t im)
+{
+    return im == (int16_t)-32768 ? (int16_t)32767 : (int16_t)(-(int)im);
+}
+
+// Right shift rounding by the last bit shifted out; the mask is formed as
+// the reference forms it on x86 (32-bit shift by shift-1 with the count
+// taken mod 32, narrowed to int16), which makes shift 0 a no-op.
+__device__ __forceinline__ int16_t shift_round(int16_t v, uint32_t shift)
+{
+    const int16_t mask = (int16_t)(uint16_t)(1u << ((shift - 1u) & 31u));
+    const int vi = v;
+    const int s = (int)(shift & 31u);
+    return wrap16(((vi & (int)mask) != 0) ? ((vi >> s) + 1) : (vi >> s));
+}
+
+struct C16 {
+    int16_t re, im;
+};
+
+__device__ __forceinline__ C16 ld(const short2* p) { short2 v = *p; return C16{v.x, v.y}; }
+__device__ __forceinline__ void st(short2* p, C16 c) { *p = make_short2(c.re, c.im); }
+
+// One 4-point butterfly on p[0..3] (stride q apart in the stage), outputs
+// written back as bins 0,2,1,3 (the reference's slot order).
+// tw: the three Q15 twiddles (x1, x2, x3) or nullptr-equivalent when notw.
+__device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool notw,
+                                      const short2* tw, uint32_t k, uint32_t q, bool doShift,
+                                      uint32_t shift)
+{
+    const int16_t s1r = wrap16(p0.re + p2.re), s1i = wrap16(p0.im + p2.im);
+    const int16_t s2r = wrap16(p1.re + p3.re), s2i = wrap16(p1.im + p3.im);
+    const int16_t d1r = wrap16(p0.re - p2.re), d1i = wrap16(p0.im - p2.im);
+    const int16_t d2r = wrap16(p1.re - p3.re), d2i = wrap16(p1.im - p3.im);
+    const int16_t jr = rot90_re(d2i), ji = d2r;
+    C16 x0{wrap16(s1r + s2r), wrap16(s1i + s2i)};
+    C16 x1{wrap16(d1r - jr), wrap16(d1i - ji)};
+    C16 x2{wrap16(s1r - s2r), wrap16(s1i - s2i)};
+    C16 x3{wrap16(d1r + jr), wrap16(d1i + ji)};
+    if (!notw) {
+        const short2 w1 = tw[k], w2 = tw[q + k], w3 = tw[2 * q + k];
+        x0 = C16{q15_scale((long long)x0.re * 32768), q15_scale((long long)x0.im * 32768)};
+        const C16 a = x1, b = x2, c = x3;
+        x1 = C16{q15_scale((long long)a.re * w1.x - (long long)a.im * w1.y),
+                 q15_scale((long long)a.re * w1.y + (long long)a.im * w1.x)};
+        x2 = C16{q15_scale((long long)b.re * w2.x - (long long)b.im * w2.y),
+                 q15_scale((long long)b.re * w2.y + (long long)b.im * w2.x)};
+        x3 = C16{q15_scale((long long)c.re * w3.x - (long long)c.im * w3.y),
+                 q15_scale((long long)c.re * w3.y + (long long)c.im * w3.x)};
+    }
+    if (doShift) {
+        x0 = C16{shift_round(x0.re, shift), shift_round(x0.im, shift)};
+        x1 = C16{shift_round(x1.re, shift), shift_round(x1.im, shift)};
+        x2 = C16{shift_round(x2.re, shift), shift_round(x2.im, shift)};
+        x3 = C16{shift_round(x3.re, shift), shift_round(x3.im, shift)};
+    }
+    // slot order: bin0 -> 0, bin2 -> q, bin1 -> 2q, bin3 -> 3q
+    p0 = x0;
+    p1 = x2;
+    p2 = x1;
+    p3 = x3;
+}
+
+// Stage with block size m (q = m/4) on the 4 points {k + b*m + i*q}.
+__device__ __forceinline__ void stage_bfly(C16* pt, uint32_t m, uint32_t k, const short2* tw,
+                                           uint32_t shift)
+{
+    const uint32_t q = m / 4u;
+    const bool notw = (m == 4u) || (m == 8u && k == 0u);
+    bfly4(pt[0], pt[1], pt[2], pt[3], notw, tw, k, q, m != 8u, shift);
+}
+
+__global__ void __launch_bounds__(256) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
+                                                 const short2* __restrict__ w,
+                                                 const uint32_t* __restrict__ shifts, uint32_t n,
+                                                 uint32_t logn, uint32_t batch)
+{
+    extern __shared__ short2 sx[];
+    const uint32_t b = blockIdx.x;
+    if (b >= batch) return;
+    const short2* src = x + (size_t)b * n;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sx[i] = src[i];
+    __syncthreads();
+
+    uint32_t m = n, stage = 0, shift = 0;
+    const short2* tw = w;
+    // pairs of radix-4 stages fused in registers: 16 points per thread
+    while (m >= 16u) {
+        const uint32_t shiftA = shifts[stage];
+        const uint32_t m2 = m / 4u;
+        const uint32_t shiftB = shifts[stage + 1];
+        const short2* tw2 = tw + 3u * (m / 4u);
+        const uint32_t s16 = m / 16u;
+        const uint32_t groups = n / 16u; // (block, k0) pairs
+        for (uint32_t gi = threadIdx.x; gi < groups; gi += blockDim.x) {
+            const uint32_t blk = gi / s16, k0 = gi - blk * s16;
+            short2* base = sx + blk * m + k0;
+            C16 p[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) p[i] = ld(base + i * s16);
+            // stage A (block m): butterflies k = k0 + i*s16, points i, i+4, i+8, i+12
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                C16 t[4] = {p[i], p[i + 4], p[i + 8], p[i + 12]};
+                stage_bfly(t, m, k0 + (uint32_t)i * s16, tw, shiftA);
+                p[i] = t[0]; p[i + 4] = t[1]; p[i + 8] = t[2]; p[i + 12] = t[3];
+            }
+            // stage B (block m/4): sub-block s (points 4s..4s+3), butterfly k0
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                C16 t[4] = {p[4 * s], p[4 * s + 1], p[4 * s + 2], p[4 * s + 3]};
+                stage_bfly(t, m2, k0, tw2, shiftB);
+                p[4 * s] = t[0]; p[4 * s + 1] = t[1]; p[4 * s + 2] = t[2]; p[4 * s + 3] = t[3];
+            }
+#pragma unroll
+            for (int i = 0; i < 16; ++i) st(base + i * s16, p[i]);
+        }
+        __syncthreads();
+        shift = shiftB;
+        tw = tw2 + 3u * (m2 / 4u);
+        m = m2 / 4u;
+        stage += 2;
+    }
+    // one remaining radix-4 stage (m == 4 or 8)
+    if (m > 2u) {
+        shift = shifts[stage];
+        const uint32_t q = m / 4u;
+        for (uint32_t j = threadIdx.x; j < n / 4u; j += blockDim.x) {
+            const uint32_t blk = j / q, k = j - blk * q;
+            short2* base = sx + blk * m + k;
+            C16 t[4] = {ld(base), ld(base + q), ld(base + 2 * q), ld(base + 3 * q)};
+            stage_bfly(t, m, k, tw, shift);
+            st(base, t[0]); st(base + q, t[1]); st(base + 2 * q, t[2]); st(base + 3 * q, t[3]);
+        }
+        __syncthreads();
+        m = q;
+    }
+    // trailing radix-2 shares the shift of the 8-point stage
+    if (m == 2u) {
+        for (uint32_t j = threadIdx.x; j < n / 2u; j += blockDim.x) {
+            const C16 a = ld(sx + 2 * j), c = ld(sx + 2 * j + 1);
+            st(sx + 2 * j, C16{shift_round(wrap16(a.re + c.re), shift), shift_round(wrap16(a.im + c.im), shift)});
+            st(sx + 2 * j + 1, C16{shift_round(wrap16(a.re - c.re), shift), shift_round(wrap16(a.im - c.im), shift)});
+        }
+        __syncthreads();
+    }
+    // bit-reversed gather into natural order
+    short2* dst = y + (size_t)b * n;
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+        const uint32_t r = logn ? (__brev(k) >> (32u - logn)) : 0u;
+        dst[k] = sx[r];
+    }
+}
+
+uint32_t i16_num_shifts(uint32_t n)
+{
+    uint32_t s = 0;
+    for (uint32_t m = n; m > 2u; m /= 4u) ++s;
+    return s;
+}
+
+cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const uint32_t* shifts,
+                           uint32_t n, uint32_t batch, cudaStream_t s)
+{
+    if (batch == 0) return cudaSuccess;
+    uint32_t logn = 0;
+    while ((1u << logn) < n) ++logn;
+    const size_t smem = (size_t)n * sizeof(short2);
+    if (smem > 48u * 1024u) {
+        cudaError_t e = cudaFuncSetAttribute(k_fft_i16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const uint32_t threads = n >= 4096u ? 256u : (n / 16u >= 32u ? n / 16u : 32u);
+    k_fft_i16<<<batch, threads, smem, s>>>((const short2*)x, (short2*)y, (const short2*)w, shifts, n, logn,
+                                           batch);
+    return cudaGetLastError();
+}
+
+} // namespace fftb200

@@ -1,0 +1,54 @@
+// fft_kernels.cu -- dispatch over the FP32 engine instantiations and the
+// FP64 twiddle-table generator.
+#include "fft_engine.h"
+
+namespace fftb200 {
+
+template <int EMAX, int MAXT>
+cudaError_t launch_generic(const FftArgs& a, cudaStream_t s);
+extern template cudaError_t launch_generic<8, 1024>(const FftArgs&, cudaStream_t);
+extern template cudaError_t launch_generic<16, 512>(const FftArgs&, cudaStream_t);
+extern template cudaError_t launch_generic<32, 512>(const FftArgs&, cudaStream_t);
+
+// W[i] = exp(-2 pi i (i mod n) / n) for i < count, evaluated in FP64 with
+// the angle reduced exactly in integers (sincospi of 2 r / n, r = i mod n)
+// and rounded once to FP32.
+__global__ void k_twiddle_f64(float2* __restrict__ w, uint32_t n, uint32_t count)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint32_t r = i % n;
+    double s, c;
+    sincospi(2.0 * (double)r / (double)n, &s, &c);
+    w[i] = make_float2((float)c, (float)(-s));
+}
+
+int engine_max_threads(int emax)
+{
+    switch (emax) {
+    case 8: return 1024;
+    case 16: return 512;
+    case 32: return 512;
+    default: return 0;
+    }
+}
+
+cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
+{
+    if (a.batch == 0) return cudaSuccess;
+    switch (emax) {
+    case 8: return launch_generic<8, 1024>(a, s);
+    case 16: return launch_generic<16, 512>(a, s);
+    case 32: return launch_generic<32, 512>(a, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s)
+{
+    if (count == 0) return cudaSuccess;
+    k_twiddle_f64<<<(count + 255) / 256, 256, 0, s>>>(w, n, count);
+    return cudaGetLastError();
+}
+
+} // namespace fftb200

@@ -1,0 +1,266 @@
+// fft_stockham.cuh -- the FP32 batched FFT engine (device side).
+//
+// One CTA holds M transforms of length N in shared memory. T threads work on
+// one transform; in each Stockham pass a thread gathers its butterflies'
+// inputs into registers (up to EMAX complex values), applies the pass
+// twiddles, runs the in-register DFT codelet and scatters the outputs.
+// The first pass reads straight from HBM (or from a shared-memory tile for
+// short transforms) and the last pass writes straight to HBM in natural
+// order, so the reference's separate bit/digit-reversal copy
+// (FFTLIB_fft1dBatched_i32fc_c32fc_o32fc_cn.c:412-491) disappears into the
+// pass index arithmetic: each transform costs one HBM read and one HBM write.
+//
+// The inverse transform is conj(FFT(conj(x))) * scale, applied on load and
+// store (FFTLIB_ifft1dBatched_i32fc_c32fc_o32fc_cn.c:209-227, 432-506).
+// Real-input variants fuse the reference's split post-process
+// (FFTLIB_fft1dBatched_i32f_c32fc_o32fc_cn.c:40-121) into an epilogue and
+// its split pre-process (FFTLIB_ifft1dBatched_i32fc_c32fc_o32f_cn.c:35-83)
+// into the first pass.
+#pragma once
+
+#include "fft_args.h"
+#include "fft_device.cuh"
+
+namespace fftb200 {
+
+// Smallest radix an engine instantiation carries: the widest one leaves the
+// short radices (many butterflies per thread, large unrolled code) to the
+// narrower instantiations.
+__host__ __device__ constexpr int engine_min_radix(int emax) { return emax >= 32 ? 8 : 1; }
+
+// Calls f(integral_constant<R>) for the runtime radix r; radices are the
+// 2^a 3^b 5^c values in [engine_min_radix(EMAX), EMAX] (1 is the trivial
+// one-point transform).
+template <int EMAX, class F>
+FFT_DEV void dispatch_radix(int r, F&& f)
+{
+    static_for<EMAX + 1>([&](auto d) {
+        constexpr int D = decltype(d)::value;
+        constexpr bool ok235 = [] {
+            int x = D;
+            if (x < 1 || x < engine_min_radix(EMAX)) return false;
+            while (x % 2 == 0) x /= 2;
+            while (x % 3 == 0) x /= 3;
+            while (x % 5 == 0) x /= 5;
+            return x == 1;
+        }();
+        if constexpr (ok235) {
+            if (r == D) f(d);
+        }
+    });
+}
+
+// Pass-0 input element idx of transform b (complex index into the pass's
+// length-N sequence), with the c2r split pre-process when requested.
+FFT_DEV float2 load_in(const FftArgs& a, uint32_t b, uint32_t idx, const float2* tile)
+{
+    float2 z;
+    if (a.ioMode == IO_C2R_SPLIT) {
+        // Z = X A' + y B' = 0.5 [(X + y) + i conj(W) (X - y)], W = W_{2h}^idx,
+        // y = conj(X[h - idx]) (inMode 0) or X[idx + h] (inMode 1).
+        const uint32_t h = a.N;
+        const uint32_t ip = a.realMode ? idx + h : h - idx;
+        float2 x, y;
+        if (a.staged) {
+            x = tile[smem_swz(idx)];
+            y = tile[smem_swz(ip)];
+        } else {
+            const float2* row = a.in + (int64_t)b * a.inBatch;
+            x = row[(int64_t)idx * a.inElem];
+            y = row[(int64_t)ip * a.inElem];
+        }
+        if (!a.realMode) y = cconj(y);
+        const float2 w = __ldg(&a.twSplit[idx]);
+        const float2 s = cadd(x, y), d = csub(x, y);
+        const float2 icw = make_float2(w.y, w.x); // i * conj(w)
+        z = cscale(cadd(s, cmul(icw, d)), 0.5f);
+    } else if (a.staged) {
+        z = tile[smem_swz(idx)];
+    } else {
+        z = a.in[(int64_t)b * a.inBatch + (int64_t)idx * a.inElem];
+    }
+    return a.conjIn ? cconj(z) : z;
+}
+
+FFT_DEV float2 finish(const FftArgs& a, float2 z)
+{
+    if (a.conjOut) z = cconj(z);
+    return cscale(z, a.scale);
+}
+
+template <int EMAX, int R>
+FFT_DEV void run_pass(const FftArgs& a, int p, float2 (&v)[EMAX], float2* sm,
+                      uint32_t t, uint32_t b, bool active)
+{
+    constexpr int BMAX = EMAX / R;
+    const PassInfo pi = a.pass[p];
+    const bool first = (p == 0);
+    const bool last = (p + 1 == (int)a.P);
+    const uint32_t T = a.T;
+    const uint32_t nb = pi.stride; // butterflies in this pass: N / R
+
+    // gather
+    static_for<BMAX>([&](auto i) {
+        const uint32_t j = t + (uint32_t)i * T;
+        if (j < nb) {
+            static_for<R>([&](auto q) {
+                const uint32_t idx = j + (uint32_t)q * nb;
+                float2 z;
+                if (first) {
+                    z = (active || a.staged) ? load_in(a, b, idx, sm) : make_float2(0.f, 0.f);
+                } else {
+                    z = sm[smem_swz(idx)];
+                }
+                v[i * R + q] = z;
+            });
+        }
+    });
+
+    // twiddle and butterfly
+    static_for<BMAX>([&](auto i) {
+        const uint32_t j = t + (uint32_t)i * T;
+        if (j < nb) {
+            if (!first) {
+                const uint32_t g = fastdiv(j, pi.Ns, pi.nsMagic);
+                const uint32_t k = j - g * pi.Ns;
+                const uint32_t step = k * pi.twStride;
+                static_for<R - 1>([&](auto q1) {
+                    constexpr int q = decltype(q1)::value + 1;
+                    v[i * R + q] = cmul(v[i * R + q], __ldg(&a.tw[q * step]));
+                });
+            }
+            dft<R>(&v[i * R]);
+        }
+    });
+
+    // scatter
+    const bool direct = last && !a.staged && a.ioMode != IO_R2C_SPLIT;
+    if (direct) {
+        if (active) {
+            float2* row = a.out + (int64_t)b * a.outBatch;
+            static_for<BMAX>([&](auto i) {
+                const uint32_t j = t + (uint32_t)i * T;
+                if (j < nb) {
+                    static_for<R>([&](auto q) {
+                        const uint32_t idx = j + (uint32_t)q * nb;
+                        float2 z = finish(a, v[i * R + q]);
+                        if (a.twBig) z = cmul(z, __ldg(&a.twBig[b * idx]));
+                        row[(int64_t)idx * a.outElem] = z;
+                    });
+                }
+            });
+        }
+        return;
+    }
+    if (!first || a.staged) __syncthreads(); // every read of this pass is done
+    static_for<BMAX>([&](auto i) {
+        const uint32_t j = t + (uint32_t)i * T;
+        if (j < nb) {
+            const uint32_t g = fastdiv(j, pi.Ns, pi.nsMagic);
+            const uint32_t k = j - g * pi.Ns;
+            const uint32_t base = g * pi.Ns * (uint32_t)R + k;
+            static_for<R>([&](auto q) { sm[smem_swz(base + (uint32_t)q * pi.Ns)] = v[i * R + q]; });
+        }
+    });
+    __syncthreads();
+}
+
+// Y[i] = E + (-i W) O, E = (Z[i] + conj Z[h-i]) / 2, O = (Z[i] - conj Z[h-i]) / 2,
+// W = W_{2h}^i: the reference's A[i] Z[i] + B[i] conj(Z[h-i]).
+FFT_DEV float2 r2c_split(float2 z, float2 zp, float2 w)
+{
+    const float2 zc = cconj(zp);
+    const float2 e = cscale(cadd(z, zc), 0.5f);
+    const float2 o = cscale(csub(z, zc), 0.5f);
+    const float2 miw = make_float2(w.y, -w.x); // -i * w
+    return cadd(e, cmul(miw, o));
+}
+
+FFT_DEV void r2c_epilogue(const FftArgs& a, const float2* sm, uint32_t t, uint32_t b, bool active)
+{
+    if (!active) return;
+    const uint32_t h = a.N;
+    float2* row = a.out + (int64_t)b * a.outBatch;
+    for (uint32_t i = t; i <= h / 2; i += a.T) {
+        if (i == 0) {
+            const float2 z0 = sm[smem_swz(0)];
+            row[0] = make_float2(z0.x + z0.y, 0.f);
+            row[h] = make_float2(z0.x - z0.y, 0.f); // Nyquist bin
+            continue;
+        }
+        const uint32_t ip = h - i;
+        const float2 zi = sm[smem_swz(i)], zp = sm[smem_swz(ip)];
+        const float2 yi = r2c_split(zi, zp, __ldg(&a.twSplit[i]));
+        row[i] = yi;
+        if (a.realMode) row[2 * h - i] = cconj(yi);
+        if (ip != i) {
+            const float2 yp = r2c_split(zp, zi, __ldg(&a.twSplit[ip]));
+            row[ip] = yp;
+            if (a.realMode) row[2 * h - ip] = cconj(yp);
+        }
+    }
+}
+
+// Cooperative, coalesced copy of the CTA's contiguous input rows into the
+// per-transform shared-memory regions.
+FFT_DEV void stage_in(const FftArgs& a, float2* smem, uint32_t b0)
+{
+    const uint32_t inCount = a.inCount, inMagic = a.inMagic, slen = a.slen;
+    const uint32_t nm = min(a.M, a.batch - b0);
+    const uint32_t total = nm * inCount;
+    const float2* src = a.in + (int64_t)b0 * a.inBatch;
+    for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
+        const uint32_t mm = fastdiv(e, inCount, inMagic);
+        const uint32_t i = e - mm * inCount;
+        smem[mm * slen + smem_swz(i)] = src[e];
+    }
+}
+
+FFT_DEV void stage_out(const FftArgs& a, const float2* smem, uint32_t b0)
+{
+    const uint32_t slen = a.slen;
+    const uint32_t nm = min(a.M, a.batch - b0);
+    const uint32_t total = nm * a.N;
+    float2* dst = a.out + (int64_t)b0 * a.outBatch;
+    for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
+        const uint32_t mm = fastdiv(e, a.N, a.nMagic);
+        const uint32_t i = e - mm * a.N;
+        dst[e] = finish(a, smem[mm * slen + smem_swz(i)]);
+    }
+}
+
+// Whole-transform body for the CTA's transforms b0 .. b0+M-1.
+template <int EMAX>
+FFT_DEV void fft_tile(const FftArgs& a, float2* smem, uint32_t b0)
+{
+    const uint32_t tid = threadIdx.x;
+    uint32_t m, t;
+    if (a.batchMinor) {
+        t = tid / a.M;
+        m = tid - t * a.M;
+    } else {
+        m = tid / a.T;
+        t = tid - m * a.T;
+    }
+    const uint32_t b = b0 + m;
+    const bool active = b < a.batch;
+    float2* sm = smem + m * a.slen;
+
+    if (a.staged) {
+        stage_in(a, smem, b0);
+        __syncthreads();
+    }
+    float2 v[EMAX];
+    for (int p = 0; p < (int)a.P; ++p) {
+        dispatch_radix<EMAX>(a.pass[p].R, [&](auto r) {
+            run_pass<EMAX, decltype(r)::value>(a, p, v, sm, t, b, active);
+        });
+    }
+    if (a.ioMode == IO_R2C_SPLIT) {
+        r2c_epilogue(a, sm, t, b, active);
+    } else if (a.staged) {
+        stage_out(a, smem, b0);
+    }
+}
+
+} // namespace fftb200

@@ -1,0 +1,75 @@
+// plan.h -- planning, plan cache and device launch sequences of the FP32
+// FFT kernels (internal to libfftlib_b200.so).
+//
+// A ComplexPlan describes one complex transform length n on one device:
+// either a single-kernel Stockham schedule (n <= kMaxSingleN) or a four-step
+// split n = n1 * n2 (column FFTs with the W_n twiddle fused into their store,
+// then row FFTs writing the transposed result). Its twiddle tables are
+// generated once on the device in FP64 and stay resident in HBM.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "fft_args.h"
+
+namespace fftb200 {
+
+constexpr uint32_t kMaxSingleN = 16384;
+
+struct EnginePlan {
+    uint32_t n = 0;
+    int emax = 0;        // register capacity of the engine instantiation
+    uint32_t T = 0;      // threads per transform
+    int P = 0;           // passes
+    int R[kMaxPasses] = {};
+    double score = 0.0;  // heuristic cost (lower is better)
+};
+
+bool is_235(uint32_t n);
+
+// All feasible single-kernel schedules for n, best heuristic first.
+std::vector<EnginePlan> engine_candidates(uint32_t n);
+bool plan_engine(uint32_t n, EnginePlan* out);
+std::string describe(const EnginePlan& e);
+// Four-step split n = n1 * n2 (n1 <= n2, both single-kernel lengths).
+bool split_four_step(uint32_t n, uint32_t* n1, uint32_t* n2);
+
+struct ComplexPlan {
+    int device = 0;
+    uint32_t n = 0;
+    bool fourStep = false;
+    EnginePlan eng;                  // single kernel
+    uint32_t n1 = 0, n2 = 0;         // four-step
+    EnginePlan eng1, eng2;
+    float2* tw = nullptr;            // W_n, n entries
+    float2* tw1 = nullptr;           // W_n1 (four-step)
+    float2* tw2 = nullptr;           // W_n2 (four-step)
+    float2* twSplit = nullptr;       // W_{2n}^i, i < n (real-input kernels)
+};
+
+// Cached per (current device, n). needSplit also creates twSplit.
+// Returns nullptr (and sets *err) if n is not 2^a 3^b 5^c or on CUDA errors.
+ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err);
+void release_all_plans();
+
+// Pick transforms-per-CTA and the staged-I/O mode for a launch.
+void finalize_launch(FftArgs& a, const EnginePlan& e, bool contiguousIn, bool contiguousOut);
+FftArgs engine_args(const EnginePlan& e, const float2* tw);
+
+// Launch sequences (device pointers, stream s, no synchronization).
+// run_c2c may overwrite `in` (four-step work buffer).
+cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse,
+                    cudaStream_t s);
+// h = p->n = numPoints / 2; x: batch x 2h reals; scratch: batch x h complex
+// (needed only for the four-step path); y: batch x (h+1) or x 2h bins.
+cudaError_t run_r2c(const ComplexPlan* p, float* x, float2* scratch, float2* y, uint32_t batch, int outmode,
+                    cudaStream_t s);
+// x: batch x (h+1) or x 2h bins; y: batch x 2h reals.
+cudaError_t run_c2r(const ComplexPlan* p, const float2* x, float2* scratch, float* y, uint32_t batch,
+                    int inmode, cudaStream_t s);
+
+} // namespace fftb200

@@ -1,0 +1,71 @@
+/*
+ * fftlib_b200_ext.h -- extensions of libfftlib_b200.so beyond the FFTLIB API.
+ * None of these has a counterpart in the reference library; existing FFTLIB
+ * callers do not need them.
+ */
+#ifndef FFTLIB_B200_EXT_H_
+#define FFTLIB_B200_EXT_H_
+
+#include "FFTLIB_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* exported from libfftlib_b200.so (built with hidden default visibility) */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* Text of the last failure on the calling thread ("" if none). */
+const char *FFTLIB_b200_lastError(void);
+
+/* Library version, major * 10000 + minor * 100 + patch. */
+int FFTLIB_b200_version(void);
+
+/* Frees every cached plan (twiddle tables) on every device. pBlocks
+ * initialised earlier must be initialised again before use. */
+void FFTLIB_b200_releasePlans(void);
+
+/* Writes the kernel schedule chosen for a complex length-numPoints transform
+ * (radices per pass, threads per transform, or the four-step split) into buf. */
+FFTLIB_STATUS FFTLIB_b200_describePlan(uint32_t numPoints, char *buf, uint32_t len);
+
+/* Asynchronous variants of the _kernel calls: every buffer must be device
+ * (or managed) memory; the work is enqueued on `stream` (a cudaStream_t;
+ * NULL is the legacy default stream) and the call returns without waiting.
+ * pBlock must come from the matching _init. These calls can be captured in
+ * a CUDA graph. */
+FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync(FFTLIB_F32 *pX, FFTLIB_F32 *pY,
+                                                                     uint32_t numPoints, uint32_t numChannels,
+                                                                     void *pBlock, void *stream);
+FFTLIB_STATUS FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32fc_kernelAsync(FFTLIB_F32 *pX, FFTLIB_F32 *pY,
+                                                                      uint32_t numPoints, uint32_t numChannels,
+                                                                      void *pBlock, void *stream);
+FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32f_c32fc_o32fc_kernelAsync(FFTLIB_F32 *pX, FFTLIB_F32 *pXFFT,
+                                                                    FFTLIB_F32 *pY, uint32_t numPoints,
+                                                                    uint32_t numChannels, uint8_t outmode,
+                                                                    void *pBlock, void *stream);
+FFTLIB_STATUS FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32f_kernelAsync(FFTLIB_F32 *pX, FFTLIB_F32 *pXFFT,
+                                                                     FFTLIB_F32 *pY, uint32_t numPoints,
+                                                                     uint32_t numChannels, uint8_t inMode,
+                                                                     void *pBlock, void *stream);
+FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync(int16_t *pX, int16_t *pW, int16_t *pY,
+                                                                     uint32_t *pShift, uint32_t numShifts,
+                                                                     uint32_t numPoints, uint32_t numChannels,
+                                                                     void *pBlock, void *stream);
+
+/* The twiddle tables the reference test drivers build for the c2c/ifft
+ * kernels and the int16 kernel, bit-identical to theirs. */
+void FFTLIB_b200_tw_gen_c2c(FFTLIB_F32 *pW, uint32_t numPoints);
+void FFTLIB_b200_tw_gen_i16(int16_t *pW, uint32_t numPoints);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFTLIB_B200_EXT_H_ */

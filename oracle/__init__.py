@@ -358,3 +358,59 @@ def real_signal(n: int, channels: int, seed: int) -> np.ndarray:
 
 def int16_input(n: int, channels: int, seed: int, lo=-2048, hi=2047) -> np.ndarray:
     return rng(seed).integers(lo, hi + 1, 2 * n * channels).astype(np.int16)
+
+
+# --------------------------------------------------------------------------
+# CPU baseline timing of the reference _cn code (bench.py's reference arm and
+# cpu_baseline leg): one thread per host core, each calling the reference on
+# a contiguous slice of channels (channels are independent in the API). The
+# input is re-copied before every repetition (the reference overwrites pX);
+# the copy is outside the timed region.
+# --------------------------------------------------------------------------
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def time_reference_c2c(n: int, channels: int, threads: int | None = None, reps: int = 3,
+                       inverse: bool = False, seed: int = 0):
+    """Median seconds for the reference _cn to transform `channels` channels
+    of length n, split over `threads` threads; returns (seconds, threads)."""
+    import threading
+    import time
+
+    threads = max(1, min(threads or host_threads(), channels))
+    kind = "ifft" if inverse else "c2c"
+    L = ref_lib(kind)
+    fn = L.FFTLIB_ifft1dBatched_i32fc_c32fc_o32fc_cn if inverse else L.FFTLIB_fft1dBatched_i32fc_c32fc_o32fc_cn
+    fn.restype = C.c_int
+    x0 = uniform_c2c(n, channels, seed)
+    w = ref_tw_gen_c2c(n)
+    per = [channels // threads + (1 if i < channels % threads else 0) for i in range(threads)]
+    starts = np.cumsum([0] + per[:-1])
+    bufs = [(np.empty(2 * n * c, np.float32), np.empty(2 * n * c, np.float32)) for c in per]
+    times = []
+    for _ in range(reps):
+        for (xb, _), s, c in zip(bufs, starts, per):
+            xb[:] = x0[2 * n * s: 2 * n * (s + c)]
+        barrier = threading.Barrier(threads + 1)
+
+        def work(i):
+            xb, yb = bufs[i]
+            c = per[i]
+            barrier.wait()
+            fn(_vp(xb), _bp(FFTLIB_FLOAT32, 2 * n * c), _vp(w), _bp(FFTLIB_FLOAT32, 2 * n), _vp(yb),
+               _bp(FFTLIB_FLOAT32, 2 * n * c), _u32(n), _u32(c))
+
+        ts = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
+        for t in ts:
+            t.start()
+        barrier.wait()
+        t0 = time.perf_counter()
+        for t in ts:
+            t.join()
+        times.append(time.perf_counter() - t0)
+    return float(np.median(times)), threads
