@@ -31,7 +31,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -74,59 +73,83 @@ def traffic_from_profile(kernel_tag):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """SM clock and throttle-reason samples taken during the timed region
+    through NVML (every ~2 ms, plus one sample at entry and exit)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {  # NVML clocks-event-reason bits
+        "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4,
+    }
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.reasons = set()
+        self.smax = None
+        self._stop = threading.Event()
+        self._nv = None
+
+    def _sample(self):
+        nv = self._nv
+        try:
+            self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            for name, bit in self.REASONS.items():
+                if bits & bit:
+                    self.reasons.add(name)
+        except Exception:
+            pass
+
+    def _handle(self, nv):
+        """NVML handle of the CUDA device (NVML ignores CUDA_VISIBLE_DEVICES):
+        by UUID, else by PCI address, else by index."""
+        import torch
+
+        prop = torch.cuda.get_device_properties(self.index)
+        uuid = getattr(prop, "uuid", None)
+        if uuid is not None:
+            try:
+                return nv.nvmlDeviceGetHandleByUUID(f"GPU-{uuid}")
+            except Exception:
+                pass
+        if hasattr(prop, "pci_bus_id"):
+            try:
+                addr = f"{getattr(prop, 'pci_domain_id', 0):08x}:{prop.pci_bus_id:02x}:{prop.pci_device_id:02x}.0"
+                return nv.nvmlDeviceGetHandleByPciBusId(addr)
+            except Exception:
+                pass
+        return nv.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _loop(self):
+        while not self._stop.is_set():
+            self._sample()
+            time.sleep(0.002)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self._nv = nv
+            self.h = self._handle(nv)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+            self._sample()
+            self.t = threading.Thread(target=self._loop, daemon=True)
             self.t.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+        except Exception:
+            self._nv = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self._nv:
+            self._stop.set()
+            self.t.join(timeout=2)
+            self._sample()
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for name, val in zip(names, f[5:9]):
-                if val.lower() == "active":
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
 def dist_setup(args):
@@ -180,7 +203,7 @@ def our_arm(args, world, rank, local):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    n, ch = N_POINTS, CHANNELS
+    n, ch = N_POINTS, args.channels
     g = torch.Generator(device="cuda").manual_seed(1234 + rank)
     X = torch.rand(2 * n * ch, device="cuda", generator=g) * 2 - 1
     Y = torch.empty_like(X)
@@ -220,6 +243,13 @@ def our_arm(args, world, rank, local):
     ms_step = ms / args.steps
     per_gpu_gbs = algo_bytes(n, ch) / (ms_step * 1e-3) / 1e9
     value = per_gpu_gbs * world
+
+    if args.quick:  # profiling runs: the timed launches only
+        if dist:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"quick": True, "ms_per_step": ms_step, "GBps": value, "channels": ch}))
+        return
 
     # parity spot check of the timed output (a few channels against FP64)
     import numpy as np
@@ -297,6 +327,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--channels", type=int, default=CHANNELS, help="channels per GPU (default: the workload's 8192)")
+    ap.add_argument("--quick", action="store_true", help="time the kernel only (for profiler captures)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":

@@ -35,7 +35,8 @@ struct PassInfo {
     uint32_t Ns;
     uint32_t nsMagic;   // fastdiv_magic(Ns)
     uint32_t stride;    // N / R
-    uint32_t twStride;  // N / (Ns * R): index step into the W_N table
+    uint32_t twOffset;  // this pass's block in the twiddle table: entry
+                        // (q-1)*Ns + k holds W_{Ns*R}^{q*k}, q = 1..R-1, k < Ns
 };
 
 enum IoMode : int32_t {
@@ -47,7 +48,7 @@ enum IoMode : int32_t {
 struct FftArgs {
     const float2* in;
     float2*       out;
-    const float2* tw;        // W_N^m = exp(-2 pi i m / N), m < N
+    const float2* tw;        // per-pass twiddle blocks (PassInfo::twOffset)
     uint32_t N;              // complex transform length handled by the passes
     uint32_t T;              // threads per transform (N / E)
     uint32_t M;              // transforms per CTA

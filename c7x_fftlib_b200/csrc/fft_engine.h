@@ -19,4 +19,13 @@ cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s);
 // W[i] = exp(-2 pi i (i mod n) / n), i < count, computed in FP64.
 cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s);
 
+// Per-pass twiddle blocks: pass j occupies entries off[j] .. off[j] +
+// (R[j]-1)*Ns[j]; entry off + (q-1)*Ns + k = W_{Ns*R}^{q*k}, computed in FP64.
+struct TwiddlePasses {
+    uint32_t P;
+    uint32_t R[kMaxPasses], Ns[kMaxPasses], off[kMaxPasses];
+    uint32_t total;
+};
+cudaError_t launch_twiddle_passes(float2* w, const TwiddlePasses& tp, cudaStream_t s);
+
 } // namespace fftb200

@@ -17,10 +17,11 @@ __global__ void __launch_bounds__(MAXT) k_fft_stockham(const __grid_constant__ F
     fft_tile<EMAX>(a, smem, blockIdx.x * a.M);
 }
 
-// Raises a kernel's dynamic shared-memory limit once per device to the
-// largest amount requested so far.
-template <class K>
-cudaError_t ensure_smem(K kernel, size_t smem)
+// Raises the dynamic shared-memory limit of one kernel instantiation, once
+// per device, to the largest amount requested so far. The bookkeeping lives
+// in the template so every instantiation keeps its own.
+template <int EMAX, int MAXT>
+cudaError_t ensure_smem(size_t smem)
 {
     if (smem <= 48u * 1024u) return cudaSuccess;
     static std::mutex mu;
@@ -30,7 +31,7 @@ cudaError_t ensure_smem(K kernel, size_t smem)
     if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lock(mu);
     if (dev < 64 && configured[dev] >= smem) return cudaSuccess;
-    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(k_fft_stockham<EMAX, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess && dev < 64) configured[dev] = smem;
     return e;
 }
@@ -39,7 +40,7 @@ template <int EMAX, int MAXT>
 cudaError_t launch_generic(const FftArgs& a, cudaStream_t s)
 {
     const size_t smem = (size_t)a.M * a.slen * sizeof(float2);
-    cudaError_t e = ensure_smem(k_fft_stockham<EMAX, MAXT>, smem);
+    cudaError_t e = ensure_smem<EMAX, MAXT>(smem);
     if (e != cudaSuccess) return e;
     const uint32_t grid = (a.batch + a.M - 1) / a.M;
     k_fft_stockham<EMAX, MAXT><<<grid, a.T * a.M, smem, s>>>(a);

@@ -23,6 +23,23 @@ __global__ void k_twiddle_f64(float2* __restrict__ w, uint32_t n, uint32_t count
     w[i] = make_float2((float)c, (float)(-s));
 }
 
+// Per-pass blocks: the angle 2 pi (q k mod Ns R) / (Ns R) is reduced
+// exactly in integers before the FP64 sincospi.
+__global__ void k_twiddle_passes(float2* __restrict__ w, const TwiddlePasses tp)
+{
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= tp.total) return;
+    uint32_t p = 0;
+    while (p + 1 < tp.P && e >= tp.off[p + 1]) ++p;
+    const uint32_t l = e - tp.off[p];
+    const uint32_t ns = tp.Ns[p], m = ns * tp.R[p];
+    const uint32_t q = l / ns + 1u, k = l % ns;
+    const uint32_t r = (uint32_t)(((uint64_t)q * k) % m);
+    double s, c;
+    sincospi(2.0 * (double)r / (double)m, &s, &c);
+    w[e] = make_float2((float)c, (float)(-s));
+}
+
 int engine_max_threads(int emax)
 {
     switch (emax) {
@@ -42,6 +59,13 @@ cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
     case 32: return launch_generic<32, 512>(a, s);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_twiddle_passes(float2* w, const TwiddlePasses& tp, cudaStream_t s)
+{
+    if (tp.total == 0) return cudaSuccess;
+    k_twiddle_passes<<<(tp.total + 255) / 256, 256, 0, s>>>(w, tp);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s)

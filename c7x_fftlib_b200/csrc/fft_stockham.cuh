@@ -123,10 +123,11 @@ FFT_DEV void run_pass(const FftArgs& a, int p, float2 (&v)[EMAX], float2* sm,
             if (!first) {
                 const uint32_t g = fastdiv(j, pi.Ns, pi.nsMagic);
                 const uint32_t k = j - g * pi.Ns;
-                const uint32_t step = k * pi.twStride;
+                // lanes of a warp read consecutive k: coalesced twiddle loads
+                const float2* tw = a.tw + pi.twOffset + k;
                 static_for<R - 1>([&](auto q1) {
                     constexpr int q = decltype(q1)::value + 1;
-                    v[i * R + q] = cmul(v[i * R + q], __ldg(&a.tw[q * step]));
+                    v[i * R + q] = cmul(v[i * R + q], __ldg(&tw[(q - 1) * pi.Ns]));
                 });
             }
             dft<R>(&v[i * R]);

@@ -130,14 +130,15 @@ FftArgs engine_args(const EnginePlan& e, const float2* tw)
     a.N = e.n;
     a.T = e.T;
     a.P = (uint32_t)e.P;
-    uint32_t ns = 1;
+    uint32_t ns = 1, off = 0;
     for (int p = 0; p < e.P; ++p) {
         const uint32_t r = (uint32_t)e.R[p];
         a.pass[p].R = (int32_t)r;
         a.pass[p].Ns = ns;
         a.pass[p].nsMagic = fastdiv_magic(ns);
         a.pass[p].stride = e.n / r;
-        a.pass[p].twStride = e.n / (ns * r);
+        a.pass[p].twOffset = off;
+        if (p > 0) off += (r - 1u) * ns;
         ns *= r;
     }
     a.scale = 1.0f;
@@ -182,6 +183,28 @@ cudaError_t make_table(float2** p, uint32_t n, uint32_t count, cudaStream_t s)
     return launch_twiddle(*p, n, count, s);
 }
 
+// Per-pass twiddle blocks of a single-kernel schedule (see PassInfo).
+cudaError_t make_pass_table(float2** p, const EnginePlan& e, cudaStream_t s)
+{
+    TwiddlePasses tp{};
+    uint32_t ns = 1, off = 0;
+    for (int i = 0; i < e.P; ++i) {
+        const uint32_t r = (uint32_t)e.R[i];
+        if (i > 0) {
+            tp.R[tp.P] = r;
+            tp.Ns[tp.P] = ns;
+            tp.off[tp.P] = off;
+            tp.P++;
+            off += (r - 1u) * ns;
+        }
+        ns *= r;
+    }
+    tp.total = off;
+    cudaError_t err = cudaMalloc((void**)p, sizeof(float2) * std::max(off, 1u));
+    if (err != cudaSuccess) return err;
+    return launch_twiddle_passes(*p, tp, s);
+}
+
 } // namespace
 
 // n = n1 * n2 with n1 <= n2, n1 as close to sqrt(n) as possible, both with
@@ -220,14 +243,14 @@ ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err)
         p->device = dev;
         p->n = n;
         if (n <= kMaxSingleN && plan_engine(n, &p->eng)) {
-            *err = make_table(&p->tw, n, n, s);
+            *err = make_pass_table(&p->tw, p->eng, s);
         } else if (split_four_step(n, &p->n1, &p->n2)) {
             p->fourStep = true;
             plan_engine(p->n1, &p->eng1);
             plan_engine(p->n2, &p->eng2);
             *err = make_table(&p->tw, n, n, s);
-            if (*err == cudaSuccess) *err = make_table(&p->tw1, p->n1, p->n1, s);
-            if (*err == cudaSuccess) *err = make_table(&p->tw2, p->n2, p->n2, s);
+            if (*err == cudaSuccess) *err = make_pass_table(&p->tw1, p->eng1, s);
+            if (*err == cudaSuccess) *err = make_pass_table(&p->tw2, p->eng2, s);
         } else {
             *err = cudaErrorInvalidValue;
         }

@@ -45,9 +45,10 @@ struct ComplexPlan {
     EnginePlan eng;                  // single kernel
     uint32_t n1 = 0, n2 = 0;         // four-step
     EnginePlan eng1, eng2;
-    float2* tw = nullptr;            // W_n, n entries
-    float2* tw1 = nullptr;           // W_n1 (four-step)
-    float2* tw2 = nullptr;           // W_n2 (four-step)
+    float2* tw = nullptr;            // single kernel: per-pass twiddle blocks;
+                                     // four-step: W_n, n entries (column step)
+    float2* tw1 = nullptr;           // per-pass blocks of the n1 schedule
+    float2* tw2 = nullptr;           // per-pass blocks of the n2 schedule
     float2* twSplit = nullptr;       // W_{2n}^i, i < n (real-input kernels)
 };
 
