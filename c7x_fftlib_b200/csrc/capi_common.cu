@@ -1,6 +1,7 @@
 // capi_common.cu -- error reporting, pointer classification and host-buffer
 // staging for the exported C ABI.
 #include "capi_common.h"
+#include "plan.h"
 
 #include <stdarg.h>
 #include <stdio.h>
@@ -113,7 +114,9 @@ cudaError_t run_channels(std::vector<ChannelBuf>& bufs, uint32_t channels, const
         cudaStream_t s = cudaStreamPerThread;
         cudaError_t e = fn(dptr, 0, channels, s);
         if (e != cudaSuccess) return e;
-        return cudaStreamSynchronize(s);
+        e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess && take_device_error()) return cudaErrorLaunchTimeout;
+        return e;
     }
     int devId = 0;
     cudaError_t e = cudaGetDevice(&devId);
@@ -159,6 +162,7 @@ cudaError_t run_channels(std::vector<ChannelBuf>& bufs, uint32_t channels, const
     }
     cudaError_t e0 = cudaStreamSynchronize(S->st[0]);
     cudaError_t e1 = cudaStreamSynchronize(S->st[1]);
+    if (e0 == cudaSuccess && e1 == cudaSuccess && take_device_error()) return cudaErrorLaunchTimeout;
     return e0 != cudaSuccess ? e0 : e1;
 }
 

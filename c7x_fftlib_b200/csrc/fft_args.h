@@ -17,7 +17,7 @@ constexpr int kMaxPasses = 8;
 
 // Magic multiplier for floor(j / d) = umulhi(j, m), m = floor(2^32 / d) + 1,
 // exact whenever j * d < 2^32 (all indices here are below 2^16).
-inline FFTB_HD uint32_t fastdiv_magic(uint32_t d)
+inline FFTB_HD constexpr uint32_t fastdiv_magic(uint32_t d)
 {
     return d <= 1u ? 0u : (uint32_t)((0x100000000ull / d) + 1ull);
 }
@@ -76,6 +76,8 @@ struct FftArgs {
     uint32_t slen;
     uint32_t inCount;
     uint32_t inMagic;            // fastdiv_magic(inCount)
+    // error word (host-visible); kernels with bounded waits report here
+    uint32_t* err;
 };
 
 } // namespace fftb200

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "fft_args.h"
 
 namespace fftb200 {
@@ -13,8 +15,25 @@ namespace fftb200 {
 // (complex values per thread) accepts; 0 if emax is not instantiated.
 int engine_max_threads(int emax);
 
-// Launch the FP32 Stockham engine described by a (grid = ceil(batch / M)).
+// Launch the FP32 Stockham engine described by a (grid = ceil(batch / M)):
+// a fixed-size kernel when one is compiled for exactly this schedule, else
+// the runtime-planned engine of width emax.
 cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s);
+
+// A compiled fixed-size schedule.
+struct StaticEntry {
+    uint32_t n;
+    int emax;
+    uint32_t T;
+    int P;
+    int R[kMaxPasses];
+    int maxThreads;
+    cudaError_t (*launch)(const FftArgs&, cudaStream_t);
+    // persistent TMA-pipelined variant (M == 1, contiguous 16-byte aligned
+    // rows, complex in and out), or null
+    cudaError_t (*launchPipelined)(const FftArgs&, cudaStream_t);
+};
+const std::vector<StaticEntry>& static_schedules();
 
 // W[i] = exp(-2 pi i (i mod n) / n), i < count, computed in FP64.
 cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s);

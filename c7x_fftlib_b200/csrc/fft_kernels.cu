@@ -50,9 +50,44 @@ int engine_max_threads(int emax)
     }
 }
 
+void register_static_a(std::vector<StaticEntry>& out);
+void register_static_b(std::vector<StaticEntry>& out);
+void register_static_c(std::vector<StaticEntry>& out);
+
+const std::vector<StaticEntry>& static_schedules()
+{
+    static const std::vector<StaticEntry> table = [] {
+        std::vector<StaticEntry> t;
+        register_static_a(t);
+        register_static_b(t);
+        register_static_c(t);
+        return t;
+    }();
+    return table;
+}
+
+namespace {
+const StaticEntry* find_static(const FftArgs& a, int emax)
+{
+    for (const StaticEntry& e : static_schedules()) {
+        if (e.n != a.N || e.emax != emax || e.T != a.T || e.P != (int)a.P) continue;
+        bool same = true;
+        for (int p = 0; p < e.P; ++p) same = same && (e.R[p] == a.pass[p].R);
+        if (same && a.T * a.M <= (uint32_t)e.maxThreads) return &e;
+    }
+    return nullptr;
+}
+} // namespace
+
 cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
 {
     if (a.batch == 0) return cudaSuccess;
+    if (const StaticEntry* st = find_static(a, emax)) {
+        const bool pipelinable = st->launchPipelined && a.err && a.M == 1 && a.ioMode == IO_C2C && !a.staged &&
+                                 !a.batchMinor && !a.twBig && a.inElem == 1 && a.outElem == 1 &&
+                                 a.inBatch == (int64_t)a.N && ((uintptr_t)a.in & 15u) == 0 && (a.N % 2u) == 0;
+        return pipelinable ? st->launchPipelined(a, s) : st->launch(a, s);
+    }
     switch (emax) {
     case 8: return launch_generic<8, 1024>(a, s);
     case 16: return launch_generic<16, 512>(a, s);

@@ -1,0 +1,172 @@
+// fft_pipeline.cuh -- persistent, TMA-pipelined fixed-size FFT kernel.
+//
+// A CTA walks over tiles of M contiguous transforms (tile = blockIdx.x,
+// blockIdx.x + gridDim.x, ...). A ring of STAGES shared-memory tiles is fed
+// by bulk asynchronous copies (cp.async.bulk global->shared, completion on an
+// mbarrier): while the CTA runs the passes of tile i out of one stage, the
+// copies for the next tiles are already in flight, so HBM reads never wait
+// for compute. The first pass reads its inputs straight from the stage, the
+// intermediate passes exchange through a padded shared-memory buffer and the
+// last pass stores to HBM from registers.
+//
+// Every wait is bounded (iteration and wall-clock limits). A wait that gives
+// up sets bit kErrPipelineTimeout in the launch's error word, drains the
+// copies still in flight (again bounded) and ends the CTA; the host reports
+// the error word after synchronizing.
+#pragma once
+
+#include "fft_stockham.cuh"
+
+namespace fftb200 {
+
+constexpr uint32_t kErrPipelineTimeout = 1u;
+
+FFT_DEV uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+FFT_DEV void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+FFT_DEV void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+FFT_DEV bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n"
+        "  .reg .pred p;\n"
+        "  mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "  selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+FFT_DEV uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for phase `parity` of bar: gives up after 2^22 polls or one
+// second, whichever comes first.
+FFT_DEV bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 0; i < (1u << 22); ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 255u) == 255u && global_ns() - t0 > 1000000000ull) return false;
+    }
+    return false;
+}
+
+FFT_DEV void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+FFT_DEV void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+FFT_DEV void fence_mbarrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Shared-memory bytes of the pipelined kernel for M transforms per tile.
+__host__ __device__ constexpr size_t pipe_smem_bytes(uint32_t n, uint32_t m, int stages)
+{
+    return (size_t)stages * m * n * 8u + (((size_t)m * smem_len(n) * 8u + 15u) & ~(size_t)15u) + 8u * (size_t)stages +
+           16u;
+}
+
+template <class S, int STAGES>
+FFT_DEV void fft_pipeline(const FftArgs& a)
+{
+    static_assert(S::P >= 2, "the pipelined kernel refills its stage between passes 0 and 1");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    constexpr uint32_t N = (uint32_t)S::N;
+    const uint32_t M = a.M;
+    const uint32_t tileElems = M * N;
+    float2* stages = (float2*)smem_raw;
+    float2* xch = stages + (size_t)STAGES * tileElems;
+    uint64_t* bar = (uint64_t*)((unsigned char*)xch + (((size_t)M * smem_len(N) * 8u + 15u) & ~(size_t)15u));
+    __shared__ uint32_t s_fail;
+
+    const uint32_t tid = threadIdx.x;
+    uint32_t m, t;
+    lane_of(a, (uint32_t)S::T, &m, &t);
+    const uint32_t tiles = (a.batch + M - 1) / M;
+    const uint32_t G = gridDim.x;
+
+    auto issue = [&](uint32_t tile, int s) {
+        const uint32_t b0 = tile * M;
+        const uint32_t nm = min(M, a.batch - b0);
+        const uint32_t bytes = nm * N * 8u;
+        mbar_expect_tx(&bar[s], bytes);
+        bulk_copy_g2s(stages + (size_t)s * tileElems, a.in + (size_t)b0 * N, bytes, &bar[s]);
+    };
+
+    if (tid == 0) {
+        s_fail = 0;
+        for (int s = 0; s < STAGES; ++s) mbar_init(&bar[s], 1);
+        fence_mbarrier_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            const uint32_t tile = blockIdx.x + (uint32_t)s * G;
+            if (tile < tiles) issue(tile, s);
+        }
+    }
+
+    float2 v[S::EMAX];
+    uint32_t it = 0;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += G, ++it) {
+        const int s = (int)(it % STAGES);
+        const uint32_t parity = (it / STAGES) & 1u;
+        if (!mbar_wait_bounded(&bar[s], parity)) atomicOr(&s_fail, 1u);
+        __syncthreads();
+        if (s_fail) break;
+
+        const uint32_t b = tile * M + m;
+        const bool active = b < a.batch;
+        const float2* raw = stages + (size_t)s * tileElems + (size_t)m * N;
+        float2* sm = xch + (size_t)m * smem_len(N);
+        static_for<S::P>([&](auto p) {
+            constexpr int P = decltype(p)::value;
+            constexpr PassInfo pi = S::pass(P);
+            if constexpr (P == 1) {
+                // every thread has read the stage (pass 0 ended with two
+                // barriers): refill it with the tile STAGES ahead
+                if (tid == 0) {
+                    fence_proxy_async_smem();
+                    const uint32_t next = tile + (uint32_t)STAGES * G;
+                    if (next < tiles) issue(next, s);
+                }
+            }
+            run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, b, active,
+                                       P == 0 ? raw : nullptr);
+        });
+    }
+
+    if (s_fail) {
+        if (tid == 0) {
+            *(volatile uint32_t*)a.err = kErrPipelineTimeout;
+            // drain the copies still in flight for the tiles after the failed one
+            for (int k = 0; k < STAGES; ++k) {
+                const uint32_t itk = it + (uint32_t)k;
+                const uint32_t tile = blockIdx.x + itk * G;
+                if (tile < tiles) mbar_wait_bounded(&bar[itk % STAGES], (itk / STAGES) & 1u);
+            }
+        }
+    }
+}
+
+} // namespace fftb200

@@ -1,0 +1,14 @@
+// Fixed-size FFT kernels (see fft_static_impl.cuh).
+#include "fft_static_impl.cuh"
+
+namespace fftb200 {
+
+void register_static_a(std::vector<StaticEntry>& out)
+{
+    out.push_back(static_entry<StaticSchedule<4096, 16, 256, 16, 16, 16>>());
+    out.push_back(static_entry<StaticSchedule<2048, 16, 128, 16, 16, 8>>());
+    out.push_back(static_entry<StaticSchedule<1024, 32, 32, 32, 32>>());
+    out.push_back(static_entry<StaticSchedule<256, 16, 16, 16, 16>>());
+}
+
+} // namespace fftb200

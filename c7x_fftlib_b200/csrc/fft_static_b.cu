@@ -1,0 +1,17 @@
+// Fixed-size FFT kernels (see fft_static_impl.cuh).
+#include "fft_static_impl.cuh"
+
+namespace fftb200 {
+
+void register_static_b(std::vector<StaticEntry>& out)
+{
+    out.push_back(static_entry<StaticSchedule<8192, 32, 256, 32, 32, 8>>());
+    out.push_back(static_entry<StaticSchedule<16384, 32, 512, 32, 32, 16>>());
+    out.push_back(static_entry<StaticSchedule<512, 32, 16, 32, 16>>());
+    out.push_back(static_entry<StaticSchedule<128, 16, 8, 16, 8>>());
+    out.push_back(static_entry<StaticSchedule<64, 8, 8, 8, 8>>());
+    out.push_back(static_entry<StaticSchedule<32, 32, 1, 32>>());
+    out.push_back(static_entry<StaticSchedule<16, 16, 1, 16>>());
+}
+
+} // namespace fftb200

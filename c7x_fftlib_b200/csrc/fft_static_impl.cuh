@@ -1,0 +1,110 @@
+// fft_static_impl.cuh -- fixed-size FFT kernels: the engine of
+// fft_stockham.cuh with the whole schedule (length, radices, threads per
+// transform, twiddle offsets) known at compile time, so every index and loop
+// bound folds to constants. Each fft_static_*.cu instantiates a few
+// schedules and registers them; launch_fft() prefers a registered fixed-size
+// kernel when the planner's schedule matches one.
+#pragma once
+
+#include <algorithm>
+#include <mutex>
+
+#include "fft_engine.h"
+#include "fft_pipeline.cuh"
+#include "fft_stockham.cuh"
+
+namespace fftb200 {
+
+template <class S, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_fft_static(const __grid_constant__ FftArgs a)
+{
+    extern __shared__ __align__(16) float2 smem[];
+    fft_tile_static<S>(a, smem, blockIdx.x * a.M);
+}
+
+template <class S, int MAXT>
+cudaError_t launch_static(const FftArgs& a, cudaStream_t s)
+{
+    const size_t smem = (size_t)a.M * a.slen * sizeof(float2);
+    if (a.T != (uint32_t)S::T || a.T * a.M > (uint32_t)MAXT) return cudaErrorInvalidConfiguration;
+    if (smem > 48u * 1024u) {
+        static std::mutex mu;
+        static size_t configured[64] = {};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev >= 64 || configured[dev] < smem) {
+            e = cudaFuncSetAttribute(k_fft_static<S, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            if (dev < 64) configured[dev] = smem;
+        }
+    }
+    const uint32_t grid = (a.batch + a.M - 1) / a.M;
+    k_fft_static<S, MAXT><<<grid, a.T * a.M, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S, int STAGES>
+__global__ void __launch_bounds__(S::T) k_fft_pipe(const __grid_constant__ FftArgs a)
+{
+    fft_pipeline<S, STAGES>(a);
+}
+
+// Persistent pipelined launch: one CTA per (SM x resident CTAs), M = 1 or a
+// whole number of transforms per tile.
+template <class S, int STAGES>
+cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
+{
+    if (a.T * a.M != (uint32_t)S::T && a.M != 1) return cudaErrorInvalidConfiguration;
+    const size_t smem = pipe_smem_bytes((uint32_t)S::N, a.M, STAGES);
+    struct Cfg {
+        size_t smem = 0;
+        int blocks = 0;
+    };
+    static std::mutex mu;
+    static Cfg cfg[64];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    int resident = 0, sms = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        Cfg& c = cfg[dev & 63];
+        if (c.smem != smem) {
+            e = cudaFuncSetAttribute(k_fft_pipe<S, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.blocks, k_fft_pipe<S, STAGES>, S::T, smem);
+            if (e != cudaSuccess) return e;
+            c.smem = smem;
+        }
+        resident = c.blocks;
+    }
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const uint32_t tiles = (a.batch + a.M - 1) / a.M;
+    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)std::max(1, resident * sms));
+    k_fft_pipe<S, STAGES><<<grid, S::T, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S>
+StaticEntry static_entry()
+{
+    StaticEntry e{};
+    e.n = (uint32_t)S::N;
+    e.emax = S::EMAX;
+    e.T = (uint32_t)S::T;
+    e.P = S::P;
+    for (int i = 0; i < S::P; ++i) e.R[i] = S::R[i];
+    constexpr int maxt = S::T > 256 ? S::T : 256;
+    e.maxThreads = maxt;
+    e.launch = &launch_static<S, maxt>;
+    if constexpr (S::P >= 2 && S::T >= 64 && (S::N % 2) == 0) {
+        e.launchPipelined = &launch_pipe<S, 2>;
+    } else {
+        e.launchPipelined = nullptr;
+    }
+    return e;
+}
+
+} // namespace fftb200

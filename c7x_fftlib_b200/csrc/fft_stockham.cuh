@@ -88,15 +88,17 @@ FFT_DEV float2 finish(const FftArgs& a, float2 z)
     return cscale(z, a.scale);
 }
 
+// One pass. pi, first, last and T are either runtime values (the generic
+// engine) or compile-time constants (the fixed-size kernels), in which case
+// all index arithmetic folds away after inlining.
+// raw: when not null, the first pass reads its input from this unpadded
+// shared-memory copy of the transform (filled by a bulk async copy).
 template <int EMAX, int R>
-FFT_DEV void run_pass(const FftArgs& a, int p, float2 (&v)[EMAX], float2* sm,
-                      uint32_t t, uint32_t b, bool active)
+FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, const bool last,
+                      const uint32_t T, float2 (&v)[EMAX], float2* sm, uint32_t t, uint32_t b, bool active,
+                      const float2* raw = nullptr)
 {
     constexpr int BMAX = EMAX / R;
-    const PassInfo pi = a.pass[p];
-    const bool first = (p == 0);
-    const bool last = (p + 1 == (int)a.P);
-    const uint32_t T = a.T;
     const uint32_t nb = pi.stride; // butterflies in this pass: N / R
 
     // gather
@@ -106,7 +108,10 @@ FFT_DEV void run_pass(const FftArgs& a, int p, float2 (&v)[EMAX], float2* sm,
             static_for<R>([&](auto q) {
                 const uint32_t idx = j + (uint32_t)q * nb;
                 float2 z;
-                if (first) {
+                if (first && raw) {
+                    z = raw[idx];
+                    if (a.conjIn) z = cconj(z);
+                } else if (first) {
                     z = (active || a.staged) ? load_in(a, b, idx, sm) : make_float2(0.f, 0.f);
                 } else {
                     z = sm[smem_swz(idx)];
@@ -153,7 +158,7 @@ FFT_DEV void run_pass(const FftArgs& a, int p, float2 (&v)[EMAX], float2* sm,
         }
         return;
     }
-    if (!first || a.staged) __syncthreads(); // every read of this pass is done
+    if (!first || a.staged || raw) __syncthreads(); // every read of this pass is done
     static_for<BMAX>([&](auto i) {
         const uint32_t j = t + (uint32_t)i * T;
         if (j < nb) {
@@ -230,19 +235,26 @@ FFT_DEV void stage_out(const FftArgs& a, const float2* smem, uint32_t b0)
     }
 }
 
-// Whole-transform body for the CTA's transforms b0 .. b0+M-1.
+// Thread -> (transform m, lane t) mapping of a CTA.
+FFT_DEV void lane_of(const FftArgs& a, uint32_t T, uint32_t* m, uint32_t* t)
+{
+    const uint32_t tid = threadIdx.x;
+    if (a.batchMinor) {
+        *t = tid / a.M;
+        *m = tid - *t * a.M;
+    } else {
+        *m = tid / T;
+        *t = tid - *m * T;
+    }
+}
+
+// Whole-transform body for the CTA's transforms b0 .. b0+M-1 (schedule read
+// from a.pass at run time).
 template <int EMAX>
 FFT_DEV void fft_tile(const FftArgs& a, float2* smem, uint32_t b0)
 {
-    const uint32_t tid = threadIdx.x;
     uint32_t m, t;
-    if (a.batchMinor) {
-        t = tid / a.M;
-        m = tid - t * a.M;
-    } else {
-        m = tid / a.T;
-        t = tid - m * a.T;
-    }
+    lane_of(a, a.T, &m, &t);
     const uint32_t b = b0 + m;
     const bool active = b < a.batch;
     float2* sm = smem + m * a.slen;
@@ -254,9 +266,58 @@ FFT_DEV void fft_tile(const FftArgs& a, float2* smem, uint32_t b0)
     float2 v[EMAX];
     for (int p = 0; p < (int)a.P; ++p) {
         dispatch_radix<EMAX>(a.pass[p].R, [&](auto r) {
-            run_pass<EMAX, decltype(r)::value>(a, p, v, sm, t, b, active);
+            run_pass<EMAX, decltype(r)::value>(a, a.pass[p], p == 0, p + 1 == (int)a.P, a.T, v, sm, t, b, active);
         });
     }
+    if (a.ioMode == IO_R2C_SPLIT) {
+        r2c_epilogue(a, sm, t, b, active);
+    } else if (a.staged) {
+        stage_out(a, smem, b0);
+    }
+}
+
+// Compile-time schedule: length N, register capacity EMAX, T threads per
+// transform, pass radices Rs... (the same pass layout and twiddle-table
+// layout as the runtime planner produces).
+template <int N_, int EMAX_, int T_, int... Rs>
+struct StaticSchedule {
+    static constexpr int N = N_, EMAX = EMAX_, T = T_, P = sizeof...(Rs);
+    static constexpr int R[P] = {Rs...};
+    static constexpr PassInfo pass(int p)
+    {
+        uint32_t ns = 1, off = 0;
+        for (int i = 0; i < p; ++i) {
+            if (i > 0) off += (uint32_t)(R[i] - 1) * ns;
+            ns *= (uint32_t)R[i];
+        }
+        PassInfo pi{};
+        pi.R = R[p];
+        pi.Ns = ns;
+        pi.nsMagic = fastdiv_magic(ns);
+        pi.stride = (uint32_t)(N / R[p]);
+        pi.twOffset = off;
+        return pi;
+    }
+};
+
+template <class S>
+FFT_DEV void fft_tile_static(const FftArgs& a, float2* smem, uint32_t b0)
+{
+    uint32_t m, t;
+    lane_of(a, (uint32_t)S::T, &m, &t);
+    const uint32_t b = b0 + m;
+    const bool active = b < a.batch;
+    float2* sm = smem + m * a.slen;
+    if (a.staged) {
+        stage_in(a, smem, b0);
+        __syncthreads();
+    }
+    float2 v[S::EMAX];
+    static_for<S::P>([&](auto p) {
+        constexpr int P = decltype(p)::value;
+        constexpr PassInfo pi = S::pass(P);
+        run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, b, active);
+    });
     if (a.ioMode == IO_R2C_SPLIT) {
         r2c_epilogue(a, sm, t, b, active);
     } else if (a.staged) {

@@ -123,9 +123,49 @@ std::string describe(const EnginePlan& e)
     return os.str();
 }
 
+const ErrorWord& error_word()
+{
+    static std::mutex mu;
+    static ErrorWord words[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        static ErrorWord none;
+        return none;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    ErrorWord& w = words[dev];
+    if (!w.dev) {
+        void* h = nullptr;
+        if (cudaHostAlloc(&h, sizeof(uint32_t), cudaHostAllocMapped) == cudaSuccess) {
+            *(volatile uint32_t*)h = 0;
+            void* d = nullptr;
+            if (cudaHostGetDevicePointer(&d, h, 0) == cudaSuccess) {
+                w.host = (volatile uint32_t*)h;
+                w.dev = (uint32_t*)d;
+            } else {
+                cudaFreeHost(h);
+                cudaGetLastError();
+            }
+        } else {
+            cudaGetLastError();
+        }
+    }
+    return w;
+}
+
+uint32_t take_device_error()
+{
+    const ErrorWord& w = error_word();
+    if (!w.host) return 0;
+    const uint32_t v = *w.host;
+    if (v) *w.host = 0;
+    return v;
+}
+
 FftArgs engine_args(const EnginePlan& e, const float2* tw)
 {
     FftArgs a{};
+    a.err = error_word().dev;
     a.tw = tw;
     a.N = e.n;
     a.T = e.T;
@@ -157,7 +197,8 @@ void finalize_launch(FftArgs& a, const EnginePlan& e, bool contiguousIn, bool co
     if (a.batchMinor) {
         M = std::max(1u, std::min(16u, maxT / e.T));
     } else {
-        M = e.T >= 256u ? 1u : 256u / e.T;
+        // T >= 128: one transform per CTA (the pipelined kernels' shape)
+        M = e.T >= 128u ? 1u : 256u / e.T;
         M = std::max(1u, std::min(M, maxT / e.T));
     }
     const uint32_t bytesPer = a.slen * (uint32_t)sizeof(float2);

@@ -52,6 +52,16 @@ struct ComplexPlan {
     float2* twSplit = nullptr;       // W_{2n}^i, i < n (real-input kernels)
 };
 
+// Host-visible error word of the current device (mapped pinned memory):
+// kernels with bounded waits write a nonzero code there instead of hanging.
+struct ErrorWord {
+    volatile uint32_t* host = nullptr;
+    uint32_t* dev = nullptr;
+};
+const ErrorWord& error_word();
+// Returns the word's value and clears it.
+uint32_t take_device_error();
+
 // Cached per (current device, n). needSplit also creates twSplit.
 // Returns nullptr (and sets *err) if n is not 2^a 3^b 5^c or on CUDA errors.
 ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err);

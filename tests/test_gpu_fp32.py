@@ -72,6 +72,17 @@ def test_c2c_vs_reference_cn(gpu, ref_cn, n, ch, inverse):
     assert O.rel_l2(y, O.fp64_c2c(x, n, ch, inverse)) <= REL_L2
 
 
+@pytest.mark.parametrize("n,ch", [(4096, 1), (4096, 297), (4096, 1000), (2048, 593), (8192, 300), (16384, 150),
+                                  (1024, 777), (960, 301)])
+def test_c2c_batch_counts(gpu, n, ch):
+    """Batch counts below, around and above the number of persistent CTAs
+    (148 SMs x resident CTAs) exercise the pipelined kernels' tile loop."""
+    x = O.uniform_c2c(n, ch, seed=n + ch)
+    for inverse in (False, True):
+        y = fftcall.c2c(x, n, ch, inverse=inverse)
+        assert O.rel_l2(y, O.fp64_c2c(x, n, ch, inverse)) <= REL_L2
+
+
 def test_c2c_golden_ref_cn(gpu):
     d = np.load(os.path.join(GOLD, "ref_cn.npz"))
     for i in range(int(d["c2c_n"])):
