@@ -13,7 +13,7 @@
 namespace fftb200 {
 
 namespace {
-thread_local std::string t_error;
+thread_local char t_error[512];
 constexpr size_t kChunkBytes = 32u << 20; // staged bytes per chunk (all host buffers)
 constexpr size_t kAlign = 256;
 
@@ -57,15 +57,13 @@ cudaError_t ensure(Staging& S, int slot, size_t bytes)
 
 void set_error(const char* fmt, ...)
 {
-    char buf[512];
     va_list ap;
     va_start(ap, fmt);
-    vsnprintf(buf, sizeof(buf), fmt, ap);
+    vsnprintf(t_error, sizeof(t_error), fmt, ap);
     va_end(ap);
-    t_error = buf;
 }
 
-const char* last_error() { return t_error.c_str(); }
+const char* last_error() { return t_error; }
 
 FFTLIB_STATUS cuda_fail(cudaError_t e, const char* what)
 {

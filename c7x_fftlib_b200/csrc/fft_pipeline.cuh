@@ -79,38 +79,49 @@ FFT_DEV void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t*
 FFT_DEV void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 FFT_DEV void fence_mbarrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
-// Shared-memory bytes of the pipelined kernel for M transforms per tile.
-__host__ __device__ constexpr size_t pipe_smem_bytes(uint32_t n, uint32_t m, int stages)
+// Stage length in complex values: the padded exchange layout of one
+// transform, rounded to an even count so every stage starts 16-byte aligned.
+__host__ __device__ constexpr uint32_t pipe_stage_len(uint32_t n) { return (smem_len(n) + 1u) & ~1u; }
+
+// Shared-memory bytes of the pipelined kernel (one transform per tile).
+__host__ __device__ constexpr size_t pipe_smem_bytes(uint32_t n, int stages)
 {
-    return (size_t)stages * m * n * 8u + (((size_t)m * smem_len(n) * 8u + 15u) & ~(size_t)15u) + 8u * (size_t)stages +
-           16u;
+    return (size_t)stages * pipe_stage_len(n) * 8u + 8u * (size_t)stages + 16u;
 }
 
+// CTAs per SM the kernel is compiled for: as many as the shared memory
+// (228 KB per SM, 1 KB reserved per CTA) and 2048 threads allow, at most 4.
+__host__ __device__ constexpr int pipe_min_blocks(uint32_t n, int t, int stages)
+{
+    const int bySmem = (int)((228u * 1024u) / (pipe_smem_bytes(n, stages) + 1024u));
+    const int byThreads = 2048 / t;
+    const int b = bySmem < byThreads ? bySmem : byThreads;
+    return b < 1 ? 1 : (b > 4 ? 4 : b);
+}
+
+// The transform is exchanged in place in its own stage: the bulk copy lands
+// the input unpadded at the start of the stage, the first pass reads it from
+// there and (after a barrier) writes its outputs back in the padded layout,
+// and so on; the stage is refilled once the last pass has read it.
 template <class S, int STAGES>
 FFT_DEV void fft_pipeline(const FftArgs& a)
 {
-    static_assert(S::P >= 2, "the pipelined kernel refills its stage between passes 0 and 1");
+    static_assert(S::P >= 2, "the pipelined kernel needs at least two passes");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr uint32_t N = (uint32_t)S::N;
-    const uint32_t M = a.M;
-    const uint32_t tileElems = M * N;
+    constexpr uint32_t SL = pipe_stage_len(N);
     float2* stages = (float2*)smem_raw;
-    float2* xch = stages + (size_t)STAGES * tileElems;
-    uint64_t* bar = (uint64_t*)((unsigned char*)xch + (((size_t)M * smem_len(N) * 8u + 15u) & ~(size_t)15u));
+    uint64_t* bar = (uint64_t*)(stages + (size_t)STAGES * SL);
     __shared__ uint32_t s_fail;
 
     const uint32_t tid = threadIdx.x;
-    uint32_t m, t;
-    lane_of(a, (uint32_t)S::T, &m, &t);
-    const uint32_t tiles = (a.batch + M - 1) / M;
+    const uint32_t t = tid;
+    const uint32_t tiles = a.batch;
     const uint32_t G = gridDim.x;
 
     auto issue = [&](uint32_t tile, int s) {
-        const uint32_t b0 = tile * M;
-        const uint32_t nm = min(M, a.batch - b0);
-        const uint32_t bytes = nm * N * 8u;
-        mbar_expect_tx(&bar[s], bytes);
-        bulk_copy_g2s(stages + (size_t)s * tileElems, a.in + (size_t)b0 * N, bytes, &bar[s]);
+        mbar_expect_tx(&bar[s], N * 8u);
+        bulk_copy_g2s(stages + (size_t)s * SL, a.in + (size_t)tile * N, N * 8u, &bar[s]);
     };
 
     if (tid == 0) {
@@ -130,41 +141,36 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
     uint32_t it = 0;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += G, ++it) {
         const int s = (int)(it % STAGES);
-        const uint32_t parity = (it / STAGES) & 1u;
-        if (!mbar_wait_bounded(&bar[s], parity)) atomicOr(&s_fail, 1u);
+        if (it > 0) {
+            // every thread has finished the previous transform: refill its
+            // stage with the tile STAGES iterations after it
+            __syncthreads();
+            if (tid == 0) {
+                fence_proxy_async_smem();
+                const uint32_t next = tile - G + (uint32_t)STAGES * G;
+                if (next < tiles) issue(next, (int)((it - 1) % STAGES));
+            }
+        }
+        if (!mbar_wait_bounded(&bar[s], (it / STAGES) & 1u)) atomicOr(&s_fail, 1u);
         __syncthreads();
         if (s_fail) break;
 
-        const uint32_t b = tile * M + m;
-        const bool active = b < a.batch;
-        const float2* raw = stages + (size_t)s * tileElems + (size_t)m * N;
-        float2* sm = xch + (size_t)m * smem_len(N);
+        float2* st = stages + (size_t)s * SL;
         static_for<S::P>([&](auto p) {
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
-            if constexpr (P == 1) {
-                // every thread has read the stage (pass 0 ended with two
-                // barriers): refill it with the tile STAGES ahead
-                if (tid == 0) {
-                    fence_proxy_async_smem();
-                    const uint32_t next = tile + (uint32_t)STAGES * G;
-                    if (next < tiles) issue(next, s);
-                }
-            }
-            run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, b, active,
-                                       P == 0 ? raw : nullptr);
+            run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true,
+                                       P == 0 ? st : nullptr);
         });
     }
 
-    if (s_fail) {
-        if (tid == 0) {
-            *(volatile uint32_t*)a.err = kErrPipelineTimeout;
-            // drain the copies still in flight for the tiles after the failed one
-            for (int k = 0; k < STAGES; ++k) {
-                const uint32_t itk = it + (uint32_t)k;
-                const uint32_t tile = blockIdx.x + itk * G;
-                if (tile < tiles) mbar_wait_bounded(&bar[itk % STAGES], (itk / STAGES) & 1u);
-            }
+    if (s_fail && tid == 0) {
+        *(volatile uint32_t*)a.err = kErrPipelineTimeout;
+        // drain every copy still in flight (bounded)
+        for (int k = 0; k < STAGES; ++k) {
+            const uint32_t itk = it + (uint32_t)k;
+            const uint32_t tile = blockIdx.x + itk * G;
+            if (tile < tiles) mbar_wait_bounded(&bar[itk % STAGES], (itk / STAGES) & 1u);
         }
     }
 }

@@ -46,21 +46,21 @@ cudaError_t launch_static(const FftArgs& a, cudaStream_t s)
 }
 
 template <class S, int STAGES>
-__global__ void __launch_bounds__(S::T) k_fft_pipe(const __grid_constant__ FftArgs a)
+__global__ void __launch_bounds__(S::T, pipe_min_blocks(S::N, S::T, STAGES)) k_fft_pipe(const __grid_constant__ FftArgs a)
 {
     fft_pipeline<S, STAGES>(a);
 }
 
-// Persistent pipelined launch: one CTA per (SM x resident CTAs), M = 1 or a
-// whole number of transforms per tile.
+// Persistent pipelined launch (one transform per tile): as many CTAs as are
+// resident on the device.
 template <class S, int STAGES>
 cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
 {
-    if (a.T * a.M != (uint32_t)S::T && a.M != 1) return cudaErrorInvalidConfiguration;
-    const size_t smem = pipe_smem_bytes((uint32_t)S::N, a.M, STAGES);
+    if (a.M != 1 || a.T != (uint32_t)S::T) return cudaErrorInvalidConfiguration;
+    const size_t smem = pipe_smem_bytes((uint32_t)S::N, STAGES);
     struct Cfg {
-        size_t smem = 0;
-        int blocks = 0;
+        int blocks = -1;
+        int sms = 0;
     };
     static std::mutex mu;
     static Cfg cfg[64];
@@ -71,18 +71,18 @@ cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
     {
         std::lock_guard<std::mutex> lock(mu);
         Cfg& c = cfg[dev & 63];
-        if (c.smem != smem) {
+        if (c.blocks < 0) {
             e = cudaFuncSetAttribute(k_fft_pipe<S, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.blocks, k_fft_pipe<S, STAGES>, S::T, smem);
             if (e != cudaSuccess) return e;
-            c.smem = smem;
+            e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess) return e;
         }
         resident = c.blocks;
+        sms = c.sms;
     }
-    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    const uint32_t tiles = (a.batch + a.M - 1) / a.M;
-    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)std::max(1, resident * sms));
+    const uint32_t grid = std::min<uint32_t>(a.batch, (uint32_t)std::max(1, resident * sms));
     k_fft_pipe<S, STAGES><<<grid, S::T, smem, s>>>(a);
     return cudaGetLastError();
 }
@@ -99,7 +99,8 @@ StaticEntry static_entry()
     constexpr int maxt = S::T > 256 ? S::T : 256;
     e.maxThreads = maxt;
     e.launch = &launch_static<S, maxt>;
-    if constexpr (S::P >= 2 && S::T >= 64 && (S::N % 2) == 0) {
+    // the stage ring and exchange buffer must fit one CTA's shared memory
+    if constexpr (S::P >= 2 && S::T >= 64 && (S::N % 2) == 0 && pipe_smem_bytes(S::N, 2) <= 227u * 1024u) {
         e.launchPipelined = &launch_pipe<S, 2>;
     } else {
         e.launchPipelined = nullptr;

@@ -48,20 +48,22 @@ void enumerate(uint32_t rem, int maxIdx, std::vector<int>& cur, std::vector<std:
 
 // Score a radix sequence on an engine width: each pass is one shared-memory
 // round trip; idle butterfly slots and wider register files cost extra.
-bool evaluate(uint32_t n, const std::vector<int>& seq, int emax, EnginePlan* e)
+bool evaluate(uint32_t n, const int* seq, int len, int emax, EnginePlan* e)
 {
     const int maxT = engine_max_threads(emax);
+    if (len > kMaxPasses) return false;
     uint32_t T = 1;
-    for (int r : seq) {
+    for (int i = 0; i < len; ++i) {
+        const int r = seq[i];
         if (r > emax || r < min_radix(emax)) return false;
         const uint32_t nb = n / (uint32_t)r;
         const uint32_t bmax = (uint32_t)(emax / r);
         T = std::max(T, (nb + bmax - 1) / bmax);
     }
-    if ((int)T > maxT || seq.size() > (size_t)kMaxPasses) return false;
+    if ((int)T > maxT) return false;
     double score = 0.0;
-    for (int r : seq) {
-        const uint32_t nb = n / (uint32_t)r;
+    for (int i = 0; i < len; ++i) {
+        const uint32_t nb = n / (uint32_t)seq[i];
         const uint32_t b = (nb + T - 1) / T;
         const double util = (double)nb / (double)(T * b);
         score += 1.0 + 0.5 * (1.0 / util - 1.0);
@@ -70,8 +72,8 @@ bool evaluate(uint32_t n, const std::vector<int>& seq, int emax, EnginePlan* e)
     e->n = n;
     e->emax = emax;
     e->T = T;
-    e->P = (int)seq.size();
-    for (size_t i = 0; i < seq.size(); ++i) e->R[i] = seq[i];
+    e->P = len;
+    for (int i = 0; i < len; ++i) e->R[i] = seq[i];
     e->score = score;
     return true;
 }
@@ -98,7 +100,7 @@ std::vector<EnginePlan> engine_candidates(uint32_t n)
     for (const auto& s : seqs) {
         for (int emax : kEmax) {
             EnginePlan e;
-            if (evaluate(n, s, emax, &e)) out.push_back(e);
+            if (evaluate(n, s.data(), (int)s.size(), emax, &e)) out.push_back(e);
         }
     }
     std::stable_sort(out.begin(), out.end(),
@@ -106,13 +108,52 @@ std::vector<EnginePlan> engine_candidates(uint32_t n)
     return out;
 }
 
+namespace {
+
+// Depth-first search over non-increasing radix sequences, keeping only the
+// best schedule (no heap allocation).
+void search_best(uint32_t n, uint32_t rem, int maxIdx, int* seq, int len, EnginePlan* best, bool* found)
+{
+    if (rem == 1u) {
+        for (int emax : kEmax) {
+            EnginePlan e;
+            if (evaluate(n, seq, len, emax, &e) && (!*found || e.score < best->score)) {
+                *best = e;
+                *found = true;
+            }
+        }
+        return;
+    }
+    if (len >= kMaxPasses) return;
+    for (int i = maxIdx; i < (int)(sizeof(kRadices) / sizeof(int)); ++i) {
+        const int r = kRadices[i];
+        if (rem % (uint32_t)r) continue;
+        seq[len] = r;
+        search_best(n, rem / (uint32_t)r, i, seq, len + 1, best, found);
+    }
+}
+
+} // namespace
+
 bool plan_engine(uint32_t n, EnginePlan* out)
 {
-    if (n > kMaxSingleN) return false;
-    auto c = engine_candidates(n);
-    if (c.empty()) return false;
-    *out = c.front();
-    return true;
+    if (n == 0 || n > kMaxSingleN || !is_235(n)) return false;
+    if (n == 1u) {
+        EnginePlan e;
+        e.n = 1;
+        e.emax = 8;
+        e.T = 1;
+        e.P = 1;
+        e.R[0] = 1;
+        *out = e;
+        return true;
+    }
+    int seq[kMaxPasses];
+    bool found = false;
+    EnginePlan best;
+    search_best(n, n, 0, seq, 0, &best, &found);
+    if (found) *out = best;
+    return found;
 }
 
 std::string describe(const EnginePlan& e)
@@ -165,7 +206,6 @@ uint32_t take_device_error()
 FftArgs engine_args(const EnginePlan& e, const float2* tw)
 {
     FftArgs a{};
-    a.err = error_word().dev;
     a.tw = tw;
     a.N = e.n;
     a.T = e.T;
@@ -354,6 +394,7 @@ cudaError_t run_four_step(const ComplexPlan* p, float2* in, float2* out, uint32_
         float2* x = in + (size_t)c * n;
         float2* y = out + (size_t)c * n;
         FftArgs a = engine_args(p->eng1, p->tw1);
+        a.err = error_word().dev;
         a.in = x;
         a.out = x;
         a.batch = n2;
@@ -370,6 +411,7 @@ cudaError_t run_four_step(const ComplexPlan* p, float2* in, float2* out, uint32_
         if (e != cudaSuccess) return e;
 
         FftArgs b = engine_args(p->eng2, p->tw2);
+        b.err = error_word().dev;
         b.in = x;
         b.out = y;
         b.batch = n1;
@@ -394,6 +436,7 @@ cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batc
     if (p->fourStep) return run_four_step(p, in, out, batch, inverse, s);
     const uint32_t n = p->n;
     FftArgs a = engine_args(p->eng, p->tw);
+    a.err = error_word().dev;
     a.in = in;
     a.out = out;
     a.batch = batch;
@@ -419,6 +462,7 @@ cudaError_t run_r2c(const ComplexPlan* p, float* x, float2* scratch, float2* y, 
         return launch_r2c_post(scratch, y, p->twSplit, h, batch, outmode, s);
     }
     FftArgs a = engine_args(p->eng, p->tw);
+    a.err = error_word().dev;
     a.in = (const float2*)x;
     a.out = y;
     a.batch = batch;
@@ -446,6 +490,7 @@ cudaError_t run_c2r(const ComplexPlan* p, const float2* x, float2* scratch, floa
         return run_four_step(p, scratch, (float2*)y, batch, true, s);
     }
     FftArgs a = engine_args(p->eng, p->tw);
+    a.err = error_word().dev;
     a.in = x;
     a.out = (float2*)y;
     a.batch = batch;
