@@ -141,33 +141,40 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
     uint32_t it = 0;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += G, ++it) {
         const int s = (int)(it % STAGES);
-        if (it > 0) {
-            // every thread has finished the previous transform: refill its
-            // stage with the tile STAGES iterations after it
-            __syncthreads();
-            if (tid == 0) {
-                fence_proxy_async_smem();
-                const uint32_t next = tile - G + (uint32_t)STAGES * G;
-                if (next < tiles) issue(next, (int)((it - 1) % STAGES));
-            }
-        }
-        if (!mbar_wait_bounded(&bar[s], (it / STAGES) & 1u)) atomicOr(&s_fail, 1u);
+        // one thread waits for the stage; the barrier passes the data (and
+        // the outcome) on to the others
+        if (tid == 0 && !mbar_wait_bounded(&bar[s], (it / STAGES) & 1u)) s_fail = 1u;
         __syncthreads();
         if (s_fail) break;
 
         float2* st = stages + (size_t)s * SL;
+        // once every thread has read this transform's input (the barrier
+        // inside pass 0), the previous transform's stage is free: refill it
+        // with the tile STAGES-1 iterations ahead
+        auto refill = [&]() {
+            if (tid == 0 && it > 0) {
+                fence_proxy_async_smem();
+                const uint32_t next = tile + (uint32_t)(STAGES - 1) * G;
+                if (next < tiles) issue(next, (int)((it - 1) % STAGES));
+            }
+        };
         static_for<S::P>([&](auto p) {
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
-            run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true,
-                                       P == 0 ? st : nullptr);
+            if constexpr (P == 0) {
+                run_pass<S::EMAX, S::R[P]>(a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true, st,
+                                           refill);
+            } else {
+                run_pass<S::EMAX, S::R[P]>(a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true);
+            }
         });
     }
 
     if (s_fail && tid == 0) {
         *(volatile uint32_t*)a.err = kErrPipelineTimeout;
-        // drain every copy still in flight (bounded)
-        for (int k = 0; k < STAGES; ++k) {
+        // drain every copy still in flight (bounded): the failed one and the
+        // STAGES-2 issued after it
+        for (int k = 0; k + 1 < STAGES; ++k) {
             const uint32_t itk = it + (uint32_t)k;
             const uint32_t tile = blockIdx.x + itk * G;
             if (tile < tiles) mbar_wait_bounded(&bar[itk % STAGES], (itk / STAGES) & 1u);

@@ -91,12 +91,25 @@ FFT_DEV float2 finish(const FftArgs& a, float2 z)
 // One pass. pi, first, last and T are either runtime values (the generic
 // engine) or compile-time constants (the fixed-size kernels), in which case
 // all index arithmetic folds away after inlining.
+struct NoHook {
+    FFT_DEV void operator()() const {}
+};
+
+// Padded index of idx0 + q*step for q < R: when step is a multiple of 16 the
+// pad of every element equals the pad of idx0 plus q*step/16, so one padded
+// base serves the whole butterfly.
+FFT_DEV uint32_t swz_step(uint32_t swzBase, uint32_t idx0, uint32_t q, uint32_t step)
+{
+    return (step & 15u) == 0u ? swzBase + q * (step + (step >> 4)) : smem_swz(idx0 + q * step);
+}
+
 // raw: when not null, the first pass reads its input from this unpadded
 // shared-memory copy of the transform (filled by a bulk async copy).
-template <int EMAX, int R>
+// afterGather runs right after the barrier that ends the pass's reads.
+template <int EMAX, int R, class Hook = NoHook>
 FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, const bool last,
                       const uint32_t T, float2 (&v)[EMAX], float2* sm, uint32_t t, uint32_t b, bool active,
-                      const float2* raw = nullptr)
+                      const float2* raw = nullptr, Hook afterGather = Hook())
 {
     constexpr int BMAX = EMAX / R;
     const uint32_t nb = pi.stride; // butterflies in this pass: N / R
@@ -105,6 +118,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
     static_for<BMAX>([&](auto i) {
         const uint32_t j = t + (uint32_t)i * T;
         if (j < nb) {
+            const uint32_t sj = smem_swz(j);
             static_for<R>([&](auto q) {
                 const uint32_t idx = j + (uint32_t)q * nb;
                 float2 z;
@@ -114,7 +128,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
                 } else if (first) {
                     z = (active || a.staged) ? load_in(a, b, idx, sm) : make_float2(0.f, 0.f);
                 } else {
-                    z = sm[smem_swz(idx)];
+                    z = sm[swz_step(sj, j, (uint32_t)q, nb)];
                 }
                 v[i * R + q] = z;
             });
@@ -158,14 +172,23 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
         }
         return;
     }
-    if (!first || a.staged || raw) __syncthreads(); // every read of this pass is done
+    if (!first || a.staged || raw) {
+        __syncthreads(); // every read of this pass is done
+        afterGather();
+    }
     static_for<BMAX>([&](auto i) {
         const uint32_t j = t + (uint32_t)i * T;
         if (j < nb) {
             const uint32_t g = fastdiv(j, pi.Ns, pi.nsMagic);
             const uint32_t k = j - g * pi.Ns;
             const uint32_t base = g * pi.Ns * (uint32_t)R + k;
-            static_for<R>([&](auto q) { sm[smem_swz(base + (uint32_t)q * pi.Ns)] = v[i * R + q]; });
+            const uint32_t sb = smem_swz(base);
+            // Ns = 1 with R = 16: base is a multiple of 16 and q < 16 share its pad
+            const bool contiguous16 = pi.Ns == 1u && R == 16;
+            static_for<R>([&](auto q) {
+                const uint32_t d = contiguous16 ? sb + (uint32_t)q : swz_step(sb, base, (uint32_t)q, pi.Ns);
+                sm[d] = v[i * R + q];
+            });
         }
     });
     __syncthreads();
