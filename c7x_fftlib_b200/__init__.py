@@ -116,6 +116,8 @@ def lib() -> C.CDLL:
     L.FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32f_kernelAsync.argtypes = [_vp, _vp, _vp, _u32, _u32, _u8, _vp, _vp]
     L.FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync.argtypes = [_vp, _vp, _vp, _vp, _u32, _u32, _u32, _vp,
                                                                          _vp]
+    L.FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc.argtypes = [_vp, _vp, _u32, _u32, _vp]
+    L.FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc.restype = C.c_int
     L.FFTLIB_b200_tw_gen_c2c.argtypes = [_vp, _u32]
     L.FFTLIB_b200_tw_gen_i16.argtypes = [_vp, _u32]
     for fn in ("tw_gen_r2c", "split_factor_gen_r2c", "ifft_c2r_tw_gen", "ifft_c2r_split_factor_gen"):

@@ -55,6 +55,29 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync(int16_t *pX
                                                                      uint32_t numPoints, uint32_t numChannels,
                                                                      void *pBlock, void *stream);
 
+/* FP32 complex-to-complex forward FFT that allocates no memory.
+ * No counterpart in the reference library. For callers that cannot allocate
+ * at call time: code that runs under a device-memory budget fixed at start-up,
+ * real-time loops that must not enter an allocator, or hosts whose allocator
+ * belongs to another runtime. The regular _init/_kernel path allocates device
+ * memory for plan tables and staging; this call uses only one scratch array
+ * that is part of the library image (a static device array of 256 KiB + 256 B,
+ * held on every GPU that loads the library until the process exits), so it
+ * calls no cudaMalloc, cudaFree or other allocator.
+ * - pX, pY: device buffers, numChannels rows of numPoints interleaved complex
+ *   floats (the layout of FFTLIB_fft1dBatched_i32fc_c32fc_o32fc); pX is not
+ *   modified.
+ * - numPoints: 2^a 3^b 5^c, at most 16384 (longer or other lengths return
+ *   FFTLIB_ERR_INVALID_DIMENSION); stream: a cudaStream_t (NULL = legacy
+ *   default stream). The call returns once the result is in pY.
+ * - The first call on a device looks up the scratch array's device address
+ *   (cudaGetSymbolAddress); make that first call before any stream capture.
+ * - Every call shares the one array and rebuilds its contents; calls that
+ *   overlap on the GPU (other threads or streams) race on it. */
+FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc(FFTLIB_F32 *pX, FFTLIB_F32 *pY,
+                                                                       uint32_t numPoints, uint32_t numChannels,
+                                                                       void *stream);
+
 /* The twiddle tables the reference test drivers build for the c2c/ifft
  * kernels and the int16 kernel, bit-identical to theirs. */
 void FFTLIB_b200_tw_gen_c2c(FFTLIB_F32 *pW, uint32_t numPoints);
