@@ -251,15 +251,15 @@ def our_arm(args, world, rank, local):
             print(json.dumps({"quick": True, "ms_per_step": ms_step, "GBps": value, "channels": ch}))
         return
 
-    # parity spot check of the timed output (a few channels against FP64)
+    # spot check of the timed output: a few channels against numpy's FFT in FP64
     import numpy as np
 
-    import oracle as O
-
     idx = [0, ch // 3, ch - 1]
-    xs = X.view(ch, 2 * n)[idx].cpu().numpy().ravel()
-    ys = Y.view(ch, 2 * n)[idx].cpu().numpy().ravel()
-    rel = O.rel_l2(ys, O.fp64_c2c(xs, n, len(idx)))
+    xs = X.view(ch, 2 * n)[idx].cpu().numpy().astype(np.float64)
+    ys = Y.view(ch, 2 * n)[idx].cpu().numpy().astype(np.float64)
+    want = np.fft.fft(xs[:, 0::2] + 1j * xs[:, 1::2], axis=1)
+    got = ys[:, 0::2] + 1j * ys[:, 1::2]
+    rel = float(np.linalg.norm(got - want) / np.linalg.norm(want))
 
     # end to end through the synchronous FFTLIB call with pinned host buffers
     e2e_steps = max(2, min(args.steps, 5))
@@ -305,7 +305,124 @@ def our_arm(args, world, rank, local):
     }
     if world == 1:
         out["cpu_baseline"] = cpu_baseline()
+        out["configs"] = secondary_configs(args)
     print(json.dumps(out))
+
+
+def _time_launches(torch, stream, fn, steps, warmup=3):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def mixed_lengths(count, seed, nmax=4096):
+    """Lengths 12 * 2^a 3^b 5^c <= nmax, log N uniform on [log 12, log nmax]
+    snapped to the nearest allowed length."""
+    import numpy as np
+
+    allowed = sorted({12 * (2 ** a) * (3 ** b) * (5 ** c) for a in range(12) for b in range(8) for c in range(6)
+                      if 12 * (2 ** a) * (3 ** b) * (5 ** c) <= nmax})
+    allowed = np.array(allowed)
+    u = np.random.default_rng(seed).uniform(np.log(12), np.log(nmax), count)
+    return allowed[np.abs(np.log(allowed)[None, :] - u[:, None]).argmin(axis=1)].astype(np.uint32)
+
+
+def secondary_configs(args):
+    """The other workloads of the benchmark configuration list, device
+    buffers, CUDA events on the launching stream."""
+    import numpy as np
+    import torch
+
+    import c7x_fftlib_b200 as F
+
+    steps = max(5, min(args.steps, 20))
+    stream = torch.cuda.Stream()
+    sp = F.ptr(stream.cuda_stream)
+    res = {}
+    g = torch.Generator(device="cuda").manual_seed(7)
+
+    # int16 c2c, N=1024 x 4096, inputs in [-2048, 2047], shift 2 per radix-4 stage
+    n, ch = 1024, 4096
+    x = torch.randint(-2048, 2048, (2 * n * ch,), device="cuda", dtype=torch.int16, generator=g)
+    y = torch.empty_like(x)
+    w = np.zeros(2 * n, np.int16)
+    F.lib().FFTLIB_b200_tw_gen_i16(F.ptr(w), n)
+    wd = torch.from_numpy(w).cuda()
+    sh = torch.full((5,), 2, dtype=torch.int32, device="cuda")
+    bx, bw, bs = F.bp(F.FFTLIB_INT16, 2 * n * ch), F.bp(F.FFTLIB_INT16, 2 * n), F.bp(F.FFTLIB_UINT32, 5)
+    pb = F.pblock("i16")
+    F.check(F.fn(F.KERNELS["i16"] + "_init")(F.ptr(x), bx, F.ptr(wd), bw, F.ptr(y), bx, F.ptr(sh), bs, n, ch, pb))
+    k = F.fn("FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync")
+    ms = _time_launches(torch, stream, lambda: k(F.ptr(x), F.ptr(wd), F.ptr(y), F.ptr(sh), 5, n, ch, pb, sp), steps)
+    res["int16_c2c_n1024_x4096"] = {"ms": round(ms, 4), "GBps": round(8.0 * n * ch / ms / 1e6, 1),
+                                     "transforms_per_s": round(ch / ms * 1e3, 1)}
+
+    # r2c then c2r, N=4096 x 8192 reals (128 MiB), outmode / inMode 0
+    n, ch = 4096, 8192
+    xr = torch.randn(n * ch, device="cuda", generator=g)
+    yc = torch.empty(2 * (n // 2 + 1) * ch, device="cuda")
+    xb = torch.empty_like(xr)
+    b = F.bp(F.FFTLIB_FLOAT32, n * ch)
+    pr, pc = F.pblock("r2c"), F.pblock("c2r")
+    F.check(F.fn(F.KERNELS["r2c"] + "_init")(F.ptr(xr), b, F.ptr(xr), b, None, b, F.ptr(xr), b, F.ptr(yc), b, n, ch,
+                                             0, pr))
+    F.check(F.fn(F.KERNELS["c2r"] + "_init")(F.ptr(yc), b, F.ptr(yc), b, None, b, F.ptr(yc), b, F.ptr(xb), b, n, ch,
+                                             0, pc))
+    kr = F.fn("FFTLIB_b200_fft1dBatched_i32f_c32fc_o32fc_kernelAsync")
+    kc = F.fn("FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32f_kernelAsync")
+    ms_r = _time_launches(torch, stream, lambda: kr(F.ptr(xr), None, F.ptr(yc), n, ch, 0, pr, sp), steps)
+    ms_c = _time_launches(torch, stream, lambda: kc(F.ptr(yc), None, F.ptr(xb), n, ch, 0, pc, sp), steps)
+    bytes_rc = (4.0 * n + 8.0 * (n // 2 + 1)) * ch
+    rt = float(torch.linalg.norm(xb - xr) / torch.linalg.norm(xr))
+    res["r2c_c2r_n4096_x8192"] = {"r2c_ms": round(ms_r, 4), "r2c_GBps": round(bytes_rc / ms_r / 1e6, 1),
+                                  "c2r_ms": round(ms_c, 4), "c2r_GBps": round(bytes_rc / ms_c / 1e6, 1),
+                                  "roundtrip_rel_l2": rt}
+
+    # uneven lengths: 20,000 c2c transforms, 12 * 2^a 3^b 5^c <= 4096, log-uniform,
+    # laid out grouped by length so per-length batched calls can run on the same memory
+    lengths = np.sort(mixed_lengths(20000, seed=2024))[::-1].copy()
+    total = int(lengths.sum())
+    xm = torch.rand(2 * total, device="cuda", generator=g) * 2 - 1
+    ym = torch.empty_like(xm)
+    mb = F.MixedBatch(lengths)
+    ms_graph = _time_launches(torch, stream, lambda: mb.exec(xm, ym, sp), steps)
+    ms_per = _time_launches(torch, stream, lambda: mb.exec_per_size(xm, ym, sp), steps)
+    # the regular batched API, one call per length (fixed-size kernels where compiled)
+    uniq, counts = np.unique(lengths, return_counts=True)
+    calls = []
+    off = 0
+    for nn, cc in sorted(zip(uniq.tolist(), counts.tolist()), reverse=True):
+        pbk = F.pblock("c2c")
+        bb = F.bp(F.FFTLIB_FLOAT32, 2 * nn * cc)
+        xs, ys = xm.data_ptr() + 8 * off, ym.data_ptr() + 8 * off
+        F.check(F.fn(F.KERNELS["c2c"] + "_init")(F.ptr(xs), bb, F.ptr(xs), F.bp(F.FFTLIB_FLOAT32, 2 * nn), F.ptr(ys),
+                                                 bb, nn, cc, pbk))
+        calls.append((xs, ys, nn, cc, pbk))
+        off += nn * cc
+    ka = F.fn("FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync")
+
+    def per_length_api():
+        for xs, ys, nn, cc, pbk in calls:
+            ka(F.ptr(xs), F.ptr(ys), nn, cc, pbk, sp)
+
+    ms_api = _time_launches(torch, stream, per_length_api, steps)
+    mbytes = 16.0 * total
+    res["mixed_20000"] = {"lengths": len(uniq), "total_points": total,
+                          "persistent_graph_ms": round(ms_graph, 4),
+                          "persistent_graph_GBps": round(mbytes / ms_graph / 1e6, 1),
+                          "per_length_same_kernel_ms": round(ms_per, 4),
+                          "per_length_batched_api_ms": round(ms_api, 4),
+                          "speedup_vs_per_length_api": round(ms_api / ms_graph, 3),
+                          "transforms_per_s": round(20000 / ms_graph * 1e3, 1)}
+    mb.close()
+    return res
 
 
 def cpu_baseline():

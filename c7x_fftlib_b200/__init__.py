@@ -118,6 +118,15 @@ def lib() -> C.CDLL:
                                                                          _vp]
     L.FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc.argtypes = [_vp, _vp, _u32, _u32, _vp]
     L.FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc.restype = C.c_int
+    L.FFTLIB_b200_fftMixed_supported.argtypes = [_u32]
+    L.FFTLIB_b200_fftMixed_create.argtypes = [C.POINTER(C.c_uint32), _u32, _u32, C.POINTER(_vp)]
+    L.FFTLIB_b200_fftMixed_exec.argtypes = [_vp, _vp, _vp, _vp]
+    L.FFTLIB_b200_fftMixed_execPerSize.argtypes = [_vp, _vp, _vp, _vp]
+    L.FFTLIB_b200_fftMixed_describe.argtypes = [_vp, C.c_char_p, _u32]
+    L.FFTLIB_b200_fftMixed_destroy.argtypes = [_vp]
+    for fname in ("fftMixed_supported", "fftMixed_create", "fftMixed_exec", "fftMixed_execPerSize",
+                  "fftMixed_describe", "fftMixed_destroy"):
+        getattr(L, "FFTLIB_b200_" + fname).restype = C.c_int
     L.FFTLIB_b200_tw_gen_c2c.argtypes = [_vp, _u32]
     L.FFTLIB_b200_tw_gen_i16.argtypes = [_vp, _u32]
     for fn in ("tw_gen_r2c", "split_factor_gen_r2c", "ifft_c2r_tw_gen", "ifft_c2r_split_factor_gen"):
@@ -163,6 +172,45 @@ def describe_plan(n: int) -> str:
     buf = C.create_string_buffer(256)
     check(lib().FFTLIB_b200_describePlan(n, buf, 256), "describePlan")
     return buf.value.decode()
+
+
+MIXED_INVERSE = 1
+MIXED_AUTOTUNE = 2
+
+
+class MixedBatch:
+    """FFTLIB_b200_fftMixed_*: uneven-length c2c batch (device buffers)."""
+
+    def __init__(self, lengths, inverse=False, autotune=False):
+        import numpy as _np
+
+        self.lengths = _np.ascontiguousarray(lengths, _np.uint32)
+        self.h = C.c_void_p()
+        flags = (MIXED_INVERSE if inverse else 0) | (MIXED_AUTOTUNE if autotune else 0)
+        arr = self.lengths.ctypes.data_as(C.POINTER(C.c_uint32))
+        check(lib().FFTLIB_b200_fftMixed_create(arr, len(self.lengths), flags, C.byref(self.h)), "fftMixed_create")
+
+    def exec(self, x, y, stream=None):
+        check(lib().FFTLIB_b200_fftMixed_exec(self.h, ptr(x), ptr(y), stream), "fftMixed_exec")
+
+    def exec_per_size(self, x, y, stream=None):
+        check(lib().FFTLIB_b200_fftMixed_execPerSize(self.h, ptr(x), ptr(y), stream), "fftMixed_execPerSize")
+
+    def describe(self) -> str:
+        buf = C.create_string_buffer(8192)
+        check(lib().FFTLIB_b200_fftMixed_describe(self.h, buf, 8192), "fftMixed_describe")
+        return buf.value.decode()
+
+    def close(self):
+        if self.h:
+            lib().FFTLIB_b200_fftMixed_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def fn(name: str):

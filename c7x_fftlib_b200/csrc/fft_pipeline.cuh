@@ -161,11 +161,13 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
         static_for<S::P>([&](auto p) {
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
+            float2* rowOut = a.out + (size_t)tile * N;
             if constexpr (P == 0) {
-                run_pass<S::EMAX, S::R[P]>(a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true, st,
-                                           refill);
+                run_pass<S::EMAX, S::R[P]>(a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true,
+                                           nullptr, rowOut, st, refill);
             } else {
-                run_pass<S::EMAX, S::R[P]>(a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true);
+                run_pass<S::EMAX, S::R[P]>(a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true,
+                                           nullptr, rowOut);
             }
         });
     }

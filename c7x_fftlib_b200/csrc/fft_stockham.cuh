@@ -52,7 +52,7 @@ FFT_DEV void dispatch_radix(int r, F&& f)
 
 // Pass-0 input element idx of transform b (complex index into the pass's
 // length-N sequence), with the c2r split pre-process when requested.
-FFT_DEV float2 load_in(const FftArgs& a, uint32_t b, uint32_t idx, const float2* tile)
+FFT_DEV float2 load_in(const FftArgs& a, const float2* rowIn, uint32_t idx, const float2* tile)
 {
     float2 z;
     if (a.ioMode == IO_C2R_SPLIT) {
@@ -65,9 +65,8 @@ FFT_DEV float2 load_in(const FftArgs& a, uint32_t b, uint32_t idx, const float2*
             x = tile[smem_swz(idx)];
             y = tile[smem_swz(ip)];
         } else {
-            const float2* row = a.in + (int64_t)b * a.inBatch;
-            x = row[(int64_t)idx * a.inElem];
-            y = row[(int64_t)ip * a.inElem];
+            x = rowIn[(int64_t)idx * a.inElem];
+            y = rowIn[(int64_t)ip * a.inElem];
         }
         if (!a.realMode) y = cconj(y);
         const float2 w = __ldg(&a.twSplit[idx]);
@@ -77,7 +76,7 @@ FFT_DEV float2 load_in(const FftArgs& a, uint32_t b, uint32_t idx, const float2*
     } else if (a.staged) {
         z = tile[smem_swz(idx)];
     } else {
-        z = a.in[(int64_t)b * a.inBatch + (int64_t)idx * a.inElem];
+        z = rowIn[(int64_t)idx * a.inElem];
     }
     return a.conjIn ? cconj(z) : z;
 }
@@ -106,10 +105,13 @@ FFT_DEV uint32_t swz_step(uint32_t swzBase, uint32_t idx0, uint32_t q, uint32_t 
 // raw: when not null, the first pass reads its input from this unpadded
 // shared-memory copy of the transform (filled by a bulk async copy).
 // afterGather runs right after the barrier that ends the pass's reads.
+// rowIn / rowOut: this lane's transform in HBM (first / last pass); b is its
+// index in the batch (four-step column twiddle).
 template <int EMAX, int R, class Hook = NoHook>
 FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, const bool last,
                       const uint32_t T, float2 (&v)[EMAX], float2* sm, uint32_t t, uint32_t b, bool active,
-                      const float2* raw = nullptr, Hook afterGather = Hook())
+                      const float2* rowIn, float2* rowOut, const float2* raw = nullptr,
+                      Hook afterGather = Hook())
 {
     constexpr int BMAX = EMAX / R;
     const uint32_t nb = pi.stride; // butterflies in this pass: N / R
@@ -126,7 +128,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
                     z = raw[idx];
                     if (a.conjIn) z = cconj(z);
                 } else if (first) {
-                    z = (active || a.staged) ? load_in(a, b, idx, sm) : make_float2(0.f, 0.f);
+                    z = (active || a.staged) ? load_in(a, rowIn, idx, sm) : make_float2(0.f, 0.f);
                 } else {
                     z = sm[swz_step(sj, j, (uint32_t)q, nb)];
                 }
@@ -157,7 +159,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
     const bool direct = last && !a.staged && a.ioMode != IO_R2C_SPLIT;
     if (direct) {
         if (active) {
-            float2* row = a.out + (int64_t)b * a.outBatch;
+            float2* row = rowOut;
             static_for<BMAX>([&](auto i) {
                 const uint32_t j = t + (uint32_t)i * T;
                 if (j < nb) {
@@ -205,11 +207,10 @@ FFT_DEV float2 r2c_split(float2 z, float2 zp, float2 w)
     return cadd(e, cmul(miw, o));
 }
 
-FFT_DEV void r2c_epilogue(const FftArgs& a, const float2* sm, uint32_t t, uint32_t b, bool active)
+FFT_DEV void r2c_epilogue(const FftArgs& a, const float2* sm, uint32_t t, float2* row, bool active)
 {
     if (!active) return;
     const uint32_t h = a.N;
-    float2* row = a.out + (int64_t)b * a.outBatch;
     for (uint32_t i = t; i <= h / 2; i += a.T) {
         if (i == 0) {
             const float2 z0 = sm[smem_swz(0)];
@@ -286,14 +287,17 @@ FFT_DEV void fft_tile(const FftArgs& a, float2* smem, uint32_t b0)
         stage_in(a, smem, b0);
         __syncthreads();
     }
+    const float2* rowIn = a.in + (int64_t)b * a.inBatch;
+    float2* rowOut = a.out + (int64_t)b * a.outBatch;
     float2 v[EMAX];
     for (int p = 0; p < (int)a.P; ++p) {
         dispatch_radix<EMAX>(a.pass[p].R, [&](auto r) {
-            run_pass<EMAX, decltype(r)::value>(a, a.pass[p], p == 0, p + 1 == (int)a.P, a.T, v, sm, t, b, active);
+            run_pass<EMAX, decltype(r)::value>(a, a.pass[p], p == 0, p + 1 == (int)a.P, a.T, v, sm, t, b, active,
+                                               rowIn, rowOut);
         });
     }
     if (a.ioMode == IO_R2C_SPLIT) {
-        r2c_epilogue(a, sm, t, b, active);
+        r2c_epilogue(a, sm, t, rowOut, active);
     } else if (a.staged) {
         stage_out(a, smem, b0);
     }
@@ -335,14 +339,17 @@ FFT_DEV void fft_tile_static(const FftArgs& a, float2* smem, uint32_t b0)
         stage_in(a, smem, b0);
         __syncthreads();
     }
+    const float2* rowIn = a.in + (int64_t)b * a.inBatch;
+    float2* rowOut = a.out + (int64_t)b * a.outBatch;
     float2 v[S::EMAX];
     static_for<S::P>([&](auto p) {
         constexpr int P = decltype(p)::value;
         constexpr PassInfo pi = S::pass(P);
-        run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, b, active);
+        run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, b, active, rowIn,
+                                   rowOut);
     });
     if (a.ioMode == IO_R2C_SPLIT) {
-        r2c_epilogue(a, sm, t, b, active);
+        r2c_epilogue(a, sm, t, rowOut, active);
     } else if (a.staged) {
         stage_out(a, smem, b0);
     }

@@ -50,7 +50,9 @@ void enumerate(uint32_t rem, int maxIdx, std::vector<int>& cur, std::vector<std:
 // round trip; idle butterfly slots and wider register files cost extra.
 bool evaluate(uint32_t n, const int* seq, int len, int emax, EnginePlan* e)
 {
-    const int maxT = engine_max_threads(emax);
+    // widths without a runtime-engine instantiation (the mixed-batch kernel's)
+    // are capped by the caller's maxT instead
+    const int maxT = engine_max_threads(emax) ? engine_max_threads(emax) : 1024;
     if (len > kMaxPasses) return false;
     uint32_t T = 1;
     for (int i = 0; i < len; ++i) {
@@ -80,7 +82,7 @@ bool evaluate(uint32_t n, const int* seq, int len, int emax, EnginePlan* e)
 
 } // namespace
 
-std::vector<EnginePlan> engine_candidates(uint32_t n)
+std::vector<EnginePlan> engine_candidates(uint32_t n, int emaxOnly, uint32_t maxT)
 {
     std::vector<EnginePlan> out;
     if (!is_235(n)) return out;
@@ -98,9 +100,10 @@ std::vector<EnginePlan> engine_candidates(uint32_t n)
     std::vector<int> cur;
     enumerate(n, 0, cur, seqs, kMaxPasses);
     for (const auto& s : seqs) {
-        for (int emax : kEmax) {
+        const int only[1] = {emaxOnly};
+        for (int emax : (emaxOnly ? std::vector<int>(only, only + 1) : std::vector<int>(kEmax, kEmax + 3))) {
             EnginePlan e;
-            if (evaluate(n, s.data(), (int)s.size(), emax, &e)) out.push_back(e);
+            if (evaluate(n, s.data(), (int)s.size(), emax, &e) && (!maxT || e.T <= maxT)) out.push_back(e);
         }
     }
     std::stable_sort(out.begin(), out.end(),
@@ -264,6 +267,8 @@ cudaError_t make_table(float2** p, uint32_t n, uint32_t count, cudaStream_t s)
     return launch_twiddle(*p, n, count, s);
 }
 
+} // namespace
+
 // Per-pass twiddle blocks of a single-kernel schedule (see PassInfo).
 cudaError_t make_pass_table(float2** p, const EnginePlan& e, cudaStream_t s)
 {
@@ -285,8 +290,6 @@ cudaError_t make_pass_table(float2** p, const EnginePlan& e, cudaStream_t s)
     if (err != cudaSuccess) return err;
     return launch_twiddle_passes(*p, tp, s);
 }
-
-} // namespace
 
 // n = n1 * n2 with n1 <= n2, n1 as close to sqrt(n) as possible, both with
 // single-kernel schedules.
@@ -324,6 +327,8 @@ ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err)
         p->device = dev;
         p->n = n;
         if (n <= kMaxSingleN && plan_engine(n, &p->eng)) {
+            EnginePlan tuned;
+            if (autotune_enabled() && tune_schedule(n, 4096, 0, 0, &tuned)) p->eng = tuned;
             *err = make_pass_table(&p->tw, p->eng, s);
         } else if (split_four_step(n, &p->n1, &p->n2)) {
             p->fourStep = true;

@@ -31,9 +31,25 @@ struct EnginePlan {
 
 bool is_235(uint32_t n);
 
-// All feasible single-kernel schedules for n, best heuristic first.
-std::vector<EnginePlan> engine_candidates(uint32_t n);
+// All feasible single-kernel schedules for n, best heuristic first
+// (emaxOnly: restrict to one engine width; maxT: cap threads per transform).
+std::vector<EnginePlan> engine_candidates(uint32_t n, int emaxOnly = 0, uint32_t maxT = 0);
 bool plan_engine(uint32_t n, EnginePlan* out);
+
+// Per-pass twiddle blocks of a schedule, allocated and filled on the device.
+cudaError_t make_pass_table(float2** p, const EnginePlan& e, cudaStream_t s);
+
+// Autotuner: times the heuristic's best candidates for (n, batch) through
+// the real launch path and returns the fastest; results are cached per
+// device, length and batch bucket in memory and in a text file
+// ($FFTLIB_B200_TUNE_CACHE, default $HOME/.cache/fftlib_b200_tune.txt).
+// timer(e, x, y, batch, stream, &ok): average milliseconds of one launch of
+// schedule e over `batch` transforms x -> y; the default times launch_fft.
+using ScheduleTimer = float (*)(const EnginePlan&, float2*, float2*, uint32_t, cudaStream_t, bool*);
+bool tune_schedule(uint32_t n, uint32_t batch, int emaxOnly, uint32_t maxT, EnginePlan* out,
+                   ScheduleTimer timer = nullptr);
+// True when $FFTLIB_B200_AUTOTUNE is set to a non-zero value.
+bool autotune_enabled();
 std::string describe(const EnginePlan& e);
 // Four-step split n = n1 * n2 (n1 <= n2, both single-kernel lengths).
 bool split_four_step(uint32_t n, uint32_t* n1, uint32_t* n2);

@@ -78,6 +78,31 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc(FFTLIB_F3
                                                                        uint32_t numPoints, uint32_t numChannels,
                                                                        void *stream);
 
+/* Batches of FP32 complex-to-complex transforms of uneven lengths, run by a
+ * single persistent kernel launch replayed from a CUDA graph. No counterpart
+ * in the reference library (its batched kernels take one length per call).
+ * Transform i has length numPoints[i] (2^a 3^b 5^c, at most 4096) and occupies
+ * 2 * numPoints[i] floats of pX and of pY, the transforms packed back to back
+ * in the order given. create() groups the transforms by length, picks each
+ * group's radix schedule (timed by the autotuner when FFTLIB_B200_MIXED_AUTOTUNE
+ * is set or $FFTLIB_B200_AUTOTUNE is non-zero; results cached in
+ * $FFTLIB_B200_TUNE_CACHE, default $HOME/.cache/fftlib_b200_tune.txt) and
+ * uploads the schedule and tile tables. exec() enqueues the transform on
+ * `stream` (device buffers) and returns; execPerSize() runs the same work as
+ * one launch per distinct length, for comparison. */
+typedef struct FFTLIB_b200_mixed *FFTLIB_b200_mixedHandle;
+#define FFTLIB_B200_MIXED_INVERSE  1u
+#define FFTLIB_B200_MIXED_AUTOTUNE 2u
+FFTLIB_STATUS FFTLIB_b200_fftMixed_supported(uint32_t numPoints);
+FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t *numPoints, uint32_t count, uint32_t flags,
+                                          FFTLIB_b200_mixedHandle *handle);
+FFTLIB_STATUS FFTLIB_b200_fftMixed_exec(FFTLIB_b200_mixedHandle handle, const FFTLIB_F32 *pX, FFTLIB_F32 *pY,
+                                        void *stream);
+FFTLIB_STATUS FFTLIB_b200_fftMixed_execPerSize(FFTLIB_b200_mixedHandle handle, const FFTLIB_F32 *pX,
+                                               FFTLIB_F32 *pY, void *stream);
+FFTLIB_STATUS FFTLIB_b200_fftMixed_describe(FFTLIB_b200_mixedHandle handle, char *buf, uint32_t len);
+FFTLIB_STATUS FFTLIB_b200_fftMixed_destroy(FFTLIB_b200_mixedHandle handle);
+
 /* The twiddle tables the reference test drivers build for the c2c/ifft
  * kernels and the int16 kernel, bit-identical to theirs. */
 void FFTLIB_b200_tw_gen_c2c(FFTLIB_F32 *pW, uint32_t numPoints);

@@ -99,3 +99,24 @@ def i16(x: np.ndarray, n: int, ch: int, shifts, w=None, on_device=True) -> np.nd
     F.check(F.fn(base + "_init")(*args, pb), base + "_init")
     F.check(F.fn(base + "_kernel")(*args, pb), base + "_kernel")
     return _host(Y) if on_device else Y
+
+
+def mixed_lengths(count: int, seed: int, nmax: int = 4096):
+    """Lengths 12 * 2^a 3^b 5^c <= nmax drawn log-uniformly: log N uniform on
+    [log 12, log nmax], snapped to the nearest allowed length in log space."""
+    allowed = []
+    a = 1
+    while 12 * a <= nmax:
+        b = a
+        while 12 * b <= nmax:
+            c = b
+            while 12 * c <= nmax:
+                allowed.append(12 * c)
+                c *= 5
+            b *= 3
+        a *= 2
+    allowed = np.array(sorted(allowed))
+    g = np.random.default_rng(seed)
+    u = g.uniform(np.log(12), np.log(nmax), count)
+    idx = np.abs(np.log(allowed)[None, :] - u[:, None]).argmin(axis=1)
+    return allowed[idx].astype(np.uint32)

@@ -274,3 +274,13 @@ def test_planner_headline_schedule():
 
 def test_planner_rejects_other_primes():
     assert F.lib().FFTLIB_b200_describePlan(7, C.create_string_buffer(64), 64) == F.FFTLIB_ERR_INVALID_DIMENSION
+
+
+def test_mixed_batch_supports_every_length_up_to_4096():
+    import fftcall
+
+    for n in _sizes_235(4096):
+        assert F.lib().FFTLIB_b200_fftMixed_supported(n) == F.FFTLIB_SUCCESS, n
+    for n in set(fftcall.mixed_lengths(2000, seed=0).tolist()):
+        assert n % 12 == 0 and n <= 4096
+    assert F.lib().FFTLIB_b200_fftMixed_supported(7) == F.FFTLIB_ERR_INVALID_DIMENSION

@@ -1,0 +1,100 @@
+"""Uneven-length batches (FFTLIB_b200_fftMixed_*): one persistent launch over
+a descriptor table must give every transform the result of its own FFT."""
+import os
+
+import numpy as np
+import pytest
+
+import c7x_fftlib_b200 as F
+import fftcall
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+REL_L2 = 2e-6
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def check_all(x, y, lengths, inverse=False):
+    off = 0
+    worst = 0.0
+    segs = {}
+    for i, n in enumerate(lengths):
+        segs.setdefault(int(n), []).append(off)
+        off += 2 * int(n)
+    for n, offs in segs.items():
+        xs = np.concatenate([x[o: o + 2 * n] for o in offs])
+        ys = np.concatenate([y[o: o + 2 * n] for o in offs])
+        err = O.rel_l2(ys, O.fp64_c2c(xs, n, len(offs), inverse))
+        worst = max(worst, err)
+        assert err <= REL_L2, (n, err)
+    return worst
+
+
+@pytest.mark.parametrize("inverse", [False, True])
+def test_mixed_matches_fp64(torch, inverse):
+    lengths = fftcall.mixed_lengths(3000, seed=4)
+    total = int(lengths.sum())
+    x = O.uniform_c2c(total, 1, seed=9)
+    X = torch.from_numpy(x).cuda()
+    Y = torch.zeros_like(X)
+    mb = F.MixedBatch(lengths, inverse=inverse)
+    mb.exec(X, Y)
+    torch.cuda.synchronize()
+    check_all(x, Y.cpu().numpy(), lengths, inverse)
+    # one launch per length computes the same numbers
+    Y2 = torch.zeros_like(X)
+    mb.exec_per_size(X, Y2)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(Y.cpu().numpy(), Y2.cpu().numpy())
+    mb.close()
+
+
+def test_mixed_buffer_change_and_repeat(torch):
+    lengths = np.array([12, 4096, 60, 60, 1536, 3000, 12, 960, 2880, 240] * 37, np.uint32)
+    total = int(lengths.sum())
+    mb = F.MixedBatch(lengths)
+    for seed in (1, 2):
+        x = O.uniform_c2c(total, 1, seed=seed)
+        X = torch.from_numpy(x).cuda()
+        Y = torch.zeros_like(X)
+        for _ in range(2):
+            mb.exec(X, Y)
+        torch.cuda.synchronize()
+        check_all(x, Y.cpu().numpy(), lengths)
+    mb.close()
+
+
+def test_mixed_every_allowed_length(torch):
+    lengths = np.array(sorted(set(fftcall.mixed_lengths(20000, seed=1)) | {1, 2, 3, 4, 5, 8, 16, 25, 4096}),
+                       np.uint32)
+    total = int(lengths.sum())
+    x = O.uniform_c2c(total, 1, seed=3)
+    X = torch.from_numpy(x).cuda()
+    Y = torch.zeros_like(X)
+    mb = F.MixedBatch(lengths)
+    mb.exec(X, Y)
+    torch.cuda.synchronize()
+    check_all(x, Y.cpu().numpy(), lengths)
+
+
+def test_mixed_autotuned(torch, tmp_path, monkeypatch):
+    monkeypatch.setenv("FFTLIB_B200_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    lengths = fftcall.mixed_lengths(500, seed=11)
+    total = int(lengths.sum())
+    x = O.uniform_c2c(total, 1, seed=12)
+    X = torch.from_numpy(x).cuda()
+    Y = torch.zeros_like(X)
+    mb = F.MixedBatch(lengths, autotune=True)
+    mb.exec(X, Y)
+    torch.cuda.synchronize()
+    check_all(x, Y.cpu().numpy(), lengths)
+    assert os.path.exists(tmp_path / "tune.txt")
+    assert len(open(tmp_path / "tune.txt").read().splitlines()) >= len(set(lengths.tolist())) - 1
