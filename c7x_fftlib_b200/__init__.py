@@ -57,6 +57,17 @@ class BufParams(C.Structure):
     _fields_ = [("data_type", C.c_uint32), ("dim_x", C.c_uint32)]
 
 
+class MmaInitArgs(C.Structure):
+    """FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs
+    (src/fft_c7xmma/FFTLIB_FFT_fft_ixX_cxX_oxX/FFTLIB_FFT_fft_ixX_cxX_oxX.h:42-64)."""
+    _fields_ = [("funcStyle", C.c_int8), ("fftSize", C.c_uint32), ("batchSize", C.c_uint32),
+                ("interleave", C.c_uint32), ("shiftVector", C.c_uint32 * 5)]
+
+
+# paths the coordinator's init picks (FFTLIB_b200_FFT_fft_path)
+MMA_PATH_TC = 1
+MMA_PATH_FFT = 2
+
 _vp = C.c_void_p
 _bpp = C.POINTER(BufParams)
 _u32 = C.c_uint32
@@ -127,6 +138,24 @@ def lib() -> C.CDLL:
     for fname in ("fftMixed_supported", "fftMixed_create", "fftMixed_exec", "fftMixed_execPerSize",
                   "fftMixed_describe", "fftMixed_destroy"):
         getattr(L, "FFTLIB_b200_" + fname).restype = C.c_int
+    M = "FFTLIB_FFT_fft_ixX_cxX_oxX_"
+    _ia = C.POINTER(MmaInitArgs)
+    getattr(L, M + "getHandleSize").argtypes = [_ia]
+    getattr(L, M + "getHandleSize").restype = C.c_int32
+    getattr(L, M + "getSizes").argtypes = [_ia, _bpp, _bpp, _bpp]
+    getattr(L, M + "twGen").argtypes = [_ia, _vp, _bpp]
+    getattr(L, M + "init").argtypes = [_vp, _bpp, _bpp, _bpp, _ia]
+    getattr(L, M + "init_checkParams").argtypes = [_vp, _bpp, _bpp, _bpp, _ia]
+    getattr(L, M + "exec").argtypes = [_vp, _vp, _vp, _vp]
+    getattr(L, M + "exec_checkParams").argtypes = [_vp, _vp, _vp, _vp]
+    for f in ("getSizes", "twGen", "init", "init_checkParams", "exec", "exec_checkParams"):
+        getattr(L, M + f).restype = C.c_int
+    L.FFTLIB_b200_FFT_fft_execAsync.argtypes = [_vp, _vp, _vp, _vp, _vp]
+    L.FFTLIB_b200_FFT_fft_execAsync.restype = C.c_int
+    L.FFTLIB_b200_FFT_fft_sync.argtypes = [_vp]
+    L.FFTLIB_b200_FFT_fft_sync.restype = C.c_int
+    L.FFTLIB_b200_FFT_fft_path.argtypes = [_vp]
+    L.FFTLIB_b200_FFT_fft_path.restype = C.c_int32
     L.FFTLIB_b200_tw_gen_c2c.argtypes = [_vp, _u32]
     L.FFTLIB_b200_tw_gen_i16.argtypes = [_vp, _u32]
     for fn in ("tw_gen_r2c", "split_factor_gen_r2c", "ifft_c2r_tw_gen", "ifft_c2r_split_factor_gen"):
@@ -216,3 +245,43 @@ class MixedBatch:
 def fn(name: str):
     """The exported C function `name` (reference name or FFTLIB_b200_*)."""
     return getattr(lib(), name)
+
+
+class DftMma:
+    """FFTLIB_FFT_fft_ixX_cxX_oxX_*: the DFT coordinator for FLOAT32
+    interleaved complex data (getSizes, twGen, init_checkParams, init, then
+    exec or the stream-ordered execAsync)."""
+
+    def __init__(self, n: int, batch: int, func_style: int = FFTLIB_FUNCTION_OPTIMIZED, w_device=True):
+        import numpy as _np
+
+        L = lib()
+        M = "FFTLIB_FFT_fft_ixX_cxX_oxX_"
+        self.n, self.batch = n, batch
+        self.args = MmaInitArgs(func_style, n, batch, 1)
+        self.bx, self.bw, self.by = (BufParams(FFTLIB_FLOAT32, 0) for _ in range(3))
+        check(getattr(L, M + "getSizes")(C.byref(self.args), self.bx, self.bw, self.by), "getSizes")
+        self.handle = C.create_string_buffer(getattr(L, M + "getHandleSize")(C.byref(self.args)))
+        check(getattr(L, M + "init_checkParams")(self.handle, self.bx, self.bw, self.by, C.byref(self.args)),
+              "init_checkParams")
+        check(getattr(L, M + "init")(self.handle, self.bx, self.bw, self.by, C.byref(self.args)), "init")
+        self.w_host = _np.zeros(self.bw.dim_x, _np.float32)
+        check(getattr(L, M + "twGen")(C.byref(self.args), ptr(self.w_host), self.bw), "twGen")
+        self.w = None
+        if w_device:
+            import torch
+
+            self.w = torch.empty(self.bw.dim_x, dtype=torch.float32, device="cuda")
+            check(getattr(L, M + "twGen")(C.byref(self.args), ptr(self.w), self.bw), "twGen (device)")
+
+    @property
+    def path(self) -> int:
+        return lib().FFTLIB_b200_FFT_fft_path(self.handle)
+
+    def exec(self, x, y, w=None):
+        w = self.w if w is None else w
+        check(lib().FFTLIB_FFT_fft_ixX_cxX_oxX_exec(self.handle, ptr(x), ptr(w), ptr(y)), "exec")
+
+    def exec_async(self, x, y, stream=None, w=None):
+        w = self.w if w is None else w
+        check(lib().FFTLIB_b200_FFT_fft_execAsync(self.handle, ptr(x), ptr(w), ptr(y), stream), "execAsync")

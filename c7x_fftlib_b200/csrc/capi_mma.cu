@@ -1,0 +1,260 @@
+// capi_mma.cu -- FFTLIB_FFT_fft_ixX_cxX_oxX_*: the DFT coordinator of the
+// reference's src/fft_c7xmma/FFTLIB_FFT_fft_ixX_cxX_oxX/
+// FFTLIB_FFT_fft_ixX_cxX_oxX.cpp:7-282, for FLOAT32 data.
+//
+// The reference picks dftSmall / dftLarge / highRadixDecompositions from
+// fftSize and batchSize (FFTLIB_FFT_fft_ixX_cxX_oxX.cpp:13-50) for its MMA
+// widths. Here init picks between two GPU paths:
+//   PATH_TC  -- funcStyle OPTIMIZED and fftSize a power of two in [8, 4096]:
+//               the split-precision tensor-core DFT (one DFT-GEMM up to 64,
+//               two DFT-GEMM stages with the twiddle fused between above);
+//   PATH_FFT -- otherwise, for fftSize = 2^a 3^b 5^c: the CUDA-core FP32 FFT
+//               of the fft1dBatched c2c kernel.
+#include <string.h>
+
+#include "capi_common.h"
+#include "fft_c7xmma.h"
+#include "fftlib_b200_ext.h"
+#include "plan.h"
+#include "tc_dft.h"
+
+using namespace fftb200;
+
+namespace {
+
+constexpr uint32_t kMmaMagic = 0x32414D4Du;  // "MMA2"
+enum MmaPath : int32_t { PATH_NONE = 0, PATH_TC = 1, PATH_FFT = 2 };
+
+struct MmaHandle {
+    uint32_t magic;
+    int32_t path;
+    int32_t device;
+    uint32_t reserved;
+    FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs init;
+    ComplexPlan* plan;  // PATH_FFT
+};
+
+int32_t choose_path(const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* a)
+{
+    if (a->fftSize == 0 || a->batchSize == 0) return PATH_NONE;
+    if (a->funcStyle == FFTLIB_FUNCTION_OPTIMIZED && tc_dft_supported(a->fftSize)) return PATH_TC;
+    if (is_235(a->fftSize)) return PATH_FFT;
+    return PATH_NONE;
+}
+
+// FLOAT32 buffer sizes in elements.
+FFTLIB_STATUS sizes_f32(const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* a, uint32_t* x, uint32_t* w, uint32_t* y)
+{
+    if (!a->interleave) {
+        set_error("FLOAT32 data must be interleaved (interleave = 1)");
+        return FFTLIB_ERR_NOT_IMPLEMENTED;
+    }
+    const int32_t path = choose_path(a);
+    if (path == PATH_NONE) {
+        set_error("fftSize %u (batchSize %u) has no FLOAT32 path: it must be 2^a 3^b 5^c", a->fftSize, a->batchSize);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    const uint64_t xy = 2ull * a->fftSize * a->batchSize;
+    if (xy > 0xFFFFFFFFull) {
+        set_error("fftSize x batchSize x 2 = %llu exceeds the 32-bit dim_x", (unsigned long long)xy);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    *x = *y = (uint32_t)xy;
+    *w = path == PATH_TC ? (uint32_t)tc_dft_w_floats(a->fftSize) : 2u * a->fftSize;
+    return FFTLIB_SUCCESS;
+}
+
+FFTLIB_STATUS not_float(uint32_t type)
+{
+    set_error("data type %u: this library implements the coordinator for FLOAT32 (%d) only", type, FFTLIB_FLOAT32);
+    return FFTLIB_ERR_NOT_IMPLEMENTED;
+}
+
+MmaHandle* handle_of(FFTLIB_kernelHandle h)
+{
+    MmaHandle* m = static_cast<MmaHandle*>(h);
+    if (!m || m->magic != kMmaMagic || m->path == PATH_NONE) {
+        set_error("handle was not set up by FFTLIB_FFT_fft_ixX_cxX_oxX_init");
+        return nullptr;
+    }
+    return m;
+}
+
+cudaError_t enqueue(const MmaHandle* m, const float* x, const float* w, float* y, uint32_t batch, cudaStream_t s)
+{
+    if (m->path == PATH_TC)
+        return launch_tc_dft(m->init.fftSize, reinterpret_cast<const float2*>(x), reinterpret_cast<float2*>(y), w,
+                             batch, error_word().dev, s);
+    // above 16384 points the FFT uses pX as four-step scratch, as the
+    // fft1dBatched kernels do
+    return run_c2c(m->plan, const_cast<float2*>(reinterpret_cast<const float2*>(x)), reinterpret_cast<float2*>(y),
+                   batch, false, s);
+}
+
+} // namespace
+
+extern "C" {
+
+int32_t FFTLIB_FFT_fft_ixX_cxX_oxX_getHandleSize(FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* pKerInitArgs)
+{
+    (void)pKerInitArgs;
+    return (int32_t)sizeof(MmaHandle);
+}
+
+FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_getSizes(const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* pKerInitArgs,
+                                                  FFTLIB_bufParams1D_t* bufParamsX, FFTLIB_bufParams1D_t* bufParamsW,
+                                                  FFTLIB_bufParams1D_t* bufParamsY)
+{
+    if (!pKerInitArgs || !bufParamsX || !bufParamsW || !bufParamsY) return FFTLIB_ERR_NULL_POINTER;
+    if (bufParamsX->data_type != FFTLIB_FLOAT32) return not_float(bufParamsX->data_type);
+    uint32_t x, w, y;
+    const FFTLIB_STATUS st = sizes_f32(pKerInitArgs, &x, &w, &y);
+    if (st != FFTLIB_SUCCESS) return st;
+    bufParamsX->dim_x = x;
+    bufParamsW->dim_x = w;
+    bufParamsY->dim_x = y;
+    return FFTLIB_SUCCESS;
+}
+
+FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_twGen(const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* pKerInitArgs, void* pW,
+                                               const FFTLIB_bufParams1D_t* bufParamsW)
+{
+    if (!pKerInitArgs || !pW || !bufParamsW) return FFTLIB_ERR_NULL_POINTER;
+    if (bufParamsW->data_type != FFTLIB_FLOAT32) return not_float(bufParamsW->data_type);
+    uint32_t x, w, y;
+    FFTLIB_STATUS st = sizes_f32(pKerInitArgs, &x, &w, &y);
+    if (st != FFTLIB_SUCCESS) return st;
+    if (bufParamsW->dim_x != w) {
+        set_error("bufParamsW->dim_x %u, expected %u", bufParamsW->dim_x, w);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    const uint32_t n = pKerInitArgs->fftSize;
+    float* out = static_cast<float*>(pW);
+    const bool dev = is_device_ptr(pW);
+    if (choose_path(pKerInitArgs) == PATH_TC) {
+        if (!dev) {
+            tc_dft_gen_w_host(out, n);
+            return FFTLIB_SUCCESS;
+        }
+        cudaError_t e = tc_dft_gen_w_device(out, n, cudaStreamPerThread);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
+        return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen");
+    }
+    if (!dev) {
+        FFTLIB_b200_tw_gen_c2c(out, n);
+        return FFTLIB_SUCCESS;
+    }
+    float* tmp = new float[2u * (size_t)n];
+    FFTLIB_b200_tw_gen_c2c(tmp, n);
+    cudaError_t e = cudaMemcpy(out, tmp, 2u * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+    delete[] tmp;
+    return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen copy");
+}
+
+FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_init_checkParams(FFTLIB_kernelHandle handle,
+                                                          const FFTLIB_bufParams1D_t* bufParamsX,
+                                                          const FFTLIB_bufParams1D_t* bufParamsW,
+                                                          const FFTLIB_bufParams1D_t* bufParamsY,
+                                                          const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* pKerInitArgs)
+{
+    if (!handle || !bufParamsX || !bufParamsW || !bufParamsY || !pKerInitArgs) return FFTLIB_ERR_NULL_POINTER;
+    if (bufParamsX->data_type != FFTLIB_FLOAT32) return not_float(bufParamsX->data_type);
+    uint32_t x, w, y;
+    const FFTLIB_STATUS st = sizes_f32(pKerInitArgs, &x, &w, &y);
+    if (st != FFTLIB_SUCCESS) return st;
+    if (bufParamsX->dim_x != x || bufParamsY->dim_x != y || bufParamsW->dim_x != w) {
+        set_error("dim_x X/W/Y = %u/%u/%u, expected %u/%u/%u", bufParamsX->dim_x, bufParamsW->dim_x,
+                  bufParamsY->dim_x, x, w, y);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    if (bufParamsW->data_type != bufParamsX->data_type || bufParamsY->data_type != bufParamsX->data_type)
+        return FFTLIB_ERR_INVALID_TYPE;
+    return FFTLIB_SUCCESS;
+}
+
+FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_init(FFTLIB_kernelHandle handle, FFTLIB_bufParams1D_t* bufParamsX,
+                                              FFTLIB_bufParams1D_t* bufParamsW, FFTLIB_bufParams1D_t* bufParamsY,
+                                              const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* pKerInitArgs)
+{
+    if (!handle || !bufParamsX || !pKerInitArgs) return FFTLIB_ERR_NULL_POINTER;
+    (void)bufParamsW;
+    (void)bufParamsY;
+    MmaHandle* m = static_cast<MmaHandle*>(handle);
+    memset(m, 0, sizeof(*m));
+    if (bufParamsX->data_type != FFTLIB_FLOAT32) return not_float(bufParamsX->data_type);
+    uint32_t x, w, y;
+    const FFTLIB_STATUS st = sizes_f32(pKerInitArgs, &x, &w, &y);
+    if (st != FFTLIB_SUCCESS) return st;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    m->init = *pKerInitArgs;
+    m->device = dev;
+    m->path = choose_path(pKerInitArgs);
+    if (m->path == PATH_FFT) {
+        m->plan = get_complex_plan(pKerInitArgs->fftSize, false, &e);
+        if (!m->plan) return cuda_fail(e, "plan creation");
+    }
+    m->magic = kMmaMagic;
+    return FFTLIB_SUCCESS;
+}
+
+FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_exec_checkParams(FFTLIB_kernelHandle handle, const void* pX, const void* pW,
+                                                          const void* pY)
+{
+    (void)handle;
+    if (!pX || !pW || !pY) return FFTLIB_ERR_NULL_POINTER;
+    return FFTLIB_SUCCESS;
+}
+
+FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_exec(FFTLIB_kernelHandle handle, void* pX, void* pW, void* pY)
+{
+    MmaHandle* m = handle_of(handle);
+    if (!m) return FFTLIB_ERR_NULL_POINTER;
+    if (!pX || !pW || !pY) return FFTLIB_ERR_NULL_POINTER;
+    DeviceScope scope(m->device);
+    const uint32_t n = m->init.fftSize;
+    const void* w = pW;
+    if (m->path == PATH_TC) {
+        cudaError_t e = device_table(pW, tc_dft_w_floats(n) * sizeof(float), 2, &w);
+        if (e != cudaSuccess) return cuda_fail(e, "computational matrix copy");
+    }
+    const size_t bytes = (size_t)n * 2u * sizeof(float);
+    std::vector<ChannelBuf> bufs = {{pX, bytes, true, false}, {pY, bytes, false, true}};
+    cudaError_t e = run_channels(bufs, m->init.batchSize,
+                                 [&](const std::vector<void*>& d, uint32_t, uint32_t cnt, cudaStream_t s) {
+                                     return enqueue(m, (const float*)d[0], (const float*)w, (float*)d[1], cnt, s);
+                                 });
+    if (e != cudaSuccess) return cuda_fail(e, "FFT_fft_ixX_cxX_oxX_exec");
+    return FFTLIB_SUCCESS;
+}
+
+FFTLIB_STATUS FFTLIB_b200_FFT_fft_execAsync(FFTLIB_kernelHandle handle, void* pX, void* pW, void* pY, void* stream)
+{
+    MmaHandle* m = handle_of(handle);
+    if (!m) return FFTLIB_ERR_NULL_POINTER;
+    if (!pX || !pW || !pY) return FFTLIB_ERR_NULL_POINTER;
+    if (!is_device_ptr(pX) || !is_device_ptr(pY) || !is_device_ptr(pW)) {
+        set_error("execAsync needs device buffers");
+        return FFTLIB_ERR_INVALID_VALUE;
+    }
+    DeviceScope scope(m->device);
+    const cudaError_t e = enqueue(m, (const float*)pX, (const float*)pW, (float*)pY, m->init.batchSize,
+                                  (cudaStream_t)stream);
+    return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "FFT_fft execAsync");
+}
+
+FFTLIB_STATUS FFTLIB_b200_FFT_fft_sync(void* stream)
+{
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e == cudaSuccess && take_device_error()) e = cudaErrorLaunchTimeout;
+    return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "FFT_fft sync");
+}
+
+int32_t FFTLIB_b200_FFT_fft_path(FFTLIB_kernelHandle handle)
+{
+    const MmaHandle* m = static_cast<const MmaHandle*>(handle);
+    return (m && m->magic == kMmaMagic) ? m->path : PATH_NONE;
+}
+
+} // extern "C"

@@ -1,0 +1,19 @@
+// tc_dft_one.cu -- one-stage tensor-core DFT instantiations (n = 8..64).
+#include "tc_dft.h"
+#include "tc_dft_launch.cuh"
+
+namespace fftb200 {
+
+cudaError_t launch_tc_one(uint32_t n, const float2* x, float2* y, const float* w, uint32_t batch, uint32_t* err,
+                          cudaStream_t s)
+{
+    switch (n) {
+    case 8: return launch_tc_shape<8, 1>(x, y, w, batch, err, s);
+    case 16: return launch_tc_shape<16, 1>(x, y, w, batch, err, s);
+    case 32: return launch_tc_shape<32, 1>(x, y, w, batch, err, s);
+    case 64: return launch_tc_shape<64, 1>(x, y, w, batch, err, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+} // namespace fftb200
