@@ -438,6 +438,36 @@ def cpu_baseline():
             "sample": f"{sample} channels of N={N_POINTS}, median of 3, reference _cn (gcc -O3), one thread per core"}
 
 
+def run_case(args):
+    """W warm-up and K timed launches of one kernel on device buffers; one
+    JSON line with the per-launch time. For profiler captures and sweeps."""
+    import torch
+
+    import c7x_fftlib_b200 as F
+
+    kind, n, batch = args.case.split(":")
+    n, batch = int(n), int(batch)
+    style = {"tc": F.FFTLIB_FUNCTION_OPTIMIZED, "fft": F.FFTLIB_FUNCTION_NATC}[kind]
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.rand(2 * n * batch, device="cuda", generator=g) * 2 - 1
+    y = torch.empty_like(x)
+    d = F.DftMma(n, batch, style)
+    stream = torch.cuda.current_stream()
+    sp = F.ptr(stream.cuda_stream)
+    for _ in range(args.warmup):
+        d.exec_async(x, y, sp)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        d.exec_async(x, y, sp)
+    e1.record(stream)
+    F.check(F.lib().FFTLIB_b200_FFT_fft_sync(sp), "sync")
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"case": args.case, "path": d.path, "ms": round(ms, 5),
+                      "GBps": round(16.0 * n * batch / ms / 1e6, 1)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -446,7 +476,13 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--channels", type=int, default=CHANNELS, help="channels per GPU (default: the workload's 8192)")
     ap.add_argument("--quick", action="store_true", help="time the kernel only (for profiler captures)")
+    ap.add_argument("--case", default=None,
+                    help="time one kernel only, for profiler captures: tc:N:batch (tensor-core DFT), "
+                         "fft:N:batch (CUDA-core FFT through the same coordinator API)")
     args = ap.parse_args()
+    if args.case:
+        run_case(args)
+        return
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         reference_arm(args, world, rank)

@@ -31,7 +31,7 @@ struct MmaHandle {
     int32_t device;
     uint32_t reserved;
     FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs init;
-    ComplexPlan* plan;  // PATH_FFT
+    ComplexPlan* plan;  // CUDA-core FFT plan of fftSize
 };
 
 int32_t choose_path(const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* a)
@@ -82,7 +82,10 @@ MmaHandle* handle_of(FFTLIB_kernelHandle h)
 
 cudaError_t enqueue(const MmaHandle* m, const float* x, const float* w, float* y, uint32_t batch, cudaStream_t s)
 {
-    if (m->path == PATH_TC)
+    // the tensor-core kernels read and prefetch whole 16-byte lines; buffers
+    // that are only 8-byte aligned take the FFT
+    const bool aligned = (((uintptr_t)x | (uintptr_t)y) & 15u) == 0;
+    if (m->path == PATH_TC && aligned)
         return launch_tc_dft(m->init.fftSize, reinterpret_cast<const float2*>(x), reinterpret_cast<float2*>(y), w,
                              batch, error_word().dev, s);
     // above 16384 points the FFT uses pX as four-step scratch, as the
@@ -191,10 +194,10 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_init(FFTLIB_kernelHandle handle, FFTLIB
     m->init = *pKerInitArgs;
     m->device = dev;
     m->path = choose_path(pKerInitArgs);
-    if (m->path == PATH_FFT) {
-        m->plan = get_complex_plan(pKerInitArgs->fftSize, false, &e);
-        if (!m->plan) return cuda_fail(e, "plan creation");
-    }
+    // the FFT plan also serves tensor-core handles called with buffers that
+    // are not 16-byte aligned
+    m->plan = get_complex_plan(pKerInitArgs->fftSize, false, &e);
+    if (!m->plan) return cuda_fail(e, "plan creation");
     m->magic = kMmaMagic;
     return FFTLIB_SUCCESS;
 }

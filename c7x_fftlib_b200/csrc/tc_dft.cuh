@@ -212,7 +212,6 @@ struct TcShape {
     static constexpr int R2 = kDirect ? 128 : T * N1;                    // stage-2 rows
     static constexpr int MB1 = R1 / 128, MB2 = R2 / 128;
     static constexpr int K1 = 2 * N1, K2 = 2 * N2;  // GEMM K (= output columns) per stage
-    static constexpr int NB = 2;
     static constexpr int LW = 8, XW = kDirect ? 0 : 8, EW = kDirect ? 8 : 4;
     static constexpr int MMA_WARP = LW + XW + EW;
     static constexpr int THREADS = 32 * (MMA_WARP + 1);
@@ -225,10 +224,20 @@ struct TcShape {
     static constexpr uint32_t TILE = 2 * HALF_TILE;
     static constexpr uint32_t W1_HALF = LW1::BYTES;
     static constexpr uint32_t W2_HALF = kSharedW ? 0u : LW2::BYTES;
+    static constexpr uint32_t D1_COLS = MB1 * K1, D2_COLS = kDirect ? 0 : MB2 * K2;
+    // one-stage epilogue staging: per warp 32 rows x 16 columns, rows padded to 80 bytes
+    static constexpr uint32_t STAGE_BYTES = kDirect ? (uint32_t)EW * 32u * 80u : 0u;
+    // tile buffers: as many as shared memory (about 200 KB for tiles and
+    // matrices) and tensor memory (512 columns) allow, between 2 and 8
+    static constexpr int NB_SMEM = (int)((200u * 1024u - 2u * (W1_HALF + W2_HALF) - STAGE_BYTES) / TILE);
+    static constexpr int NB_TMEM = (int)(512u / (D1_COLS + D2_COLS));
+    static constexpr int NB_MAX = NB_SMEM < NB_TMEM ? NB_SMEM : NB_TMEM;
+    static constexpr int NB = NB_MAX > 8 ? 8 : (NB_MAX < 2 ? 2 : NB_MAX);
     static constexpr int TABA = kDirect ? 0 : N / 64 + 1, TABB = kDirect ? 0 : 64;
     static constexpr uint32_t OFF_W1 = NB * TILE;
     static constexpr uint32_t OFF_W2 = OFF_W1 + 2 * W1_HALF;
-    static constexpr uint32_t OFF_TAB = OFF_W2 + 2 * W2_HALF;
+    static constexpr uint32_t OFF_STAGE = OFF_W2 + 2 * W2_HALF;
+    static constexpr uint32_t OFF_TAB = OFF_STAGE + STAGE_BYTES;
     static constexpr uint32_t OFF_S1 = OFF_TAB + 8u * (TABA + TABB);
     static constexpr uint32_t OFF_S2 = OFF_S1 + 4u * 2 * NB * R1;
     static constexpr uint32_t OFF_PART = OFF_S2 + 4u * 2 * NB * T;
@@ -237,7 +246,6 @@ struct TcShape {
     static constexpr int NBARS = 6 * NB + 1;
     static constexpr uint32_t OFF_MISC = OFF_BAR + 8u * NBARS;
     static constexpr uint32_t SMEM = OFF_MISC + 16u + 1024u;  // + slack to align the base to 1024
-    static constexpr uint32_t D1_COLS = MB1 * K1, D2_COLS = kDirect ? 0 : MB2 * K2;
     static constexpr uint32_t TMEM_USED = NB * (D1_COLS + D2_COLS);
     static constexpr uint32_t TMEM_COLS =
         TMEM_USED <= 32 ? 32 : TMEM_USED <= 64 ? 64 : TMEM_USED <= 128 ? 128 : TMEM_USED <= 256 ? 256 : 512;
@@ -368,8 +376,20 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
     if (warp < S::LW) {
         // ================= loaders: HBM -> scale -> hi/lo operand =================
         const int j = threadIdx.x;  // 0..255
+        // the next tile's input (contiguous) is pulled into L2 while this one
+        // is converted, so its loads do not wait a full HBM latency
+        auto prefetch = [&](uint32_t tl) {
+            if (j != 0 || tl >= numTiles) return;
+            const uint32_t first = tl * (uint32_t)T;
+            const uint32_t cnt = min((uint32_t)T, batch - first);
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(x + (size_t)first * N),
+                         "r"(cnt * (uint32_t)N * 8u)
+                         : "memory");
+        };
+        prefetch(blockIdx.x);
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
+            prefetch(tile + gridDim.x);
             const int b = (int)(i % NB);
             const uint32_t u = i / NB, slot = i % (2 * NB);
             unsigned char* hiB = sm + b * S::TILE;
@@ -507,6 +527,7 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
             const int q = warp & 3, ch = (warp - S::LW) >> 2;
             constexpr int HC = S::K1 / 2;  // accumulator columns per half
             constexpr int CW = HC >= 16 ? 16 : 8;
+            constexpr int SEG = N2 < 32 ? N2 : 32;
             const uint32_t laneBase = (uint32_t)(32 * q) << 16;
             uint32_t i = 0;
             for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
@@ -533,16 +554,31 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
                         for (int e = 0; e < CW; ++e) pm = fmaxf(pm, fabsf(f[e]));
                     }
                     const int eRaw = (int)((__float_as_uint(pm) >> 23) & 0xFFu);
-                    part[ch * S::R1 + row] = pm > 0.f ? eRaw - s1ring[slot * S::R1 + row] : -100000;
+                    int ez = pm > 0.f ? eRaw - s1ring[slot * S::R1 + row] : -100000;
+                    // rows of one transform are SEG-lane segments of the warp
+#pragma unroll
+                    for (int o = SEG / 2; o >= 1; o >>= 1) ez = max(ez, __shfl_xor_sync(0xffffffffu, ez, o));
+                    if ((lane & (SEG - 1)) == 0) part[ch * (S::R1 / SEG) + row / SEG] = ez;
                 }
                 group_sync(2, 32 * S::XW);
                 for (int tt = xt; tt < T; tt += 32 * S::XW) {
                     int E = -100000;
-                    for (int rr = tt * N2; rr < (tt + 1) * N2; ++rr) E = max(E, max(part[rr], part[S::R1 + rr]));
+#pragma unroll
+                    for (int sg = 0; sg < N2 / SEG; ++sg) {
+                        const int id = tt * (N2 / SEG) + sg;
+                        E = max(E, max(part[id], part[S::R1 / SEG + id]));
+                    }
                     s2ring[slot * T + tt] = E < -50000 ? 0 : clampi(141 - E + kTcWShift, -100, 100);
                 }
                 group_sync(2, 32 * S::XW);
-                // pass 2: rescale, twiddle, split, write transposed
+                // pass 2: rescale, twiddle, split, write transposed. Row r2 =
+                // t N1 + k1 of the stage-2 operand gets (re, im) of Z' at K
+                // position 2 n2. Within a group of 8 consecutive k1 (r2 = 8j+e)
+                // the swizzle term is a constant of e, and the twiddles
+                // W_N^(n2 k1) follow from one table product by the
+                // recurrence w <- w W_N^n2 (the power-of-two rescale rides on
+                // the first factor).
+                using L2 = typename S::L2;
                 unsigned char* hiB = sm + b * S::TILE;
                 unsigned char* loB = hiB + S::HALF_TILE;
 #pragma unroll
@@ -551,7 +587,10 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
                     const int t = row / N2, n2 = row % N2;
                     const int s2 = s2ring[slot * T + t];
                     const float f = exp2i(clampi(s2 - s1ring[slot * S::R1 + row] - kTcWShift, -126, 126));
-                    const uint32_t kb = (uint32_t)(n2 & 3) * 4u;
+                    const float2 step = tabB[n2];  // W_N^n2 (n2 < 64)
+                    const uint32_t kbytes = (uint32_t)(n2 >> 2) * 16u;
+                    const uint32_t colOff = kbytes % L2::W;
+                    const uint32_t rowOff = (kbytes / L2::W) * L2::REGION + (uint32_t)(n2 & 3) * 4u;
 #pragma unroll
                     for (int c0 = 0; c0 < HC; c0 += CW) {
                         float v[CW];
@@ -559,16 +598,23 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
                             tmem_ld16(dcol + m * S::K1 + ch * HC + c0, v);
                         else
                             tmem_ld8(dcol + m * S::K1 + ch * HC + c0, v);
+                        const int kbase = (ch * HC + c0) / 2;  // multiple of 8
+                        const int ex = n2 * kbase;
+                        const float2 ta = tabA[ex >> 6], tb = tabB[ex & 63];
+                        float wr = (ta.x * tb.x - ta.y * tb.y) * f, wi = (ta.x * tb.y + ta.y * tb.x) * f;
+                        const uint32_t base = rowOff + (uint32_t)(t * N1 + kbase) * L2::W;
 #pragma unroll
                         for (int e = 0; e < CW / 2; ++e) {
-                            const int k1 = (ch * HC + c0) / 2 + e;
-                            const int ex = n2 * k1;
-                            const float2 ta = tabA[ex >> 6], tb = tabB[ex & 63];
-                            const float wr = ta.x * tb.x - ta.y * tb.y, wi = ta.x * tb.y + ta.y * tb.x;
-                            const float zr = v[2 * e] * f, zi = v[2 * e + 1] * f;
+                            if (e > 0) {
+                                const float nr = wr * step.x - wi * step.y;
+                                wi = wr * step.y + wi * step.x;
+                                wr = nr;
+                            }
+                            const float zr = v[2 * e], zi = v[2 * e + 1];
                             uint32_t hh, ll;
                             split2(zr * wr - zi * wi, zr * wi + zi * wr, hh, ll);
-                            const uint32_t off = S::L2::chunk(t * N1 + k1, n2 >> 2) + kb;
+                            const uint32_t swz = ((((uint32_t)e * L2::W) >> 7) & L2::MASK) << 4;
+                            const uint32_t off = base + (uint32_t)e * L2::W + (colOff ^ swz);
                             *reinterpret_cast<uint32_t*>(hiB + off) = hh;
                             *reinterpret_cast<uint32_t*>(loB + off) = ll;
                         }
@@ -599,13 +645,19 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
             if (group_sync_or(3, 32 * S::EW, bad)) break;
             tc_fence_after();
             if constexpr (S::kDirect) {
+                // each warp owns 32 rows (transforms) x half the columns; a
+                // 16-column slice goes TMEM -> registers -> a padded staging
+                // tile -> HBM with 4 lanes per row (64-byte runs)
                 const int ch = (warp - S::LW) >> 2;
                 constexpr int HC = S::K1 / 2;
                 constexpr int CW = HC >= 16 ? 16 : 8;
+                constexpr int LPR = CW / 4;      // lanes per row on the way out
+                constexpr int RPI = 32 / LPR;    // rows per store instruction
                 const int r = 32 * q + lane;
-                const uint32_t gt = tile * 128u + (uint32_t)r;
                 const float f = exp2i(-(s1ring[slot * S::R1 + r] + kTcWShift));
                 const uint32_t dcol = tmem + laneBase + b * S::D1_COLS + ch * HC;
+                float* stg = reinterpret_cast<float*>(sm + S::OFF_STAGE) + (warp - S::LW) * (32 * 20);
+                const int pr = lane / LPR, pc = lane % LPR;
 #pragma unroll
                 for (int c0 = 0; c0 < HC; c0 += CW) {
                     float v[CW];
@@ -613,12 +665,20 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
                         tmem_ld16(dcol + c0, v);
                     else
                         tmem_ld8(dcol + c0, v);
-                    if (gt < batch) {
-                        float4* dst = reinterpret_cast<float4*>(y + (size_t)gt * N1 + (ch * HC + c0) / 2);
 #pragma unroll
-                        for (int e = 0; e < CW / 4; ++e)
-                            dst[e] = make_float4(v[4 * e] * f, v[4 * e + 1] * f, v[4 * e + 2] * f, v[4 * e + 3] * f);
+                    for (int e = 0; e < CW / 4; ++e)
+                        *reinterpret_cast<float4*>(stg + lane * 20 + 4 * e) =
+                            make_float4(v[4 * e] * f, v[4 * e + 1] * f, v[4 * e + 2] * f, v[4 * e + 3] * f);
+                    __syncwarp();
+#pragma unroll
+                    for (int it = 0; it < 32 / RPI; ++it) {
+                        const int rr = it * RPI + pr;
+                        const uint32_t gt = tile * 128u + (uint32_t)(32 * q + rr);
+                        const float4 o = *reinterpret_cast<const float4*>(stg + rr * 20 + 4 * pc);
+                        if (gt < batch)
+                            *reinterpret_cast<float4*>(y + (size_t)gt * N1 + (ch * HC + c0) / 2 + 2 * pc) = o;
                     }
+                    __syncwarp();
                 }
             } else {
                 constexpr int CW = S::K2 >= 16 ? 16 : 8;

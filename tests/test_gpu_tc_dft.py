@@ -161,3 +161,19 @@ def test_tc_dft_large_batch_properties():
     pa = (ya.double() ** 2).view(batch, -1).sum(1) / n
     pt = (a.double() ** 2).view(batch, -1).sum(1)
     assert float(((pa - pt).abs() / pt).max()) <= 4e-6
+
+
+def test_tc_handle_with_8_byte_aligned_buffers(oracle_mod):
+    """Buffers that are 8- but not 16-byte aligned are transformed correctly
+    (they take the CUDA-core FFT inside the same handle)."""
+    import torch
+
+    O = oracle_mod
+    n, batch = 64, 100
+    x = O.uniform_c2c(n, batch, seed=4)
+    d = F.DftMma(n, batch)
+    X = torch.zeros(2 * n * batch + 2, device="cuda")
+    Y = torch.zeros_like(X)
+    X[2:] = torch.from_numpy(x).cuda()
+    d.exec(X[2:], Y[2:])
+    assert O.rel_l2(Y[2:].cpu().numpy(), O.fp64_c2c(x, n, batch)) <= TOL
