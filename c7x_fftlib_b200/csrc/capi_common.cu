@@ -170,9 +170,10 @@ cudaError_t device_table(const void* p, size_t bytes, int slot, const void** out
         *out = p;
         return cudaSuccess;
     }
+    if (slot < 0 || slot >= kTableSlots) return cudaErrorInvalidValue;
     struct Tab {
-        void* ptr[2] = {nullptr, nullptr};
-        size_t cap[2] = {0, 0};
+        void* ptr[kTableSlots] = {};
+        size_t cap[kTableSlots] = {};
         int dev = -1;
     };
     thread_local Tab tabs[8];

@@ -65,7 +65,8 @@ cudaError_t run_channels(std::vector<ChannelBuf>& bufs, uint32_t channels, const
 
 // Device copy of a small host table (twiddles, shift vector), copied
 // synchronously and valid until the next call on this thread with the same
-// slot; device pointers are returned unchanged.
+// slot (0 <= slot < kTableSlots); device pointers are returned unchanged.
+constexpr int kTableSlots = 4;
 cudaError_t device_table(const void* p, size_t bytes, int slot, const void** out);
 
 } // namespace fftb200

@@ -83,10 +83,17 @@ cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
 {
     if (a.batch == 0) return cudaSuccess;
     if (const StaticEntry* st = find_static(a, emax)) {
-        const bool pipelinable = st->launchPipelined && a.err && a.M == 1 && a.ioMode == IO_C2C && !a.staged &&
-                                 !a.batchMinor && !a.twBig && a.inElem == 1 && a.outElem == 1 &&
-                                 a.inBatch == (int64_t)a.N && ((uintptr_t)a.in & 15u) == 0 && (a.N % 2u) == 0;
-        return pipelinable ? st->launchPipelined(a, s) : st->launch(a, s);
+        // the pipelined kernel brings whole tiles in with bulk copies, so the
+        // static kernel's staged I/O (for transforms of few threads) is moot
+        const bool pipelinable = st->launchPipelined && a.err && a.ioMode == IO_C2C && !a.batchMinor && !a.twBig &&
+                                 a.inElem == 1 && a.outElem == 1 && a.inBatch == (int64_t)a.N &&
+                                 ((uintptr_t)a.in & 15u) == 0 && (a.N % 2u) == 0;
+        if (pipelinable) {
+            FftArgs b = a;
+            b.staged = 0;
+            return st->launchPipelined(b, s);
+        }
+        return st->launch(a, s);
     }
     switch (emax) {
     case 8: return launch_generic<8, 1024>(a, s);

@@ -83,45 +83,55 @@ FFT_DEV void fence_mbarrier_init() { asm volatile("fence.mbarrier_init.release.c
 // transform, rounded to an even count so every stage starts 16-byte aligned.
 __host__ __device__ constexpr uint32_t pipe_stage_len(uint32_t n) { return (smem_len(n) + 1u) & ~1u; }
 
-// Shared-memory bytes of the pipelined kernel (one transform per tile).
-__host__ __device__ constexpr size_t pipe_smem_bytes(uint32_t n, int stages)
+// Shared-memory bytes of the pipelined kernel (m transforms per tile).
+__host__ __device__ constexpr size_t pipe_smem_bytes(uint32_t n, int stages, int m = 1)
 {
-    return (size_t)stages * pipe_stage_len(n) * 8u + 8u * (size_t)stages + 16u;
+    return (size_t)stages * (size_t)m * pipe_stage_len(n) * 8u + 8u * (size_t)stages + 16u;
 }
+
+// Transforms per tile: enough to give the CTA 256 threads for short
+// transforms, one for transforms of 128 threads or more.
+__host__ __device__ constexpr int pipe_tile(int t) { return t >= 128 ? 1 : (256 / t < 1 ? 1 : 256 / t); }
 
 // CTAs per SM the kernel is compiled for: as many as the shared memory
-// (228 KB per SM, 1 KB reserved per CTA) and 2048 threads allow, at most 4.
-__host__ __device__ constexpr int pipe_min_blocks(uint32_t n, int t, int stages)
+// (228 KB per SM, 1 KB reserved per CTA) and 2048 threads allow, at most 8.
+__host__ __device__ constexpr int pipe_min_blocks(uint32_t n, int threads, int stages, int m = 1)
 {
-    const int bySmem = (int)((228u * 1024u) / (pipe_smem_bytes(n, stages) + 1024u));
-    const int byThreads = 2048 / t;
+    const int bySmem = (int)((228u * 1024u) / (pipe_smem_bytes(n, stages, m) + 1024u));
+    const int byThreads = 2048 / threads;
     const int b = bySmem < byThreads ? bySmem : byThreads;
-    return b < 1 ? 1 : (b > 4 ? 4 : b);
+    return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
 
-// The transform is exchanged in place in its own stage: the bulk copy lands
-// the input unpadded at the start of the stage, the first pass reads it from
-// there and (after a barrier) writes its outputs back in the padded layout,
-// and so on; the stage is refilled once the last pass has read it.
-template <class S, int STAGES>
+// A tile is M consecutive transforms. One bulk copy lands their inputs,
+// unpadded and back to back, at the start of the stage; the first pass of
+// transform m reads its input from there and (after the CTA-wide barrier
+// inside the pass, when every input has been read) writes its outputs in the
+// padded layout at m * SL, and so on; the stage is refilled once the first
+// pass has read it.
+template <class S, int STAGES, int M>
 FFT_DEV void fft_pipeline(const FftArgs& a)
 {
     static_assert(S::P >= 2, "the pipelined kernel needs at least two passes");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr uint32_t N = (uint32_t)S::N;
     constexpr uint32_t SL = pipe_stage_len(N);
+    constexpr uint32_t STL = (uint32_t)M * SL;
     float2* stages = (float2*)smem_raw;
-    uint64_t* bar = (uint64_t*)(stages + (size_t)STAGES * SL);
+    uint64_t* bar = (uint64_t*)(stages + (size_t)STAGES * STL);
     __shared__ uint32_t s_fail;
 
     const uint32_t tid = threadIdx.x;
-    const uint32_t t = tid;
-    const uint32_t tiles = a.batch;
+    const uint32_t m = tid / (uint32_t)S::T;
+    const uint32_t t = tid - m * (uint32_t)S::T;
+    const uint32_t tiles = (a.batch + (uint32_t)M - 1u) / (uint32_t)M;
     const uint32_t G = gridDim.x;
 
     auto issue = [&](uint32_t tile, int s) {
-        mbar_expect_tx(&bar[s], N * 8u);
-        bulk_copy_g2s(stages + (size_t)s * SL, a.in + (size_t)tile * N, N * 8u, &bar[s]);
+        const uint32_t first = tile * (uint32_t)M;
+        const uint32_t count = min((uint32_t)M, a.batch - first);
+        mbar_expect_tx(&bar[s], count * N * 8u);
+        bulk_copy_g2s(stages + (size_t)s * STL, a.in + (size_t)first * N, count * N * 8u, &bar[s]);
     };
 
     if (tid == 0) {
@@ -147,10 +157,12 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
         __syncthreads();
         if (s_fail) break;
 
-        float2* st = stages + (size_t)s * SL;
-        // once every thread has read this transform's input (the barrier
-        // inside pass 0), the previous transform's stage is free: refill it
-        // with the tile STAGES-1 iterations ahead
+        float2* st = stages + (size_t)s * STL;
+        const uint32_t gidx = tile * (uint32_t)M + m;
+        const bool active = gidx < a.batch;
+        // once every thread has read this tile's inputs (the barrier inside
+        // pass 0), the previous tile's stage is free: refill it with the
+        // tile STAGES-1 iterations ahead
         auto refill = [&]() {
             if (tid == 0 && it > 0) {
                 fence_proxy_async_smem();
@@ -158,16 +170,16 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
                 if (next < tiles) issue(next, (int)((it - 1) % STAGES));
             }
         };
+        float2* rowOut = a.out + (size_t)gidx * (size_t)a.outBatch;
         static_for<S::P>([&](auto p) {
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
-            float2* rowOut = a.out + (size_t)tile * N;
             if constexpr (P == 0) {
-                run_pass<S::EMAX, S::R[P]>(a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true,
-                                           nullptr, rowOut, st, refill);
+                run_pass<S::EMAX, S::R[P]>(a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, gidx,
+                                           active, nullptr, rowOut, st + m * N, refill);
             } else {
-                run_pass<S::EMAX, S::R[P]>(a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st, t, tile, true,
-                                           nullptr, rowOut);
+                run_pass<S::EMAX, S::R[P]>(a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, gidx,
+                                           active, nullptr, rowOut);
             }
         });
     }

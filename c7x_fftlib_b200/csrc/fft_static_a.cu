@@ -7,7 +7,7 @@ void register_static_a(std::vector<StaticEntry>& out)
 {
     out.push_back(static_entry<StaticSchedule<4096, 16, 256, 16, 16, 16>>());
     out.push_back(static_entry<StaticSchedule<2048, 16, 128, 16, 16, 8>>());
-    out.push_back(static_entry<StaticSchedule<1024, 32, 32, 32, 32>>());
+    out.push_back(static_entry<StaticSchedule<1024, 16, 64, 16, 16, 4>>());
     out.push_back(static_entry<StaticSchedule<256, 16, 16, 16, 16>>());
 }
 

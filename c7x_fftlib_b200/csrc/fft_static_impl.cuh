@@ -46,18 +46,20 @@ cudaError_t launch_static(const FftArgs& a, cudaStream_t s)
 }
 
 template <class S, int STAGES>
-__global__ void __launch_bounds__(S::T, pipe_min_blocks(S::N, S::T, STAGES)) k_fft_pipe(const __grid_constant__ FftArgs a)
+__global__ void __launch_bounds__(S::T * pipe_tile(S::T), pipe_min_blocks(S::N, S::T * pipe_tile(S::T), STAGES, pipe_tile(S::T)))
+    k_fft_pipe(const __grid_constant__ FftArgs a)
 {
-    fft_pipeline<S, STAGES>(a);
+    fft_pipeline<S, STAGES, pipe_tile(S::T)>(a);
 }
 
-// Persistent pipelined launch (one transform per tile): as many CTAs as are
-// resident on the device.
+// Persistent pipelined launch (pipe_tile(T) transforms per tile): as many
+// CTAs as are resident on the device.
 template <class S, int STAGES>
 cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
 {
-    if (a.M != 1 || a.T != (uint32_t)S::T) return cudaErrorInvalidConfiguration;
-    const size_t smem = pipe_smem_bytes((uint32_t)S::N, STAGES);
+    constexpr int M = pipe_tile(S::T);
+    if (a.T != (uint32_t)S::T) return cudaErrorInvalidConfiguration;
+    const size_t smem = pipe_smem_bytes((uint32_t)S::N, STAGES, M);
     struct Cfg {
         int blocks = -1;
         int sms = 0;
@@ -74,7 +76,7 @@ cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
         if (c.blocks < 0) {
             e = cudaFuncSetAttribute(k_fft_pipe<S, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.blocks, k_fft_pipe<S, STAGES>, S::T, smem);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.blocks, k_fft_pipe<S, STAGES>, S::T * M, smem);
             if (e != cudaSuccess) return e;
             e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev);
             if (e != cudaSuccess) return e;
@@ -82,8 +84,9 @@ cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
         resident = c.blocks;
         sms = c.sms;
     }
-    const uint32_t grid = std::min<uint32_t>(a.batch, (uint32_t)std::max(1, resident * sms));
-    k_fft_pipe<S, STAGES><<<grid, S::T, smem, s>>>(a);
+    const uint32_t tiles = (a.batch + (uint32_t)M - 1u) / (uint32_t)M;
+    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)std::max(1, resident * sms));
+    k_fft_pipe<S, STAGES><<<grid, S::T * M, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -100,7 +103,7 @@ StaticEntry static_entry()
     e.maxThreads = maxt;
     e.launch = &launch_static<S, maxt>;
     // the stage ring and exchange buffer must fit one CTA's shared memory
-    if constexpr (S::P >= 2 && S::T >= 64 && (S::N % 2) == 0 && pipe_smem_bytes(S::N, 2) <= 227u * 1024u) {
+    if constexpr (S::P >= 2 && (S::N % 2) == 0 && pipe_smem_bytes(S::N, 2, pipe_tile(S::T)) <= 227u * 1024u) {
         e.launchPipelined = &launch_pipe<S, 2>;
     } else {
         e.launchPipelined = nullptr;

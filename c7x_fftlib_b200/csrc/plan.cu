@@ -70,7 +70,10 @@ bool evaluate(uint32_t n, const int* seq, int len, int emax, EnginePlan* e)
         const double util = (double)nb / (double)(T * b);
         score += 1.0 + 0.5 * (1.0 / util - 1.0);
     }
-    score += emax == 32 ? 0.5 : emax == 16 ? 0.15 : 0.0;
+    // measured on B200: the 32-wide engine (90-115 registers per thread)
+    // runs at about a third of the 16-wide one's throughput, so it is kept
+    // for lengths nothing narrower can plan
+    score += emax == 32 ? 2.5 : emax == 16 ? 0.15 : 0.0;
     e->n = n;
     e->emax = emax;
     e->T = T;
