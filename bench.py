@@ -58,6 +58,15 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def measured_peaks():
+    """The driver-measured peaks (hbm_gbs, bf16_tflops, ...) or {}."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
 def traffic_from_profile(kernel_tag):
     """Per-launch DRAM bytes of the kernel from the committed ncu summary
     (lines 'traffic <tag> <bytes>'), or None."""
@@ -422,7 +431,65 @@ def secondary_configs(args):
                           "speedup_vs_per_length_api": round(ms_api / ms_graph, 3),
                           "transforms_per_s": round(20000 / ms_graph * 1e3, 1)}
     mb.close()
+    res["tc_dft"] = tc_dft_configs(args, steps)
     return res
+
+
+def tc_flops(n: int) -> float:
+    """Executed tensor-core FLOPs of one split-precision DFT of length n:
+    3 FP16 products of the real-embedding GEMMs (one stage: rows x 2n x 2n;
+    two stages n = n1 n2: n2 rows x (2 n1)^2 then n1 rows x (2 n2)^2)."""
+    import c7x_fftlib_b200 as F  # noqa: F401
+
+    two = {128: (16, 8), 256: (16, 16), 512: (32, 16), 1024: (32, 32), 2048: (64, 32), 4096: (64, 64)}
+    if n in two:
+        n1, n2 = two[n]
+        return 3.0 * (2.0 * n2 * (2 * n1) ** 2 + 2.0 * n1 * (2 * n2) ** 2)
+    return 3.0 * 2.0 * (2 * n) ** 2
+
+
+def tc_dft_configs(args, steps):
+    """Split-FP16 tensor-core DFT (the fft_c7xmma coordinator, funcStyle
+    OPTIMIZED) against the CUDA-core FP32 FFT (funcStyle NATC) on the same
+    inputs: 2^20 rows for n = 16..256 and n = 4096 x 8192. Relative L2 error
+    of sampled rows against numpy's FP64 FFT."""
+    import numpy as np
+    import torch
+
+    import c7x_fftlib_b200 as F
+
+    peaks = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs") or 6650.0)
+    tfl = float(peaks.get("bf16_tflops") or 1590.0)  # dense FP16 runs at the BF16 rate
+    stream = torch.cuda.Stream()
+    sp = F.ptr(stream.cuda_stream)
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(5)
+    for n, batch in [(16, 1 << 20), (32, 1 << 20), (64, 1 << 20), (128, 1 << 20), (256, 1 << 20), (4096, 8192)]:
+        x = torch.rand(2 * n * batch, device="cuda", generator=g) * 2 - 1
+        y = torch.empty_like(x)
+        yf = torch.empty_like(x)
+        tc = F.DftMma(n, batch, F.FFTLIB_FUNCTION_OPTIMIZED)
+        ff = F.DftMma(n, batch, F.FFTLIB_FUNCTION_NATC)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            ms_tc = _time_launches(torch, stream, lambda: tc.exec_async(x, y, sp), steps)
+        ms_ff = _time_launches(torch, stream, lambda: ff.exec_async(x, yf, sp), steps)
+        F.check(F.lib().FFTLIB_b200_FFT_fft_sync(sp), "sync")
+        rows = np.random.default_rng(n).choice(batch, size=min(batch, 256), replace=False)
+        xs = x.view(batch, 2 * n)[torch.from_numpy(rows).cuda()].cpu().numpy().astype(np.float64)
+        ys = y.view(batch, 2 * n)[torch.from_numpy(rows).cuda()].cpu().numpy().astype(np.float64)
+        want = np.fft.fft(xs[:, 0::2] + 1j * xs[:, 1::2], axis=1)
+        rel = float(np.linalg.norm(ys[:, 0::2] + 1j * ys[:, 1::2] - want) / np.linalg.norm(want))
+        gbs = 16.0 * n * batch / ms_tc / 1e6
+        tfs = tc_flops(n) * batch / ms_tc / 1e9
+        out[str(n)] = {"rows": batch, "tc_ms": round(ms_tc, 4), "tc_GBps": round(gbs, 1),
+                       "tc_hbm_frac": round(gbs / hbm, 3), "tc_tensor_TFLOPs": round(tfs, 1),
+                       "tc_tensor_frac": round(tfs / tfl, 3),
+                       "fft_ms": round(ms_ff, 4), "fft_GBps": round(16.0 * n * batch / ms_ff / 1e6, 1),
+                       "tc_speedup_vs_fft": round(ms_ff / ms_tc, 3), "tc_rel_l2_vs_fp64": rel,
+                       "tc_clocks": clk.summary()}
+        del x, y, yf
+    return out
 
 
 def cpu_baseline():
@@ -440,32 +507,85 @@ def cpu_baseline():
 
 def run_case(args):
     """W warm-up and K timed launches of one kernel on device buffers; one
-    JSON line with the per-launch time. For profiler captures and sweeps."""
+    JSON line with the per-launch time. For profiler captures and sweeps.
+    Cases: tc:N:rows (tensor-core DFT), fft:N:rows (CUDA-core FFT through the
+    coordinator), c2c:N:channels, r2c:N:channels, c2r:N:channels,
+    i16:N:channels (fft1dBatched kernels)."""
+    import numpy as np
     import torch
 
     import c7x_fftlib_b200 as F
 
     kind, n, batch = args.case.split(":")
     n, batch = int(n), int(batch)
-    style = {"tc": F.FFTLIB_FUNCTION_OPTIMIZED, "fft": F.FFTLIB_FUNCTION_NATC}[kind]
     g = torch.Generator(device="cuda").manual_seed(1)
-    x = torch.rand(2 * n * batch, device="cuda", generator=g) * 2 - 1
-    y = torch.empty_like(x)
-    d = F.DftMma(n, batch, style)
     stream = torch.cuda.current_stream()
     sp = F.ptr(stream.cuda_stream)
+    nbytes = 16.0 * n * batch
+    if kind in ("tc", "fft"):
+        style = {"tc": F.FFTLIB_FUNCTION_OPTIMIZED, "fft": F.FFTLIB_FUNCTION_NATC}[kind]
+        x = torch.rand(2 * n * batch, device="cuda", generator=g) * 2 - 1
+        y = torch.empty_like(x)
+        d = F.DftMma(n, batch, style)
+
+        def launch():
+            d.exec_async(x, y, sp)
+    elif kind == "c2c":
+        x = torch.rand(2 * n * batch, device="cuda", generator=g) * 2 - 1
+        y = torch.empty_like(x)
+        pb = F.pblock("c2c")
+        bb = F.bp(F.FFTLIB_FLOAT32, 2 * n * batch)
+        F.check(F.fn(F.KERNELS["c2c"] + "_init")(F.ptr(x), bb, F.ptr(x), F.bp(F.FFTLIB_FLOAT32, 2 * n), F.ptr(y),
+                                                 bb, n, batch, pb))
+        k = F.fn("FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync")
+
+        def launch():
+            k(F.ptr(x), F.ptr(y), n, batch, pb, sp)
+    elif kind in ("r2c", "c2r"):
+        nb = 4 * n + 8 * (n // 2 + 1)
+        nbytes = float(nb) * batch
+        xr = torch.randn(n * batch, device="cuda", generator=g)
+        yc = torch.randn(2 * (n // 2 + 1) * batch, device="cuda", generator=g)
+        b = F.bp(F.FFTLIB_FLOAT32, n * batch)
+        pb = F.pblock(kind)
+        src, dst = (xr, yc) if kind == "r2c" else (yc, xr)
+        F.check(F.fn(F.KERNELS[kind] + "_init")(F.ptr(src), b, F.ptr(src), b, None, b, F.ptr(src), b, F.ptr(dst), b,
+                                                n, batch, 0, pb))
+        k = F.fn("FFTLIB_b200_fft1dBatched_i32f_c32fc_o32fc_kernelAsync" if kind == "r2c"
+                 else "FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32f_kernelAsync")
+
+        def launch():
+            k(F.ptr(src), None, F.ptr(dst), n, batch, 0, pb, sp)
+    elif kind == "i16":
+        nbytes = 8.0 * n * batch
+        x = torch.randint(-2048, 2048, (2 * n * batch,), device="cuda", dtype=torch.int16, generator=g)
+        y = torch.empty_like(x)
+        w = np.zeros(2 * n, np.int16)
+        F.lib().FFTLIB_b200_tw_gen_i16(F.ptr(w), n)
+        wd = torch.from_numpy(w).cuda()
+        ns = max(1, (n.bit_length() - 1 + 1) // 2)
+        sh = torch.full((ns,), 2, dtype=torch.int32, device="cuda")
+        bx = F.bp(F.FFTLIB_INT16, 2 * n * batch)
+        pb = F.pblock("i16")
+        F.check(F.fn(F.KERNELS["i16"] + "_init")(F.ptr(x), bx, F.ptr(wd), F.bp(F.FFTLIB_INT16, 2 * n), F.ptr(y), bx,
+                                                 F.ptr(sh), F.bp(F.FFTLIB_UINT32, ns), n, batch, pb))
+        k = F.fn("FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync")
+
+        def launch():
+            k(F.ptr(x), F.ptr(wd), F.ptr(y), F.ptr(sh), ns, n, batch, pb, sp)
+    else:
+        raise SystemExit(f"unknown case kind {kind}")
     for _ in range(args.warmup):
-        d.exec_async(x, y, sp)
+        launch()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        d.exec_async(x, y, sp)
+        launch()
     e1.record(stream)
-    F.check(F.lib().FFTLIB_b200_FFT_fft_sync(sp), "sync")
+    torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    print(json.dumps({"case": args.case, "path": d.path, "ms": round(ms, 5),
-                      "GBps": round(16.0 * n * batch / ms / 1e6, 1)}))
+    print(json.dumps({"case": args.case, "ms": round(ms, 5), "GBps": round(nbytes / ms / 1e6, 1)}))
 
 
 def main():

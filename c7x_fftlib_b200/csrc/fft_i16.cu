@@ -25,13 +25,25 @@ namespace fftb200 {
 
 __device__ __forceinline__ int16_t wrap16(int v) { return (int16_t)(uint16_t)(unsigned)v; }
 
-// ((x + 0x4000) << 1) clamped to [-2^31, 0x7FFF0000], then >> 16.
-__device__ __forceinline__ int16_t q15_scale(long long x)
+// Q15 product with the reference's rounding and saturation: x = a*b +/- c*d
+// formed exactly, then ((x + 0x4000) << 1) clamped to [-2^31, 0x7FFF0000]
+// and shifted right by 16, which equals clamp((x + 0x4000) >> 15) to
+// [-32768, 32767] ((2u) >> 16 == u >> 15 with floor semantics, and the clamp
+// bounds map onto each other). Products of int16 values lie in
+// [-(2^30 - 2^15), 2^30], and 2^30 only for (-32768)^2, so a difference
+// always fits in int32 and a sum does too except for 2^31 exactly (all four
+// factors -32768), which wraps to INT_MIN and saturates to 32767. Elsewhere
+// |x| <= 2^31 - 2^15, so x + 0x4000 cannot overflow.
+__device__ __forceinline__ int16_t q15_round(int x)
 {
-    long long t = (x + 0x4000LL) * 2LL;
-    t = t > 0x7FFF0000LL ? 0x7FFF0000LL : t;
-    t = t < -0x80000000LL ? -0x80000000LL : t;
-    return (int16_t)(t >> 16);
+    const int u = (x + 0x4000) >> 15;
+    return (int16_t)max(-32768, min(32767, u));
+}
+__device__ __forceinline__ int16_t q15_dot_sub(int a, int b, int c, int d) { return q15_round(a * b - c * d); }
+__device__ __forceinline__ int16_t q15_dot_add(int a, int b, int c, int d)
+{
+    const int x = (int)((unsigned)(a * b) + (unsigned)(c * d));
+    return x == (int)0x80000000 ? (int16_t)32767 : q15_round(x);
 }
 
 // -im with the VCROT90H saturation of -(-32768) to 32767.
@@ -50,6 +62,25 @@ __device__ __forceinline__ int16_t shift_round(int16_t v, uint32_t shift)
     const int s = (int)(shift & 31u);
     return wrap16(((vi & (int)mask) != 0) ? ((vi >> s) + 1) : (vi >> s));
 }
+
+// The same rounding shift with the per-stage constants precomputed: the
+// value is shifted by `s` and, when the reference's mask is non-zero (shift
+// in 1..16), bit `s - 1` is added back.
+struct ShiftRound {
+    int s, rb, rm;
+    __device__ __forceinline__ explicit ShiftRound(uint32_t shift)
+    {
+        s = (int)(shift & 31u);
+        const bool rounds = (uint16_t)(1u << ((shift - 1u) & 31u)) != 0;
+        rb = rounds ? (int)((shift - 1u) & 31u) : 0;
+        rm = rounds ? 1 : 0;
+    }
+    __device__ __forceinline__ int16_t operator()(int16_t v) const
+    {
+        const int vi = v;
+        return wrap16((vi >> s) + ((vi >> rb) & rm));
+    }
+};
 
 struct C16 {
     int16_t re, im;
@@ -75,21 +106,20 @@ __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool n
     C16 x2{wrap16(s1r - s2r), wrap16(s1i - s2i)};
     C16 x3{wrap16(d1r + jr), wrap16(d1i + ji)};
     if (!notw) {
+        // x0's Q15 product with 32767+1 (the reference's 0x7FFF0000 >> 16
+        // scale of x0 by 2^15) rounds back to x0 exactly: no change
         const short2 w1 = tw[k], w2 = tw[q + k], w3 = tw[2 * q + k];
-        x0 = C16{q15_scale((long long)x0.re * 32768), q15_scale((long long)x0.im * 32768)};
         const C16 a = x1, b = x2, c = x3;
-        x1 = C16{q15_scale((long long)a.re * w1.x - (long long)a.im * w1.y),
-                 q15_scale((long long)a.re * w1.y + (long long)a.im * w1.x)};
-        x2 = C16{q15_scale((long long)b.re * w2.x - (long long)b.im * w2.y),
-                 q15_scale((long long)b.re * w2.y + (long long)b.im * w2.x)};
-        x3 = C16{q15_scale((long long)c.re * w3.x - (long long)c.im * w3.y),
-                 q15_scale((long long)c.re * w3.y + (long long)c.im * w3.x)};
+        x1 = C16{q15_dot_sub(a.re, w1.x, a.im, w1.y), q15_dot_add(a.re, w1.y, a.im, w1.x)};
+        x2 = C16{q15_dot_sub(b.re, w2.x, b.im, w2.y), q15_dot_add(b.re, w2.y, b.im, w2.x)};
+        x3 = C16{q15_dot_sub(c.re, w3.x, c.im, w3.y), q15_dot_add(c.re, w3.y, c.im, w3.x)};
     }
     if (doShift) {
-        x0 = C16{shift_round(x0.re, shift), shift_round(x0.im, shift)};
-        x1 = C16{shift_round(x1.re, shift), shift_round(x1.im, shift)};
-        x2 = C16{shift_round(x2.re, shift), shift_round(x2.im, shift)};
-        x3 = C16{shift_round(x3.re, shift), shift_round(x3.im, shift)};
+        const ShiftRound sr(shift);
+        x0 = C16{sr(x0.re), sr(x0.im)};
+        x1 = C16{sr(x1.re), sr(x1.im)};
+        x2 = C16{sr(x2.re), sr(x2.im)};
+        x3 = C16{sr(x3.re), sr(x3.im)};
     }
     // slot order: bin0 -> 0, bin2 -> q, bin1 -> 2q, bin3 -> 3q
     p0 = x0;

@@ -294,12 +294,15 @@ FFT_DEV void issue_split_gemm(uint32_t d, uint32_t aHi, uint32_t aLo, uint32_t b
 #pragma unroll
     for (int m = 0; m < MB; ++m) {
         const uint32_t dd = d + (uint32_t)(m * NCOL);
+        // the two small cross products first: the accumulator rounds at
+        // every update relative to its running value, so only the KS
+        // hi.hi updates that come last round at full magnitude
 #pragma unroll
-        for (int s = 0; s < KS; ++s) tc_mma_f16(dd, LA::desc(aHi, m, s), LB::desc(bHi, 0, s), idesc, s > 0 ? 1u : 0u);
-#pragma unroll
-        for (int s = 0; s < KS; ++s) tc_mma_f16(dd, LA::desc(aHi, m, s), LB::desc(bLo, 0, s), idesc, 1u);
+        for (int s = 0; s < KS; ++s) tc_mma_f16(dd, LA::desc(aHi, m, s), LB::desc(bLo, 0, s), idesc, s > 0 ? 1u : 0u);
 #pragma unroll
         for (int s = 0; s < KS; ++s) tc_mma_f16(dd, LA::desc(aLo, m, s), LB::desc(bHi, 0, s), idesc, 1u);
+#pragma unroll
+        for (int s = 0; s < KS; ++s) tc_mma_f16(dd, LA::desc(aHi, m, s), LB::desc(bHi, 0, s), idesc, 1u);
     }
 }
 
@@ -599,13 +602,16 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
                         else
                             tmem_ld8(dcol + m * S::K1 + ch * HC + c0, v);
                         const int kbase = (ch * HC + c0) / 2;  // multiple of 8
-                        const int ex = n2 * kbase;
-                        const float2 ta = tabA[ex >> 6], tb = tabB[ex & 63];
-                        float wr = (ta.x * tb.x - ta.y * tb.y) * f, wi = (ta.x * tb.y + ta.y * tb.x) * f;
                         const uint32_t base = rowOff + (uint32_t)(t * N1 + kbase) * L2::W;
+                        float wr = 0.f, wi = 0.f;
 #pragma unroll
                         for (int e = 0; e < CW / 2; ++e) {
-                            if (e > 0) {
+                            if ((e & 3) == 0) {  // re-anchor every 4: at most 3 recurrence steps
+                                const int ex = n2 * (kbase + e);
+                                const float2 ta = tabA[ex >> 6], tb = tabB[ex & 63];
+                                wr = (ta.x * tb.x - ta.y * tb.y) * f;
+                                wi = (ta.x * tb.y + ta.y * tb.x) * f;
+                            } else {
                                 const float nr = wr * step.x - wi * step.y;
                                 wi = wr * step.y + wi * step.x;
                                 wr = nr;
