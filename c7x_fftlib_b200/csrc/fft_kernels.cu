@@ -85,7 +85,8 @@ cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
     if (const StaticEntry* st = find_static(a, emax)) {
         // the pipelined kernel brings whole tiles in with bulk copies, so the
         // static kernel's staged I/O (for transforms of few threads) is moot
-        const bool pipelinable = st->launchPipelined && a.err && a.ioMode == IO_C2C && !a.batchMinor && !a.twBig &&
+        const bool pipelinable = st->launchPipelined && a.err && (a.ioMode == IO_C2C || a.ioMode == IO_R2C_SPLIT) &&
+                                 !a.batchMinor && !a.twBig &&
                                  a.inElem == 1 && a.outElem == 1 && a.inBatch == (int64_t)a.N &&
                                  ((uintptr_t)a.in & 15u) == 0 && (a.N % 2u) == 0;
         if (pipelinable) {

@@ -103,7 +103,8 @@ __host__ __device__ constexpr int pipe_min_blocks(uint32_t n, int threads, int s
     return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
 
-// A tile is M consecutive transforms. One bulk copy lands their inputs,
+// A tile is M consecutive transforms (c2c, or the half-length complex FFT
+// of r2c with its split epilogue). One bulk copy lands their inputs,
 // unpadded and back to back, at the start of the stage; the first pass of
 // transform m reads its input from there and (after the CTA-wide barrier
 // inside the pass, when every input has been read) writes its outputs in the
@@ -182,6 +183,10 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
                                            active, nullptr, rowOut);
             }
         });
+        // r2c: the last pass left Z in natural order in the padded layout;
+        // the split writes the h + 1 (or 2h) bins. The stage is refilled only
+        // after the next iteration's first barrier, when this has finished.
+        if (a.ioMode == IO_R2C_SPLIT) r2c_epilogue(a, st + m * SL, t, rowOut, active);
     }
 
     if (s_fail && tid == 0) {
