@@ -17,6 +17,7 @@
 // runs both stages in registers and stores once, halving shared-memory
 // traffic and barriers.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <stdint.h>
 
 #include "fft_i16.h"
@@ -137,85 +138,134 @@ __device__ __forceinline__ void stage_bfly(C16* pt, uint32_t m, uint32_t k, cons
     bfly4(pt[0], pt[1], pt[2], pt[3], notw, tw, k, q, m != 8u, shift);
 }
 
+// Shared-memory index with one pad word per 16: the 16-point gathers of the
+// fused stages and the bit-reversed final gather hit distinct banks.
+__device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
+
+// Persistent CTAs of G groups; a group of tg threads owns one transform at a
+// time (its own padded shared-memory region) and the CTA walks the batch G
+// transforms at a step. The caller's twiddle table and the shift vector are
+// copied into shared memory once per CTA.
 __global__ void __launch_bounds__(256) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
                                                  const short2* __restrict__ w,
-                                                 const uint32_t* __restrict__ shifts, uint32_t n,
-                                                 uint32_t logn, uint32_t batch)
+                                                 const uint32_t* __restrict__ shifts, uint32_t nsh, uint32_t n,
+                                                 uint32_t logn, uint32_t batch, uint32_t tg, bool vec)
 {
-    extern __shared__ short2 sx[];
-    const uint32_t b = blockIdx.x;
-    if (b >= batch) return;
-    const short2* src = x + (size_t)b * n;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sx[i] = src[i];
+    extern __shared__ short2 smem[];
+    __shared__ uint32_t s_shift[8];
+    const uint32_t padn = n + (n >> 4);
+    const uint32_t G = blockDim.x / tg;
+    const uint32_t g = threadIdx.x / tg, t = threadIdx.x - g * tg;
+    short2* stw = smem;
+    short2* sx = smem + n + g * padn;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) stw[i] = w[i];
+    if (threadIdx.x < nsh && threadIdx.x < 8u) s_shift[threadIdx.x] = shifts[threadIdx.x];
     __syncthreads();
 
-    uint32_t m = n, stage = 0, shift = 0;
-    const short2* tw = w;
-    // pairs of radix-4 stages fused in registers: 16 points per thread
-    while (m >= 16u) {
-        const uint32_t shiftA = shifts[stage];
-        const uint32_t m2 = m / 4u;
-        const uint32_t shiftB = shifts[stage + 1];
-        const short2* tw2 = tw + 3u * (m / 4u);
-        const uint32_t s16 = m / 16u;
-        const uint32_t groups = n / 16u; // (block, k0) pairs
-        for (uint32_t gi = threadIdx.x; gi < groups; gi += blockDim.x) {
-            const uint32_t blk = gi / s16, k0 = gi - blk * s16;
-            short2* base = sx + blk * m + k0;
-            C16 p[16];
-#pragma unroll
-            for (int i = 0; i < 16; ++i) p[i] = ld(base + i * s16);
-            // stage A (block m): butterflies k = k0 + i*s16, points i, i+4, i+8, i+12
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                C16 t[4] = {p[i], p[i + 4], p[i + 8], p[i + 12]};
-                stage_bfly(t, m, k0 + (uint32_t)i * s16, tw, shiftA);
-                p[i] = t[0]; p[i + 4] = t[1]; p[i + 8] = t[2]; p[i + 12] = t[3];
+    for (uint32_t b0 = blockIdx.x * G; b0 < batch; b0 += gridDim.x * G) {
+        const uint32_t b = b0 + g;
+        const bool active = b < batch;
+        if (active) {
+            const short2* src = x + (size_t)b * n;
+            if (vec) {  // 16-byte loads: four points each
+                const int4* s4 = reinterpret_cast<const int4*>(src);
+                for (uint32_t i4 = t; i4 < n / 4u; i4 += tg) {
+                    const int4 v = __ldg(s4 + i4);
+                    const uint32_t i = 4u * i4;
+                    sx[pad16(i)] = *reinterpret_cast<const short2*>(&v.x);
+                    sx[pad16(i + 1)] = *reinterpret_cast<const short2*>(&v.y);
+                    sx[pad16(i + 2)] = *reinterpret_cast<const short2*>(&v.z);
+                    sx[pad16(i + 3)] = *reinterpret_cast<const short2*>(&v.w);
+                }
+            } else {
+                for (uint32_t i = t; i < n; i += tg) sx[pad16(i)] = src[i];
             }
-            // stage B (block m/4): sub-block s (points 4s..4s+3), butterfly k0
+        }
+        __syncthreads();
+
+        uint32_t m = n, stage = 0, shift = 0;
+        const short2* tw = stw;
+        // pairs of radix-4 stages fused in registers: 16 points per thread
+        while (m >= 16u) {
+            const uint32_t shiftA = s_shift[stage];
+            const uint32_t m2 = m / 4u;
+            const uint32_t shiftB = s_shift[stage + 1];
+            const short2* tw2 = tw + 3u * (m / 4u);
+            const uint32_t s16 = m / 16u;
+            const uint32_t groups = n / 16u; // (block, k0) pairs
+            if (active) {
+                for (uint32_t gi = t; gi < groups; gi += tg) {
+                    const uint32_t blk = gi / s16, k0 = gi - blk * s16;
+                    const uint32_t base = blk * m + k0;
+                    C16 p[16];
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                C16 t[4] = {p[4 * s], p[4 * s + 1], p[4 * s + 2], p[4 * s + 3]};
-                stage_bfly(t, m2, k0, tw2, shiftB);
-                p[4 * s] = t[0]; p[4 * s + 1] = t[1]; p[4 * s + 2] = t[2]; p[4 * s + 3] = t[3];
+                    for (int i = 0; i < 16; ++i) p[i] = ld(sx + pad16(base + (uint32_t)i * s16));
+                    // stage A (block m): butterflies k = k0 + i*s16, points i, i+4, i+8, i+12
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        C16 q4[4] = {p[i], p[i + 4], p[i + 8], p[i + 12]};
+                        stage_bfly(q4, m, k0 + (uint32_t)i * s16, tw, shiftA);
+                        p[i] = q4[0]; p[i + 4] = q4[1]; p[i + 8] = q4[2]; p[i + 12] = q4[3];
+                    }
+                    // stage B (block m/4): sub-block s (points 4s..4s+3), butterfly k0
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) {
+                        C16 q4[4] = {p[4 * s], p[4 * s + 1], p[4 * s + 2], p[4 * s + 3]};
+                        stage_bfly(q4, m2, k0, tw2, shiftB);
+                        p[4 * s] = q4[0]; p[4 * s + 1] = q4[1]; p[4 * s + 2] = q4[2]; p[4 * s + 3] = q4[3];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) st(sx + pad16(base + (uint32_t)i * s16), p[i]);
+                }
             }
-#pragma unroll
-            for (int i = 0; i < 16; ++i) st(base + i * s16, p[i]);
+            __syncthreads();
+            shift = shiftB;
+            tw = tw2 + 3u * (m2 / 4u);
+            m = m2 / 4u;
+            stage += 2;
         }
-        __syncthreads();
-        shift = shiftB;
-        tw = tw2 + 3u * (m2 / 4u);
-        m = m2 / 4u;
-        stage += 2;
-    }
-    // one remaining radix-4 stage (m == 4 or 8)
-    if (m > 2u) {
-        shift = shifts[stage];
-        const uint32_t q = m / 4u;
-        for (uint32_t j = threadIdx.x; j < n / 4u; j += blockDim.x) {
-            const uint32_t blk = j / q, k = j - blk * q;
-            short2* base = sx + blk * m + k;
-            C16 t[4] = {ld(base), ld(base + q), ld(base + 2 * q), ld(base + 3 * q)};
-            stage_bfly(t, m, k, tw, shift);
-            st(base, t[0]); st(base + q, t[1]); st(base + 2 * q, t[2]); st(base + 3 * q, t[3]);
+        // one remaining radix-4 stage (m == 4 or 8)
+        if (m > 2u) {
+            shift = s_shift[stage];
+            const uint32_t q = m / 4u;
+            if (active) {
+                for (uint32_t j = t; j < n / 4u; j += tg) {
+                    const uint32_t blk = j / q, k = j - blk * q;
+                    const uint32_t base = blk * m + k;
+                    C16 q4[4] = {ld(sx + pad16(base)), ld(sx + pad16(base + q)), ld(sx + pad16(base + 2 * q)),
+                                 ld(sx + pad16(base + 3 * q))};
+                    stage_bfly(q4, m, k, tw, shift);
+                    st(sx + pad16(base), q4[0]);
+                    st(sx + pad16(base + q), q4[1]);
+                    st(sx + pad16(base + 2 * q), q4[2]);
+                    st(sx + pad16(base + 3 * q), q4[3]);
+                }
+            }
+            __syncthreads();
+            m = q;
         }
-        __syncthreads();
-        m = q;
-    }
-    // trailing radix-2 shares the shift of the 8-point stage
-    if (m == 2u) {
-        for (uint32_t j = threadIdx.x; j < n / 2u; j += blockDim.x) {
-            const C16 a = ld(sx + 2 * j), c = ld(sx + 2 * j + 1);
-            st(sx + 2 * j, C16{shift_round(wrap16(a.re + c.re), shift), shift_round(wrap16(a.im + c.im), shift)});
-            st(sx + 2 * j + 1, C16{shift_round(wrap16(a.re - c.re), shift), shift_round(wrap16(a.im - c.im), shift)});
+        // trailing radix-2 shares the shift of the 8-point stage
+        if (m == 2u) {
+            if (active) {
+                for (uint32_t j = t; j < n / 2u; j += tg) {
+                    const C16 a = ld(sx + pad16(2 * j)), c = ld(sx + pad16(2 * j + 1));
+                    st(sx + pad16(2 * j),
+                       C16{shift_round(wrap16(a.re + c.re), shift), shift_round(wrap16(a.im + c.im), shift)});
+                    st(sx + pad16(2 * j + 1),
+                       C16{shift_round(wrap16(a.re - c.re), shift), shift_round(wrap16(a.im - c.im), shift)});
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
-    }
-    // bit-reversed gather into natural order
-    short2* dst = y + (size_t)b * n;
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
-        const uint32_t r = logn ? (__brev(k) >> (32u - logn)) : 0u;
-        dst[k] = sx[r];
+        // bit-reversed gather into natural order
+        if (active) {
+            short2* dst = y + (size_t)b * n;
+            for (uint32_t k = t; k < n; k += tg) {
+                const uint32_t r = logn ? (__brev(k) >> (32u - logn)) : 0u;
+                dst[k] = sx[pad16(r)];
+            }
+        }
+        __syncthreads();  // the region is reloaded next iteration
     }
 }
 
@@ -232,14 +282,27 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
     if (batch == 0) return cudaSuccess;
     uint32_t logn = 0;
     while ((1u << logn) < n) ++logn;
-    const size_t smem = (size_t)n * sizeof(short2);
+    const uint32_t tg = n >= 4096u ? 256u : (n / 16u >= 1u ? n / 16u : 1u);
+    const uint32_t G = 256u / tg;
+    const uint32_t threads = tg * G;
+    const size_t smem = ((size_t)n + (size_t)G * (n + (n >> 4))) * sizeof(short2);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
     if (smem > 48u * 1024u) {
-        cudaError_t e = cudaFuncSetAttribute(k_fft_i16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(k_fft_i16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    const uint32_t threads = n >= 4096u ? 256u : (n / 16u >= 32u ? n / 16u : 32u);
-    k_fft_i16<<<batch, threads, smem, s>>>((const short2*)x, (short2*)y, (const short2*)w, shifts, n, logn,
-                                           batch);
+    int perSm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_fft_i16, (int)threads, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t steps = (batch + G - 1u) / G;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(steps, (uint64_t)std::max(1, perSm) * (uint64_t)sms);
+    const bool vec = (((uintptr_t)x & 15u) == 0) && (n % 4u) == 0;
+    k_fft_i16<<<grid, threads, smem, s>>>((const short2*)x, (short2*)y, (const short2*)w, shifts, i16_num_shifts(n),
+                                          n, logn, batch, tg, vec);
     return cudaGetLastError();
 }
 
