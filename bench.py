@@ -510,7 +510,8 @@ def run_case(args):
     JSON line with the per-launch time. For profiler captures and sweeps.
     Cases: tc:N:rows (tensor-core DFT), fft:N:rows (CUDA-core FFT through the
     coordinator), c2c:N:channels, r2c:N:channels, c2r:N:channels,
-    i16:N:channels (fft1dBatched kernels)."""
+    i16:N:channels (fft1dBatched kernels), mixed:COUNT:SEED (uneven lengths,
+    one graph launch)."""
     import numpy as np
     import torch
 
@@ -573,6 +574,16 @@ def run_case(args):
 
         def launch():
             k(F.ptr(x), F.ptr(wd), F.ptr(y), F.ptr(sh), ns, n, batch, pb, sp)
+    elif kind == "mixed":  # mixed:COUNT:SEED -- the uneven-length batch, one graph launch
+        lengths = np.sort(mixed_lengths(n, seed=batch))[::-1].copy()
+        total = int(lengths.sum())
+        nbytes = 16.0 * total
+        x = torch.rand(2 * total, device="cuda", generator=g) * 2 - 1
+        y = torch.empty_like(x)
+        mb = F.MixedBatch(lengths)
+
+        def launch():
+            mb.exec(x, y, sp)
     else:
         raise SystemExit(f"unknown case kind {kind}")
     for _ in range(args.warmup):

@@ -24,6 +24,10 @@ __global__ void __launch_bounds__(BLK) k_fft_mixed(const MixedGroup* __restrict_
 {
     extern __shared__ __align__(16) float2 smem[];
     __shared__ uint32_t s_tile;
+    // the group's schedule is read many times per pass: keep a copy in
+    // shared memory for the tile instead of re-reading it from global memory
+    __shared__ __align__(16) FftArgs s_args;
+    static_assert(sizeof(FftArgs) % 4 == 0 && sizeof(FftArgs) / 4 <= BLK, "FftArgs copy");
     const uint32_t tid = threadIdx.x;
     for (;;) {
         if (tid == 0) s_tile = atomicAdd(counter, 1u);
@@ -31,7 +35,10 @@ __global__ void __launch_bounds__(BLK) k_fft_mixed(const MixedGroup* __restrict_
         const uint32_t ti = s_tile;
         if (ti >= numTiles) break;
         const MixedTile tl = tiles[ti];
-        const FftArgs& a = groups[tl.group].args;
+        if (tid < sizeof(FftArgs) / 4)
+            reinterpret_cast<uint32_t*>(&s_args)[tid] = reinterpret_cast<const uint32_t*>(&groups[tl.group].args)[tid];
+        __syncthreads();
+        const FftArgs& a = s_args;
         const uint32_t T = a.T, used = T * a.M;
         // threads beyond T*M get a lane index past every butterfly: they only
         // take part in the barriers
