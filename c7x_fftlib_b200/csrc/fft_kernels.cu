@@ -85,10 +85,13 @@ cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
     if (const StaticEntry* st = find_static(a, emax)) {
         // the pipelined kernel brings whole tiles in with bulk copies, so the
         // static kernel's staged I/O (for transforms of few threads) is moot
-        const bool pipelinable = st->launchPipelined && a.err && (a.ioMode == IO_C2C || a.ioMode == IO_R2C_SPLIT) &&
-                                 !a.batchMinor && !a.twBig &&
-                                 a.inElem == 1 && a.outElem == 1 && a.inBatch == (int64_t)a.N &&
-                                 ((uintptr_t)a.in & 15u) == 0 && (a.N % 2u) == 0;
+        // inputs: rows of N (c2c, r2c) or N + 1 bins (c2r inMode 0, which
+        // the stage holds beside its padded exchange layout for N >= 64)
+        const bool rowsOk = ((a.ioMode == IO_C2C || a.ioMode == IO_R2C_SPLIT) && a.inBatch == (int64_t)a.N) ||
+                            (a.ioMode == IO_C2R_SPLIT && !a.realMode && a.inBatch == (int64_t)a.N + 1 && a.N >= 64u);
+        const bool pipelinable = st->launchPipelined && a.err && rowsOk && !a.batchMinor && !a.twBig &&
+                                 a.inElem == 1 && a.outElem == 1 && ((uintptr_t)a.in & 15u) == 0 &&
+                                 (a.N % 2u) == 0;
         if (pipelinable) {
             FftArgs b = a;
             b.staged = 0;

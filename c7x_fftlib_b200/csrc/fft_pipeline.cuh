@@ -103,8 +103,41 @@ __host__ __device__ constexpr int pipe_min_blocks(uint32_t n, int threads, int s
     return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
 
-// A tile is M consecutive transforms (c2c, or the half-length complex FFT
-// of r2c with its split epilogue). One bulk copy lands their inputs,
+// c2r split of bin x against the mirrored bin xm: ((x + y) + i conj(w) (x - y)) / 2,
+// y = conj(xm).
+FFT_DEV float2 c2r_z(float2 x, float2 xm, float2 w)
+{
+    const float2 y = cconj(xm);
+    const float2 sum = cadd(x, y), d = csub(x, y);
+    const float2 icw = make_float2(w.y, w.x);  // i * conj(w)
+    return cscale(cadd(sum, cmul(icw, d)), 0.5f);
+}
+
+// Input span of a tile of m transforms with input rows of ic complex values:
+// the copy starts at the even element s0 at or below the tile's first value
+// (shift = 0 or 1 elements before it) and covers ncopy (even) elements, all
+// of the nelem the tile needs except, at the very end of the input, one.
+struct TileSpan {
+    uint64_t s0;
+    uint32_t shift, ncopy, nelem;
+};
+FFT_DEV TileSpan tile_span(uint32_t tile, uint32_t m, uint32_t batch, uint64_t ic, uint64_t totalIn)
+{
+    const uint64_t first = (uint64_t)tile * m;
+    const uint64_t count = min((uint64_t)m, (uint64_t)batch - first);
+    const uint64_t b = first * ic;
+    TileSpan t;
+    t.s0 = b & ~1ull;
+    t.shift = (uint32_t)(b - t.s0);
+    t.nelem = t.shift + (uint32_t)(count * ic);
+    const uint64_t want = ((uint64_t)t.nelem + 1u) & ~1ull;
+    t.ncopy = (uint32_t)(min(want, totalIn - t.s0) & ~1ull);
+    return t;
+}
+
+// A tile is M consecutive transforms (c2c; the half-length complex FFT of
+// r2c with its split epilogue; or of c2r, inMode 0, with the split computed
+// from the raw bins in pass 0). One bulk copy lands their inputs,
 // unpadded and back to back, at the start of the stage; the first pass of
 // transform m reads its input from there and (after the CTA-wide barrier
 // inside the pass, when every input has been read) writes its outputs in the
@@ -128,11 +161,14 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
     const uint32_t tiles = (a.batch + (uint32_t)M - 1u) / (uint32_t)M;
     const uint32_t G = gridDim.x;
 
+    // a tile's inputs are count * IC contiguous complex values (IC = the
+    // input row length: N, or N + 1 bins for c2r); see tile_span
+    const uint64_t IC = (uint64_t)a.inBatch;
+    const uint64_t totalIn = (uint64_t)a.batch * IC;
     auto issue = [&](uint32_t tile, int s) {
-        const uint32_t first = tile * (uint32_t)M;
-        const uint32_t count = min((uint32_t)M, a.batch - first);
-        mbar_expect_tx(&bar[s], count * N * 8u);
-        bulk_copy_g2s(stages + (size_t)s * STL, a.in + (size_t)first * N, count * N * 8u, &bar[s]);
+        const TileSpan sp = tile_span(tile, (uint32_t)M, a.batch, IC, totalIn);
+        mbar_expect_tx(&bar[s], sp.ncopy * 8u);
+        bulk_copy_g2s(stages + (size_t)s * STL, a.in + sp.s0, sp.ncopy * 8u, &bar[s]);
     };
 
     if (tid == 0) {
@@ -154,11 +190,16 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
         const int s = (int)(it % STAGES);
         // one thread waits for the stage; the barrier passes the data (and
         // the outcome) on to the others
-        if (tid == 0 && !mbar_wait_bounded(&bar[s], (it / STAGES) & 1u)) s_fail = 1u;
+        float2* st = stages + (size_t)s * STL;
+        const TileSpan sp = tile_span(tile, (uint32_t)M, a.batch, IC, totalIn);
+        const uint32_t shift = sp.shift;
+        if (tid == 0) {
+            if (!mbar_wait_bounded(&bar[s], (it / STAGES) & 1u)) s_fail = 1u;
+            else if (sp.nelem > sp.ncopy) st[sp.ncopy] = a.in[sp.s0 + sp.ncopy];  // odd element at the very end
+        }
         __syncthreads();
         if (s_fail) break;
 
-        float2* st = stages + (size_t)s * STL;
         const uint32_t gidx = tile * (uint32_t)M + m;
         const bool active = gidx < a.batch;
         // once every thread has read this tile's inputs (the barrier inside
@@ -172,12 +213,27 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
             }
         };
         float2* rowOut = a.out + (size_t)gidx * (size_t)a.outBatch;
+        if (a.ioMode == IO_C2R_SPLIT) {
+            // c2r (inMode 0): turn the h + 1 bins into the h-point input Z in
+            // place, Z[i] = ((X[i] + y) + i conj(W) (X[i] - y)) / 2 with
+            // y = conj(X[h - i]); each thread owns the pair (i, h - i)
+            float2* row = st + shift + m * (uint32_t)IC;
+            if (active) {
+                for (uint32_t i = t; i <= N / 2u; i += (uint32_t)S::T) {
+                    const uint32_t ip = N - i;
+                    const float2 xi = row[i], xp = row[ip];
+                    row[i] = c2r_z(xi, xp, __ldg(&a.twSplit[i]));
+                    if (i != 0u && ip != i) row[ip] = c2r_z(xp, xi, __ldg(&a.twSplit[ip]));
+                }
+            }
+            __syncthreads();
+        }
         static_for<S::P>([&](auto p) {
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
             if constexpr (P == 0) {
                 run_pass<S::EMAX, S::R[P]>(a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, gidx,
-                                           active, nullptr, rowOut, st + m * N, refill);
+                                           active, nullptr, rowOut, st + shift + m * (uint32_t)IC, refill);
             } else {
                 run_pass<S::EMAX, S::R[P]>(a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, gidx,
                                            active, nullptr, rowOut);
