@@ -207,7 +207,9 @@ struct TcShape {
     static constexpr int N1 = N1_, N2 = N2_;
     static constexpr bool kDirect = (N2 == 1);
     static constexpr int N = N1 * N2;
-    static constexpr int T = kDirect ? 128 : 128 / (N1 < N2 ? N1 : N2);  // transforms per tile
+    // transforms per tile: 256 rows per stage up to N = 1024 (short tiles
+    // would spend their time in hand-offs), 128 above
+    static constexpr int T = kDirect ? 128 : (N1 * N2 <= 1024 ? 256 : 128) / (N1 < N2 ? N1 : N2);
     static constexpr int R1 = kDirect ? 128 : T * N2;                    // stage-1 rows
     static constexpr int R2 = kDirect ? 128 : T * N1;                    // stage-2 rows
     static constexpr int MB1 = R1 / 128, MB2 = R2 / 128;
