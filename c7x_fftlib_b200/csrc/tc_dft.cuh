@@ -9,28 +9,27 @@
 // FP32 in tensor memory. Their sum carries about 22 significant bits of
 // every operand, so the result is within a few 1e-7 of the FP64 DFT.
 //
-// Two shapes, both persistent (one CTA per SM walks tiles of transforms):
-//  * direct, N <= 64: one GEMM per tile of 128 transforms, rows = transforms,
-//    K = 2N (the dftSmall / dftLarge variants of the reference coordinator,
-//    src/fft_c7xmma/FFTLIB_FFT_fft_ixX_cxX_oxX/FFTLIB_FFT_fft_ixX_cxX_oxX.cpp:13-50);
-//  * two-stage, N = N1 * N2 (the high-radix decomposition, reference
-//    src/fft_c7xmma/FFTLIB_FFT_highRadixDecompositions_ixX_cxX_oxX/
-//    FFTLIB_FFT_highRadixDecompositions_ixX_cxX_oxX_cn.cpp:20-438, restated
-//    here as one Cooley-Tukey split): with n = N2 n1 + n2 and k = k1 + N1 k2,
+// This file holds the shared tcgen05 helpers and the two-stage kernel
+// (N = N1 * N2, the reference coordinator's highRadixDecompositions variant,
+// src/fft_c7xmma/FFTLIB_FFT_highRadixDecompositions_ixX_cxX_oxX/
+// FFTLIB_FFT_highRadixDecompositions_ixX_cxX_oxX_cn.cpp:20-438, restated here
+// as one Cooley-Tukey split); the one-stage kernel for N <= 64 (dftSmall /
+// dftLarge) is in tc_dft_small.cuh. With n = N2 n1 + n2 and k = k1 + N1 k2:
 //      stage 1 (rows (t, n2), K = n1):  Z[n2][k1] = sum_n1 x[N2 n1 + n2] W_N1^(n1 k1)
 //      twiddle (fused into the stage-1 epilogue): Z'[n2][k1] = Z[n2][k1] W_N^(n2 k1)
 //      stage 2 (rows (t, k1), K = n2): y[k1 + N1 k2] = sum_n2 Z'[n2][k1] W_N2^(n2 k2)
-//    The stage-1 epilogue reads the accumulator row of (t, n2) from tensor
-//    memory, rescales, twiddles, splits and writes it transposed into the
-//    K-major stage-2 operand in shared memory; the stage-2 epilogue writes
-//    natural-order output straight to HBM.
+// The stage-1 epilogue reads the accumulator row of (t, n2) from tensor
+// memory, rescales, twiddles, splits and writes it transposed into the
+// K-major stage-2 operand in shared memory; the stage-2 epilogue writes
+// natural-order output straight to HBM. One persistent CTA per SM walks
+// tiles of T transforms (256 rows per stage up to N = 1024, 128 above).
 //
 // Warp roles: 8 loader warps (HBM -> registers -> scale/split -> swizzled
-// shared-memory operand), 8 transposer warps (two-stage only), 4 or 8
-// epilogue warps, and one warp whose elected lane allocates tensor memory and
-// issues every tcgen05.mma. Hand-offs use mbarriers over NB = 2 tile buffers;
-// every wait is bounded and a wait that gives up sets kErrTcTimeout in the
-// launch's error word and makes every role leave its loop.
+// shared-memory operand), 8 transposer warps, 4 epilogue warps, and one warp
+// whose elected lane allocates tensor memory and issues every tcgen05.mma.
+// Hand-offs use mbarriers over NB tile buffers (2 to 8, by shared and tensor
+// memory); every wait is bounded and a wait that gives up sets kErrTcTimeout
+// in the launch's error word and makes every role leave its loop.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -205,41 +204,37 @@ struct KMajor {
 template <int N1_, int N2_>
 struct TcShape {
     static constexpr int N1 = N1_, N2 = N2_;
-    static constexpr bool kDirect = (N2 == 1);
     static constexpr int N = N1 * N2;
     // transforms per tile: 256 rows per stage up to N = 1024 (short tiles
     // would spend their time in hand-offs), 128 above
-    static constexpr int T = kDirect ? 128 : (N1 * N2 <= 1024 ? 256 : 128) / (N1 < N2 ? N1 : N2);
-    static constexpr int R1 = kDirect ? 128 : T * N2;                    // stage-1 rows
-    static constexpr int R2 = kDirect ? 128 : T * N1;                    // stage-2 rows
+    static constexpr int T = (N1 * N2 <= 1024 ? 256 : 128) / (N1 < N2 ? N1 : N2);
+    static constexpr int R1 = T * N2;  // stage-1 rows
+    static constexpr int R2 = T * N1;  // stage-2 rows
     static constexpr int MB1 = R1 / 128, MB2 = R2 / 128;
     static constexpr int K1 = 2 * N1, K2 = 2 * N2;  // GEMM K (= output columns) per stage
-    static constexpr int LW = 8, XW = kDirect ? 0 : 8, EW = kDirect ? 8 : 4;
+    static constexpr int LW = 8, XW = 8, EW = 4;
     static constexpr int MMA_WARP = LW + XW + EW;
     static constexpr int THREADS = 32 * (MMA_WARP + 1);
     using L1 = KMajor<R1, K1>;
-    using L2 = KMajor<R2, (kDirect ? 16 : K2)>;
+    using L2 = KMajor<R2, K2>;
     using LW1 = KMajor<K1, K1>;
-    using LW2 = KMajor<(kDirect ? 16 : K2), (kDirect ? 16 : K2)>;
-    static constexpr bool kSharedW = kDirect || N1 == N2;
+    using LW2 = KMajor<K2, K2>;
+    static constexpr bool kSharedW = N1 == N2;
     static constexpr uint32_t HALF_TILE = L1::BYTES;  // one of hi / lo
     static constexpr uint32_t TILE = 2 * HALF_TILE;
     static constexpr uint32_t W1_HALF = LW1::BYTES;
     static constexpr uint32_t W2_HALF = kSharedW ? 0u : LW2::BYTES;
-    static constexpr uint32_t D1_COLS = MB1 * K1, D2_COLS = kDirect ? 0 : MB2 * K2;
-    // one-stage epilogue staging: per warp 32 rows x 16 columns, rows padded to 80 bytes
-    static constexpr uint32_t STAGE_BYTES = kDirect ? (uint32_t)EW * 32u * 80u : 0u;
+    static constexpr uint32_t D1_COLS = MB1 * K1, D2_COLS = MB2 * K2;
     // tile buffers: as many as shared memory (about 200 KB for tiles and
     // matrices) and tensor memory (512 columns) allow, between 2 and 8
-    static constexpr int NB_SMEM = (int)((200u * 1024u - 2u * (W1_HALF + W2_HALF) - STAGE_BYTES) / TILE);
+    static constexpr int NB_SMEM = (int)((200u * 1024u - 2u * (W1_HALF + W2_HALF)) / TILE);
     static constexpr int NB_TMEM = (int)(512u / (D1_COLS + D2_COLS));
     static constexpr int NB_MAX = NB_SMEM < NB_TMEM ? NB_SMEM : NB_TMEM;
     static constexpr int NB = NB_MAX > 8 ? 8 : (NB_MAX < 2 ? 2 : NB_MAX);
-    static constexpr int TABA = kDirect ? 0 : N / 64 + 1, TABB = kDirect ? 0 : 64;
+    static constexpr int TABA = N / 64 + 1, TABB = 64;
     static constexpr uint32_t OFF_W1 = NB * TILE;
     static constexpr uint32_t OFF_W2 = OFF_W1 + 2 * W1_HALF;
-    static constexpr uint32_t OFF_STAGE = OFF_W2 + 2 * W2_HALF;
-    static constexpr uint32_t OFF_TAB = OFF_STAGE + STAGE_BYTES;
+    static constexpr uint32_t OFF_TAB = OFF_W2 + 2 * W2_HALF;
     static constexpr uint32_t OFF_S1 = OFF_TAB + 8u * (TABA + TABB);
     static constexpr uint32_t OFF_S2 = OFF_S1 + 4u * 2 * NB * R1;
     static constexpr uint32_t OFF_PART = OFF_S2 + 4u * 2 * NB * T;
@@ -253,7 +248,10 @@ struct TcShape {
         TMEM_USED <= 32 ? 32 : TMEM_USED <= 64 ? 64 : TMEM_USED <= 128 ? 128 : TMEM_USED <= 256 ? 256 : 512;
     static_assert(TMEM_USED <= 512, "tensor memory holds 512 columns");
     static_assert(SMEM <= 227u * 1024u, "shared memory per CTA");
-    static_assert(K1 >= 16 && K1 <= 256 && (kDirect || (K2 >= 16 && K2 <= 256)), "MMA N in [16, 256]");
+    static_assert(K1 >= 16 && K1 <= 256 && K2 >= 16 && K2 <= 256, "MMA N in [16, 256]");
+    // the transposer's swizzle constants need the k1 of each half-row group
+    // to start at a multiple of 8
+    static_assert(N1 >= 16, "N1 >= 16");
     static_assert(R1 % 128 == 0 && R2 % 128 == 0 && R1 <= 256, "rows per stage");
     // barrier indices
     static constexpr int A_FULL = 0, D1_FULL = NB, D1_FREE = 2 * NB, S2_FULL = 3 * NB, D2_FULL = 4 * NB,
@@ -364,7 +362,7 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
         tmem_relinquish();
     }
     fill_dft_operand<typename S::LW1>(sm + S::OFF_W1, sm + S::OFF_W1 + S::W1_HALF, w, S::K1);
-    if constexpr (!S::kDirect) {
+    {
         const float* w2 = w + (size_t)S::K1 * S::K1;
         if constexpr (!S::kSharedW)
             fill_dft_operand<typename S::LW2>(sm + S::OFF_W2, sm + S::OFF_W2 + S::W2_HALF, w2, S::K2);
@@ -399,43 +397,7 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
             const uint32_t u = i / NB, slot = i % (2 * NB);
             unsigned char* hiB = sm + b * S::TILE;
             unsigned char* loB = hiB + S::HALF_TILE;
-            if constexpr (S::kDirect) {
-                constexpr int LPR = N1 / 2;  // lanes per row, 2 complex per lane
-                constexpr int RPI = 32 / LPR;
-                constexpr int NI = 16 / RPI;  // 16 rows per warp
-                const int g = lane / LPR, p = lane % LPR;
-                float4 v[NI];
-#pragma unroll
-                for (int k = 0; k < NI; ++k) {
-                    const int r = warp * 16 + k * RPI + g;
-                    const uint32_t gt = tile * 128u + (uint32_t)r;
-                    v[k] = gt < batch ? __ldg(reinterpret_cast<const float4*>(x + (size_t)gt * N1) + p)
-                                      : make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-                int sh[NI];
-#pragma unroll
-                for (int k = 0; k < NI; ++k) {
-                    float m = fmaxf(fmaxf(fabsf(v[k].x), fabsf(v[k].y)), fmaxf(fabsf(v[k].z), fabsf(v[k].w)));
-#pragma unroll
-                    for (int o = LPR / 2; o >= 1; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-                    sh[k] = row_shift(m);
-                }
-                bool bad = false;
-                if (u >= 1 && j == 0) bad = !tc_wait(&bars[S::D1_FULL + b], (u - 1) & 1u, abortFlag, err);
-                if (group_sync_or(1, 32 * S::LW, bad)) break;
-#pragma unroll
-                for (int k = 0; k < NI; ++k) {
-                    const int r = warp * 16 + k * RPI + g;
-                    const float sc = exp2i(sh[k]);
-                    uint32_t h0, h1, l0, l1;
-                    split2(v[k].x * sc, v[k].y * sc, h0, l0);
-                    split2(v[k].z * sc, v[k].w * sc, h1, l1);
-                    const uint32_t off = S::L1::chunk(r, p >> 1) + (uint32_t)(p & 1) * 8u;
-                    *reinterpret_cast<uint2*>(hiB + off) = make_uint2(h0, h1);
-                    *reinterpret_cast<uint2*>(loB + off) = make_uint2(l0, l1);
-                    if (p == 0) s1ring[slot * S::R1 + r] = sh[k];
-                }
-            } else {
+            {
                 constexpr int H = 256 / S::R1;  // threads per row
                 constexpr int CPH = N1 / H;     // complex values per thread
                 constexpr int NCH = CPH / 4;    // 16-byte chunks per thread
@@ -510,24 +472,19 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
                 tc_commit(&bars[S::D2_FULL + b]);
                 return true;
             };
-            if constexpr (S::kDirect) {
-                for (uint32_t i = 0; i < count; ++i)
-                    if (!stage1(i)) break;
-            } else {
-                bool ok = count == 0 || stage1(0);
-                for (uint32_t i = 0; ok && i < count; ++i) {
-                    if (i + 1 < count) ok = stage1(i + 1);
-                    if (ok) ok = stage2(i);
-                }
+            bool ok = count == 0 || stage1(0);
+            for (uint32_t i = 0; ok && i < count; ++i) {
+                if (i + 1 < count) ok = stage1(i + 1);
+                if (ok) ok = stage2(i);
             }
             // wait for every MMA issued above before tensor memory is released
             tc_commit(&bars[S::DRAIN]);
             mbar_wait_bounded(&bars[S::DRAIN], 0);
         }
         __syncwarp();
-    } else if (!S::kDirect && warp < S::LW + S::XW) {
+    } else if (warp < S::LW + S::XW) {
         // ================= transposers: D1 -> twiddle -> stage-2 operand =================
-        if constexpr (!S::kDirect) {
+        {
             const int xt = threadIdx.x - 32 * S::LW;  // 0..255
             const int q = warp & 3, ch = (warp - S::LW) >> 2;
             constexpr int HC = S::K1 / 2;  // accumulator columns per half
@@ -646,49 +603,13 @@ __global__ void __launch_bounds__(TcShape<N1, N2>::THREADS, 1)
         for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
             const int b = (int)(i % NB);
             const uint32_t u = i / NB, slot = i % (2 * NB);
-            const int fullBar = S::kDirect ? S::D1_FULL : S::D2_FULL;
-            const int freeBar = S::kDirect ? S::D1_FREE : S::D2_FREE;
+            const int fullBar = S::D2_FULL;
+            const int freeBar = S::D2_FREE;
             bool bad = false;
             if (et == 0) bad = !tc_wait(&bars[fullBar + b], u & 1u, abortFlag, err);
             if (group_sync_or(3, 32 * S::EW, bad)) break;
             tc_fence_after();
-            if constexpr (S::kDirect) {
-                // each warp owns 32 rows (transforms) x half the columns; a
-                // 16-column slice goes TMEM -> registers -> a padded staging
-                // tile -> HBM with 4 lanes per row (64-byte runs)
-                const int ch = (warp - S::LW) >> 2;
-                constexpr int HC = S::K1 / 2;
-                constexpr int CW = HC >= 16 ? 16 : 8;
-                constexpr int LPR = CW / 4;      // lanes per row on the way out
-                constexpr int RPI = 32 / LPR;    // rows per store instruction
-                const int r = 32 * q + lane;
-                const float f = exp2i(-(s1ring[slot * S::R1 + r] + kTcWShift));
-                const uint32_t dcol = tmem + laneBase + b * S::D1_COLS + ch * HC;
-                float* stg = reinterpret_cast<float*>(sm + S::OFF_STAGE) + (warp - S::LW) * (32 * 20);
-                const int pr = lane / LPR, pc = lane % LPR;
-#pragma unroll
-                for (int c0 = 0; c0 < HC; c0 += CW) {
-                    float v[CW];
-                    if constexpr (CW == 16)
-                        tmem_ld16(dcol + c0, v);
-                    else
-                        tmem_ld8(dcol + c0, v);
-#pragma unroll
-                    for (int e = 0; e < CW / 4; ++e)
-                        *reinterpret_cast<float4*>(stg + lane * 20 + 4 * e) =
-                            make_float4(v[4 * e] * f, v[4 * e + 1] * f, v[4 * e + 2] * f, v[4 * e + 3] * f);
-                    __syncwarp();
-#pragma unroll
-                    for (int it = 0; it < 32 / RPI; ++it) {
-                        const int rr = it * RPI + pr;
-                        const uint32_t gt = tile * 128u + (uint32_t)(32 * q + rr);
-                        const float4 o = *reinterpret_cast<const float4*>(stg + rr * 20 + 4 * pc);
-                        if (gt < batch)
-                            *reinterpret_cast<float4*>(y + (size_t)gt * N1 + (ch * HC + c0) / 2 + 2 * pc) = o;
-                    }
-                    __syncwarp();
-                }
-            } else {
+            {
                 constexpr int CW = S::K2 >= 16 ? 16 : 8;
 #pragma unroll
                 for (int m = 0; m < S::MB2; ++m) {
