@@ -76,10 +76,12 @@ struct ShiftRound {
         rb = rounds ? (int)((shift - 1u) & 31u) : 0;
         rm = rounds ? 1 : 0;
     }
+    // (v >> s) plus the rounding bit always fits in int16 (for s = 0 no bit
+    // is added), so no wrap is needed
     __device__ __forceinline__ int16_t operator()(int16_t v) const
     {
         const int vi = v;
-        return wrap16((vi >> s) + ((vi >> rb) & rm));
+        return (int16_t)((vi >> s) + ((vi >> rb) & rm));
     }
 };
 
@@ -92,16 +94,21 @@ __device__ __forceinline__ void st(short2* p, C16 c) { *p = make_short2(c.re, c.
 
 // One 4-point butterfly on p[0..3] (stride q apart in the stage), outputs
 // written back as bins 0,2,1,3 (the reference's slot order).
-// tw: the three Q15 twiddles (x1, x2, x3) or nullptr-equivalent when notw.
+// tw: the three Q15 twiddles (x1, x2, x3) unless notw.
+// Sums and differences are formed in int32 and wrapped to int16 only where
+// the reference's value is used non-linearly: the j-rotation's saturation
+// test and the four outputs (wrapping is linear modulo 2^16, so delaying it
+// gives the same bits).
 __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool notw,
                                       const short2* tw, uint32_t k, uint32_t q, bool doShift,
-                                      uint32_t shift)
+                                      const ShiftRound& sr)
 {
-    const int16_t s1r = wrap16(p0.re + p2.re), s1i = wrap16(p0.im + p2.im);
-    const int16_t s2r = wrap16(p1.re + p3.re), s2i = wrap16(p1.im + p3.im);
-    const int16_t d1r = wrap16(p0.re - p2.re), d1i = wrap16(p0.im - p2.im);
-    const int16_t d2r = wrap16(p1.re - p3.re), d2i = wrap16(p1.im - p3.im);
-    const int16_t jr = rot90_re(d2i), ji = d2r;
+    const int s1r = p0.re + p2.re, s1i = p0.im + p2.im;
+    const int s2r = p1.re + p3.re, s2i = p1.im + p3.im;
+    const int d1r = p0.re - p2.re, d1i = p0.im - p2.im;
+    const int d2r = p1.re - p3.re;
+    const int16_t d2i = wrap16(p1.im - p3.im);
+    const int jr = rot90_re(d2i), ji = d2r;
     C16 x0{wrap16(s1r + s2r), wrap16(s1i + s2i)};
     C16 x1{wrap16(d1r - jr), wrap16(d1i - ji)};
     C16 x2{wrap16(s1r - s2r), wrap16(s1i - s2i)};
@@ -116,7 +123,6 @@ __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool n
         x3 = C16{q15_dot_sub(c.re, w3.x, c.im, w3.y), q15_dot_add(c.re, w3.y, c.im, w3.x)};
     }
     if (doShift) {
-        const ShiftRound sr(shift);
         x0 = C16{sr(x0.re), sr(x0.im)};
         x1 = C16{sr(x1.re), sr(x1.im)};
         x2 = C16{sr(x2.re), sr(x2.im)};
@@ -130,12 +136,11 @@ __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool n
 }
 
 // Stage with block size m (q = m/4) on the 4 points {k + b*m + i*q}.
-__device__ __forceinline__ void stage_bfly(C16* pt, uint32_t m, uint32_t k, const short2* tw,
-                                           uint32_t shift)
+__device__ __forceinline__ void stage_bfly(C16* pt, uint32_t m, uint32_t k, const short2* tw, const ShiftRound& sr)
 {
     const uint32_t q = m / 4u;
     const bool notw = (m == 4u) || (m == 8u && k == 0u);
-    bfly4(pt[0], pt[1], pt[2], pt[3], notw, tw, k, q, m != 8u, shift);
+    bfly4(pt[0], pt[1], pt[2], pt[3], notw, tw, k, q, m != 8u, sr);
 }
 
 // Shared-memory index with one pad word per 16: the 16-point gathers of the
@@ -190,6 +195,7 @@ __global__ void __launch_bounds__(256) k_fft_i16(const short2* __restrict__ x, s
             const uint32_t shiftA = s_shift[stage];
             const uint32_t m2 = m / 4u;
             const uint32_t shiftB = s_shift[stage + 1];
+            const ShiftRound srA(shiftA), srB(shiftB);
             const short2* tw2 = tw + 3u * (m / 4u);
             const uint32_t s16 = m / 16u;
             const uint32_t groups = n / 16u; // (block, k0) pairs
@@ -204,14 +210,14 @@ __global__ void __launch_bounds__(256) k_fft_i16(const short2* __restrict__ x, s
 #pragma unroll
                     for (int i = 0; i < 4; ++i) {
                         C16 q4[4] = {p[i], p[i + 4], p[i + 8], p[i + 12]};
-                        stage_bfly(q4, m, k0 + (uint32_t)i * s16, tw, shiftA);
+                        stage_bfly(q4, m, k0 + (uint32_t)i * s16, tw, srA);
                         p[i] = q4[0]; p[i + 4] = q4[1]; p[i + 8] = q4[2]; p[i + 12] = q4[3];
                     }
                     // stage B (block m/4): sub-block s (points 4s..4s+3), butterfly k0
 #pragma unroll
                     for (int s = 0; s < 4; ++s) {
                         C16 q4[4] = {p[4 * s], p[4 * s + 1], p[4 * s + 2], p[4 * s + 3]};
-                        stage_bfly(q4, m2, k0, tw2, shiftB);
+                        stage_bfly(q4, m2, k0, tw2, srB);
                         p[4 * s] = q4[0]; p[4 * s + 1] = q4[1]; p[4 * s + 2] = q4[2]; p[4 * s + 3] = q4[3];
                     }
 #pragma unroll
@@ -234,7 +240,7 @@ __global__ void __launch_bounds__(256) k_fft_i16(const short2* __restrict__ x, s
                     const uint32_t base = blk * m + k;
                     C16 q4[4] = {ld(sx + pad16(base)), ld(sx + pad16(base + q)), ld(sx + pad16(base + 2 * q)),
                                  ld(sx + pad16(base + 3 * q))};
-                    stage_bfly(q4, m, k, tw, shift);
+                    stage_bfly(q4, m, k, tw, ShiftRound(shift));
                     st(sx + pad16(base), q4[0]);
                     st(sx + pad16(base + q), q4[1]);
                     st(sx + pad16(base + 2 * q), q4[2]);
