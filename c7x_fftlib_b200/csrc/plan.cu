@@ -48,7 +48,7 @@ void enumerate(uint32_t rem, int maxIdx, std::vector<int>& cur, std::vector<std:
 
 // Score a radix sequence on an engine width: each pass is one shared-memory
 // round trip; idle butterfly slots and wider register files cost extra.
-bool evaluate(uint32_t n, const int* seq, int len, int emax, EnginePlan* e)
+bool evaluate(uint32_t n, const int* seq, int len, int emax, EnginePlan* e, bool pipelined = false)
 {
     // widths without a runtime-engine instantiation (the mixed-batch kernel's)
     // are capped by the caller's maxT instead
@@ -74,6 +74,10 @@ bool evaluate(uint32_t n, const int* seq, int len, int emax, EnginePlan* e)
     // runs at about a third of the 16-wide one's throughput, so it is kept
     // for lengths nothing narrower can plan
     score += emax == 32 ? 2.5 : emax == 16 ? 0.15 : 0.0;
+    // a one-pass schedule cannot run in the bulk-copy pipelined kernel (its
+    // first pass is its last): at N = 8 and 16 it measured 2.7 TB/s, so the
+    // two-pass schedules with fixed-size pipelined kernels (4x2, 8x2) win
+    if (pipelined && len == 1 && (n == 8u || n == 16u)) score += 1.5;
     e->n = n;
     e->emax = emax;
     e->T = T;
@@ -106,7 +110,8 @@ std::vector<EnginePlan> engine_candidates(uint32_t n, int emaxOnly, uint32_t max
         const int only[1] = {emaxOnly};
         for (int emax : (emaxOnly ? std::vector<int>(only, only + 1) : std::vector<int>(kEmax, kEmax + 3))) {
             EnginePlan e;
-            if (evaluate(n, s.data(), (int)s.size(), emax, &e) && (!maxT || e.T <= maxT)) out.push_back(e);
+            if (evaluate(n, s.data(), (int)s.size(), emax, &e, emaxOnly == 0) && (!maxT || e.T <= maxT))
+                out.push_back(e);
         }
     }
     std::stable_sort(out.begin(), out.end(),
@@ -123,7 +128,7 @@ void search_best(uint32_t n, uint32_t rem, int maxIdx, int* seq, int len, Engine
     if (rem == 1u) {
         for (int emax : kEmax) {
             EnginePlan e;
-            if (evaluate(n, seq, len, emax, &e) && (!*found || e.score < best->score)) {
+            if (evaluate(n, seq, len, emax, &e, true) && (!*found || e.score < best->score)) {
                 *best = e;
                 *found = true;
             }
