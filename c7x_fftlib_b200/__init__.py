@@ -1,4 +1,5 @@
-"""c7x_fftlib_b200 -- B200-native FFTLIB batched FFT hot path.
+"""c7x_fftlib_b200 -- B200-native FFTLIB 1-D FFT hot path (batched and
+single-transform kernels, the DFT coordinator, mixed-size batches).
 
 The product is ``libfftlib_b200.so`` (hand-written sm_100a CUDA behind the
 FFTLIB C API, headers in ``include/``). This package builds it in-tree
@@ -45,6 +46,11 @@ PBLOCK_SIZE = {
     "r2c": 41 * SE_PARAM_SIZE + 18 * 4,
     "c2r": 41 * SE_PARAM_SIZE + 18 * 4,
     "i16": 13 * SE_PARAM_SIZE,
+    "1d_c2c": 27 * SE_PARAM_SIZE + 16 * 4,
+    "1d_ifft": 27 * SE_PARAM_SIZE + 16 * 4,
+    "1d_r2c": 35 * SE_PARAM_SIZE + 18 * 4,
+    "1d_c2r": 34 * SE_PARAM_SIZE + 16 * 4,
+    "1d_i16": 9 * SE_PARAM_SIZE,
 }
 
 
@@ -83,6 +89,13 @@ _SIGS = {
     "real_check_cn": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32, _u8],
     "i16": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32, _vp],
     "i16_cn": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _u32, _u32],
+    # single-transform kernels: lengths from bufParamsX->dim_x
+    "1d_c2c": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp],
+    "1d_c2c_cn": [_vp, _bpp, _vp, _bpp, _vp, _bpp],
+    "1d_real": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _vp],
+    "1d_real_cn": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp],
+    "1d_i16": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp, _vp],
+    "1d_i16_cn": [_vp, _bpp, _vp, _bpp, _vp, _bpp, _vp, _bpp],
 }
 
 KERNELS = {
@@ -91,6 +104,11 @@ KERNELS = {
     "r2c": "FFTLIB_fft1dBatched_i32f_c32fc_o32fc",
     "c2r": "FFTLIB_ifft1dBatched_i32fc_c32fc_o32f",
     "i16": "FFTLIB_fft1dBatched_i16sc_c16sc_o16sc",
+    "1d_c2c": "FFTLIB_fft1d_i32fc_c32fc_o32fc",
+    "1d_ifft": "FFTLIB_ifft1d_i32fc_c32fc_o32fc",
+    "1d_r2c": "FFTLIB_fft1d_i32f_c32fc_o32fc",
+    "1d_c2r": "FFTLIB_ifft1d_i32fc_c32fc_o32f",
+    "1d_i16": "FFTLIB_fft1d_i16sc_c16sc_o16sc",
 }
 
 _lib = None
@@ -110,8 +128,17 @@ def lib() -> C.CDLL:
         elif kind in ("r2c", "c2r"):
             fam = {"_init": "real", "_kernel": "real", "_checkParams": "real_check", "_cn": "real_cn",
                    "_checkParams_cn": "real_check_cn"}
-        else:
+        elif kind == "i16":
             fam = {"_init": "i16", "_kernel": "i16", "_checkParams": "i16", "_cn": "i16_cn", "_checkParams_cn": "i16_cn"}
+        elif kind in ("1d_c2c", "1d_ifft"):
+            fam = {"_init": "1d_c2c", "_kernel": "1d_c2c", "_checkParams": "1d_c2c", "_cn": "1d_c2c_cn",
+                   "_checkParams_cn": "1d_c2c_cn"}
+        elif kind in ("1d_r2c", "1d_c2r"):
+            fam = {"_init": "1d_real", "_kernel": "1d_real", "_checkParams": "1d_c2c", "_cn": "1d_real_cn",
+                   "_checkParams_cn": "1d_c2c_cn"}
+        else:
+            fam = {"_init": "1d_i16", "_kernel": "1d_i16", "_checkParams": "1d_i16", "_cn": "1d_i16_cn",
+                   "_checkParams_cn": "1d_i16_cn"}
         for suffix, sig in fam.items():
             fn = getattr(L, base + suffix)
             fn.argtypes = _SIGS[sig]

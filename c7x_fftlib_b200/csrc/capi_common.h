@@ -15,7 +15,10 @@ struct ComplexPlan;
 
 // Plan record kept at the start of the caller's pBlock by every _init.
 constexpr uint32_t kRecordMagic = 0x42323030u; // "B200"
-enum RecordKind : uint32_t { REC_C2C = 1, REC_IFFT = 2, REC_R2C = 3, REC_C2R = 4, REC_I16 = 5 };
+enum RecordKind : uint32_t {
+    REC_C2C = 1, REC_IFFT = 2, REC_R2C = 3, REC_C2R = 4, REC_I16 = 5,  // batched kernels
+    REC_1D_C2C = 6, REC_1D_IFFT = 7, REC_1D_R2C = 8, REC_1D_C2R = 9, REC_1D_I16 = 10,  // single-transform kernels
+};
 
 struct PlanRecord {
     uint32_t magic;

@@ -153,7 +153,7 @@ FFTLIB_STATUS FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32f_kernelAsync(FFTLIB_F32*
     PlanRecord r;
     FFTLIB_STATUS st = async_record(pBlock, REC_C2R, numPoints, &r);
     if (st != FFTLIB_SUCCESS) return st;
-    if (r.plan->fourStep && !pXFFT) return FFTLIB_ERR_NULL_POINTER;
+    if (c2r_needs_scratch(r.plan, inMode ? 1 : 0) && !pXFFT) return FFTLIB_ERR_NULL_POINTER;
     return launched(run_c2r(r.plan, (const float2*)pX, (float2*)pXFFT, pY, numChannels, inMode ? 1 : 0,
                             (cudaStream_t)stream),
                     "ifft1dBatched c2r");

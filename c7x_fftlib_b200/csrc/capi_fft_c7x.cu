@@ -17,7 +17,7 @@
 // vectors), reported with FFTLIB_ERR_INVALID_DIMENSION.
 #include <string.h>
 
-#include "capi_common.h"
+#include "capi_exec.h"
 #include "fft_c7x.h"
 #include "fft_i16.h"
 #include "plan.h"
@@ -28,7 +28,9 @@ namespace {
 
 bool has_235(uint32_t n) { return is_235(n); }
 
-PlanRecord* record(void* pBlock) { return (PlanRecord*)pBlock; }
+} // namespace
+
+namespace fftb200 {
 
 FFTLIB_STATUS write_record(void* pBlock, uint32_t kind, uint32_t n, uint32_t c, uint32_t mode, ComplexPlan* plan)
 {
@@ -62,6 +64,10 @@ FFTLIB_STATUS read_record(void* pBlock, uint32_t kind, uint32_t n, PlanRecord* o
     }
     return FFTLIB_SUCCESS;
 }
+
+} // namespace fftb200
+
+namespace {
 
 // ---- checks ---------------------------------------------------------------
 
@@ -119,6 +125,10 @@ FFTLIB_STATUS check_i16(const void* pX, const FFTLIB_bufParams1D_t* bX, const vo
     if (p4 != bW->dim_x && p4 * 2u != bW->dim_x) return FFTLIB_ERR_INVALID_DIMENSION;
     return FFTLIB_SUCCESS;
 }
+
+} // namespace
+
+namespace fftb200 {
 
 // ---- execution ----------------------------------------------------------------
 
@@ -180,13 +190,14 @@ FFTLIB_STATUS exec_c2r(float* pX, float* pXFFT, float* pY, uint32_t n, uint32_t 
         if (!plan) return cuda_fail(e, "plan creation");
     }
     DeviceScope scope(plan->device);
-    if (plan->fourStep && !pXFFT) {
+    const bool scratch = c2r_needs_scratch(plan, inmode);
+    if (scratch && !pXFFT) {
         set_error("pXFFT work buffer required for numPoints %u", n);
         return FFTLIB_ERR_NULL_POINTER;
     }
     const size_t nIn = inmode ? n : h + 1u;
     std::vector<ChannelBuf> bufs = {{pX, nIn * sizeof(float2), true, false},
-                                    {plan->fourStep ? pXFFT : nullptr, (size_t)h * sizeof(float2), false, false},
+                                    {scratch ? pXFFT : nullptr, (size_t)h * sizeof(float2), false, false},
                                     {pY, (size_t)n * sizeof(float), false, true}};
     cudaError_t e = run_channels(bufs, c, [&](const std::vector<void*>& d, uint32_t, uint32_t cnt, cudaStream_t s) {
         return run_c2r(plan, (const float2*)d[0], (float2*)d[1], (float*)d[2], cnt, inmode, s);
@@ -221,9 +232,8 @@ FFTLIB_STATUS exec_i16(int16_t* pX, const int16_t* pW, int16_t* pY, const uint32
     return FFTLIB_SUCCESS;
 }
 
-FFTLIB_STATUS init_fp32(void* pBlock, uint32_t kind, uint32_t n, uint32_t c, uint32_t mode)
+FFTLIB_STATUS init_fp32(void* pBlock, uint32_t kind, uint32_t n, uint32_t c, uint32_t mode, bool real)
 {
-    const bool real = kind == REC_R2C || kind == REC_C2R;
     if (real && (n & 1u)) {
         set_error("numPoints %u is odd", n);
         return FFTLIB_ERR_INVALID_DIMENSION;
@@ -234,7 +244,7 @@ FFTLIB_STATUS init_fp32(void* pBlock, uint32_t kind, uint32_t n, uint32_t c, uin
     return write_record(pBlock, kind, n, c, mode, plan);
 }
 
-} // namespace
+} // namespace fftb200
 
 extern "C" {
 
@@ -268,7 +278,7 @@ FFTLIB_STATUS FFTLIB_fft1dBatched_i32fc_c32fc_o32fc_init(FFTLIB_F32* pX, FFTLIB_
     FFTLIB_STATUS st = FFTLIB_fft1dBatched_i32fc_c32fc_o32fc_checkParams(pX, bufParamsX, pW, bufParamsW, pY, bufParamsY,
                                                                          numPoints, numChannels, pBlock);
     if (st != FFTLIB_SUCCESS) return st;
-    return init_fp32(pBlock, REC_C2C, numPoints, numChannels, 0);
+    return init_fp32(pBlock, REC_C2C, numPoints, numChannels, 0, false);
 }
 
 FFTLIB_STATUS FFTLIB_fft1dBatched_i32fc_c32fc_o32fc_kernel(FFTLIB_F32* pX, FFTLIB_bufParams1D_t* bufParamsX,
@@ -324,7 +334,7 @@ FFTLIB_STATUS FFTLIB_ifft1dBatched_i32fc_c32fc_o32fc_init(FFTLIB_F32* pX, FFTLIB
     FFTLIB_STATUS st = FFTLIB_ifft1dBatched_i32fc_c32fc_o32fc_checkParams(pX, bufParamsX, pW, bufParamsW, pY,
                                                                           bufParamsY, numPoints, numChannels, pBlock);
     if (st != FFTLIB_SUCCESS) return st;
-    return init_fp32(pBlock, REC_IFFT, numPoints, numChannels, 0);
+    return init_fp32(pBlock, REC_IFFT, numPoints, numChannels, 0, false);
 }
 
 FFTLIB_STATUS FFTLIB_ifft1dBatched_i32fc_c32fc_o32fc_kernel(FFTLIB_F32* pX, FFTLIB_bufParams1D_t* bufParamsX,
@@ -385,7 +395,7 @@ FFTLIB_STATUS FFTLIB_fft1dBatched_i32f_c32fc_o32fc_init(FFTLIB_F32* pX, FFTLIB_b
                                                                         numPoints, numChannels, outmode, pBlock);
     if (st != FFTLIB_SUCCESS) return st;
     if (!pBlock) return FFTLIB_ERR_NULL_POINTER;
-    return init_fp32(pBlock, REC_R2C, numPoints, numChannels, outmode);
+    return init_fp32(pBlock, REC_R2C, numPoints, numChannels, outmode, true);
 }
 
 FFTLIB_STATUS FFTLIB_fft1dBatched_i32f_c32fc_o32fc_kernel(FFTLIB_F32* pX, FFTLIB_bufParams1D_t* bufParamsX,
@@ -455,7 +465,7 @@ FFTLIB_STATUS FFTLIB_ifft1dBatched_i32fc_c32fc_o32f_init(FFTLIB_F32* pX, FFTLIB_
                                                                          numPoints, numChannels, inMode, pBlock);
     if (st != FFTLIB_SUCCESS) return st;
     if (!pBlock) return FFTLIB_ERR_NULL_POINTER;
-    return init_fp32(pBlock, REC_C2R, numPoints, numChannels, inMode);
+    return init_fp32(pBlock, REC_C2R, numPoints, numChannels, inMode, true);
 }
 
 FFTLIB_STATUS FFTLIB_ifft1dBatched_i32fc_c32fc_o32f_kernel(FFTLIB_F32* pX, FFTLIB_bufParams1D_t* bufParamsX,

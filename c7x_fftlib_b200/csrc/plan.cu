@@ -490,12 +490,37 @@ cudaError_t run_r2c(const ComplexPlan* p, float* x, float2* scratch, float2* y, 
     return launch_fft(a, p->eng.emax, s);
 }
 
+namespace {
+
+// The single-kernel c2r stages a whole input row (inCount bins) in the
+// transform's shared-memory region; the full spectrum (inMode 1) of the
+// longest single-kernel lengths does not fit in one CTA's 227 KB.
+bool c2r_staged_fits(uint32_t h, uint32_t inCount)
+{
+    return (size_t)smem_len(std::max(h, inCount)) * sizeof(float2) <= 227u * 1024u;
+}
+
+} // namespace
+
+bool c2r_needs_scratch(const ComplexPlan* p, int inmode)
+{
+    const uint32_t h = p->n;
+    return p->fourStep || !c2r_staged_fits(h, inmode ? 2u * h : h + 1u);
+}
+
 cudaError_t run_c2r(const ComplexPlan* p, const float2* x, float2* scratch, float* y, uint32_t batch, int inmode,
                     cudaStream_t s)
 {
     if (batch == 0) return cudaSuccess;
     const uint32_t h = p->n;
     const uint32_t inCount = inmode ? 2u * h : h + 1u;
+    if (!p->fourStep && !c2r_staged_fits(h, inCount)) {
+        // split as a pre-pass into the work buffer, then the plain inverse
+        if (!scratch) return cudaErrorInvalidValue;
+        cudaError_t e = launch_c2r_pre(x, scratch, p->twSplit, h, batch, inmode, s);
+        if (e != cudaSuccess) return e;
+        return run_c2c(p, scratch, (float2*)y, batch, true, s);
+    }
     if (p->fourStep) {
         if (!scratch) return cudaErrorInvalidValue;
         cudaError_t e = launch_c2r_pre(x, scratch, p->twSplit, h, batch, inmode, s);

@@ -95,7 +95,9 @@ cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batc
 // (needed only for the four-step path); y: batch x (h+1) or x 2h bins.
 cudaError_t run_r2c(const ComplexPlan* p, float* x, float2* scratch, float2* y, uint32_t batch, int outmode,
                     cudaStream_t s);
-// x: batch x (h+1) or x 2h bins; y: batch x 2h reals.
+// x: batch x (h+1) or x 2h bins; y: batch x 2h reals. scratch (batch x h
+// complex) is needed when c2r_needs_scratch says so.
+bool c2r_needs_scratch(const ComplexPlan* p, int inmode);
 cudaError_t run_c2r(const ComplexPlan* p, const float2* x, float2* scratch, float* y, uint32_t batch,
                     int inmode, cudaStream_t s);
 

@@ -7,6 +7,7 @@
 
 #include "fftlib_b200/FFTLIB_types.h"
 #include "fftlib_b200/fft_c7x.h"
+#include "fftlib_b200/fft1d_c7x.h"
 #include "fftlib_b200/fft_c7xmma.h"
 #include "fftlib_b200/fftlib_b200_ext.h"
 

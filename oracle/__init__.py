@@ -331,6 +331,104 @@ def ref_c2c_i16(x, n, channels, shifts, w=None):
 
 
 # --------------------------------------------------------------------------
+# Single-transform kernels FFTLIB_{fft,ifft}1d_* (length from dim_x)
+#
+# Restatement: each is the batched kernel with one channel --
+#   fft1d c2c / ifft1d c2c : FFTLIB_{fft,ifft}1d_i32fc_c32fc_o32fc_cn.c, the
+#       same mixed-radix DIF + digit reversal (ifft: conjugate in, conjugate
+#       and 1/N out, ..._ifft1d_i32fc_c32fc_o32fc_cn.c:436-437)
+#   fft1d r2c  : FFTLIB_fft1d_i32f_c32fc_o32fc_cn.c:34-140, the N/2-point
+#       batched c2c then the split post-process over the full spectrum
+#       (outmode 1 of the batched kernel)
+#   ifft1d c2r : FFTLIB_ifft1d_i32fc_c32fc_o32f_cn.c:39-74, the split
+#       pre-process reading bins i and i+N/2 (inMode 1) then the single
+#       N/2-point ifft
+#   fft1d int16: FFTLIB_fft1d_i16sc_c16sc_o16sc_cn.c:189-306, the batched
+#       int16 loop with one channel
+# --------------------------------------------------------------------------
+
+def fft1d_c2c_f32(x: np.ndarray, n: int, inverse: bool = False) -> np.ndarray:
+    return fft_c2c_f32(x, n, 1, inverse)
+
+
+def fft1d_r2c_f32(x: np.ndarray, n: int) -> np.ndarray:
+    return fft_r2c_f32(x, n, 1, 1)
+
+
+def fft1d_c2r_f32(x: np.ndarray, n: int) -> np.ndarray:
+    return fft_c2r_f32(x, n, 1, 1)
+
+
+def fft1d_c2c_i16(x: np.ndarray, n: int, shifts) -> np.ndarray:
+    return fft_c2c_i16(x, n, 1, shifts)
+
+
+def ref1d_available() -> bool:
+    return all(os.path.exists(os.path.join(REF_DIR, f"libref_1d_{k}.so"))
+               for k in ("c2c", "ifft", "r2c", "c2r", "i16"))
+
+
+def ref_fft1d_c2c_f32(x, n, inverse=False, w=None):
+    """Reference FFTLIB_{fft,ifft}1d_i32fc_c32fc_o32fc_cn (dim_x = 2n)."""
+    xin = np.ascontiguousarray(x, np.float32).copy()
+    y = np.zeros(max(2 * n, 2), np.float32)
+    w = ref_tw_gen_c2c(n) if w is None else np.ascontiguousarray(w, np.float32)
+    L = ref_lib("1d_ifft" if inverse else "1d_c2c")
+    fn = L.FFTLIB_ifft1d_i32fc_c32fc_o32fc_cn if inverse else L.FFTLIB_fft1d_i32fc_c32fc_o32fc_cn
+    b = _bp(FFTLIB_FLOAT32, 2 * n)
+    rc = fn(_vp(xin), b, _vp(w), b, _vp(y), b)
+    if rc:
+        raise ValueError(f"reference fft1d c2c returned {rc}")
+    return y[: 2 * n]
+
+
+def ref_fft1d_r2c_f32(x, n):
+    """Reference FFTLIB_fft1d_i32f_c32fc_o32fc_cn (dim_x = n). Its output
+    buffer gets one spare bin: the reference also stores bin n (the conjugate
+    of bin 0) there."""
+    xin = np.ascontiguousarray(x, np.float32).copy()
+    y = np.zeros(2 * (n + 1), np.float32)
+    xfft = np.zeros(2 * (n + 1), np.float32)
+    w = ref_tw_gen_r2c(n)
+    sf = ref_split_factor_r2c(n)
+    b = _bp(FFTLIB_FLOAT32, n)
+    rc = ref_lib("1d_r2c").FFTLIB_fft1d_i32f_c32fc_o32fc_cn(_vp(xin), b, _vp(w), b, _vp(xfft), b, _vp(sf), b,
+                                                             _vp(y), b)
+    if rc:
+        raise ValueError(f"reference fft1d r2c returned {rc}")
+    return y[: 2 * n]
+
+
+def ref_fft1d_c2r_f32(x, n):
+    """Reference FFTLIB_ifft1d_i32fc_c32fc_o32f_cn (dim_x = n; n bins in)."""
+    xin = np.ascontiguousarray(x, np.float32).copy()
+    y = np.zeros(max(n, 2), np.float32)
+    xfft = np.zeros(2 * (n + 1), np.float32)
+    w = ref_tw_gen_c2r(n)
+    sf = ref_split_factor_c2r(n)
+    b = _bp(FFTLIB_FLOAT32, n)
+    rc = ref_lib("1d_c2r").FFTLIB_ifft1d_i32fc_c32fc_o32f_cn(_vp(xin), b, _vp(w), b, _vp(xfft), b, _vp(sf), b,
+                                                              _vp(y), b)
+    if rc:
+        raise ValueError(f"reference ifft1d c2r returned {rc}")
+    return y[:n]
+
+
+def ref_fft1d_c2c_i16(x, n, shifts, w=None):
+    """Reference FFTLIB_fft1d_i16sc_c16sc_o16sc_cn (dim_x = 2n)."""
+    xin = np.ascontiguousarray(x, np.int16).copy()
+    y = np.zeros(2 * n, np.int16)
+    w = ref_tw_gen_i16(n) if w is None else np.ascontiguousarray(w, np.int16)
+    sh = np.ascontiguousarray(shifts, np.uint32)
+    b = _bp(FFTLIB_INT16, 2 * n)
+    rc = ref_lib("1d_i16").FFTLIB_fft1d_i16sc_c16sc_o16sc_cn(_vp(xin), b, _vp(w), b, _vp(y), b, _vp(sh),
+                                                              _bp(FFTLIB_UINT32, len(sh)))
+    if rc:
+        raise ValueError(f"reference fft1d int16 returned {rc}")
+    return y
+
+
+# --------------------------------------------------------------------------
 # Seeded synthetic inputs (splitmix64-free: numpy PCG64 with a fixed seed)
 # --------------------------------------------------------------------------
 

@@ -22,6 +22,20 @@ fixtures themselves):
   does) on seeded inputs.
 * ``ref_cn.npz`` -- outputs of the reference's own ``_cn`` C code
   (oracle/_ref) on seeded inputs, for every batched kernel.
+* ``fft1d_r2c_static.npz`` / ``fft1d_c2r_static.npz`` -- the reference's
+  committed static vectors for the single-transform real-input kernels
+  (test/fft_c7x/FFTLIB_fft1d_i32f_c32fc_o32fc/test_data/extended_test_cases,
+  test/fft_c7x/FFTLIB_ifft1d_i32fc_c32fc_o32f/test_data/extended_test_cases),
+  numPoints from the test drivers' parameter tables (..._idat.c).
+* ``fft1d_i16_pymodel.npz`` -- outputs of the reference's bit-exact Python
+  model of the single-transform int16 kernel (test/fft_c7x/FFTLIB_idat_gen/
+  FFTLIB_fft1d_i16sc_c16sc_o16sc/fft1d_i16sc_c16sc_o16sc.py) on the cases of
+  its test_cases_list.csv, seeded inputs in its range [-1000, 1000], stored
+  as the reference C _cn result with a flag for whether the model agrees.
+* ``fft1d_c2c_pymodel.npz`` -- outputs of the reference's Python generators
+  of the single-transform c2c and ifft c2c on seeded inputs.
+
+``--only NAME[,NAME]`` regenerates just the named fixtures (file stems).
 """
 from __future__ import annotations
 
@@ -188,19 +202,113 @@ def ref_cn():
     return d
 
 
+IDAT_RE = re.compile(r"STATIC,\s*//[^\n]*\n\s*staticRefIn(\d+),[^\n]*\n[^\n]*\n\s*(\d+),\s*// numPoints")
+
+
+def single_static(ref, kernel):
+    """The single-transform real-input kernels' static vectors: every
+    staticRefCase file, with numPoints from the driver's parameter table,
+    kept if the oracle reproduces it within the driver's own tolerance
+    (r2c 2^-3: FFTLIB_fft1d_i32f_c32fc_o32fc_d.c:194; c2r 0.1:
+    FFTLIB_ifft1d_i32fc_c32fc_o32f_d.c:192)."""
+    r2c = "i32f_c32fc" in kernel
+    tdir = os.path.join(ref, "test", "fft_c7x", kernel)
+    with open(os.path.join(tdir, kernel + "_idat.c")) as f:
+        npts = {int(i): int(n) for i, n in IDAT_RE.findall(f.read())}
+    base = os.path.join(tdir, "test_data", "extended_test_cases")
+    d, ids = {}, []
+    for fn in sorted(os.listdir(base)):
+        m = re.fullmatch(r"staticRefCase(\d+)\.h", fn)
+        if not m:
+            continue
+        cid = int(m.group(1))
+        arr = parse_c_arrays(os.path.join(base, fn))
+        xin, yout, n = arr[f"staticRefIn{cid}"], arr[f"staticRefOut{cid}"], npts[cid]
+        got = O.fft1d_r2c_f32(xin, n) if r2c else O.fft1d_c2r_f32(xin, n)
+        err = float(np.abs(got - yout).max())
+        if err > (2.0 ** -3 if r2c else 0.1):
+            print(f"skip {kernel} static case {cid}: oracle differs by {err}")
+            continue
+        ids.append(cid)
+        d[f"n_{cid}"] = np.array(n)
+        d[f"in_{cid}"] = xin.astype(np.float32)
+        d[f"out_{cid}"] = yout.astype(np.float32)
+    d["ids"] = np.array(sorted(ids))
+    return d
+
+
+def fft1d_i16_pymodel(ref):
+    """Cases of the model's CSV (one of its two 16384-point rows). ``out`` is
+    the reference C _cn result; ``model_agrees`` says whether the Python
+    model gives the same bits: it does unless a 16-bit intermediate
+    overflows, which the model keeps in unbounded Python integers where the
+    C code wraps (FFTLIB_fft1d_i16sc_c16sc_o16sc_cn.c:107-136)."""
+    gen = os.path.join(ref, "test", "fft_c7x", "FFTLIB_idat_gen", "FFTLIB_fft1d_i16sc_c16sc_o16sc")
+    cls = load_module(os.path.join(gen, "fft1d_i16sc_c16sc_o16sc.py"), "ref_i16_single").FFTLIB_fft1d_i16sc_c16sc_o16sc
+    with open(os.path.join(gen, "test_cases_list.csv")) as f:
+        rows = [(int(r["ID"]), int(r["numPoints"]), [int(v) for v in r["shiftVector"].strip("[]").split(",")])
+                for r in csv.DictReader(f)]
+    rows = [r for r in rows if r[0] != 13]
+    d = {"n_cases": np.array(len(rows))}
+    for i, (cid, n, sh) in enumerate(rows):
+        x = O.int16_input(n, 1, 6000 + cid, -1000, 1000)
+        g = x.astype(np.float64).reshape(n, 2)
+        model = cls(n, list(sh))
+        out = np.asarray(model.exec(g[:, 0] + 1j * g[:, 1]))
+        ym = np.stack([out.real, out.imag], -1).astype(np.int16).ravel()
+        yr = O.ref_fft1d_c2c_i16(x, n, sh, np.array(model.pW, np.int16))
+        d[f"case{i}_n"] = np.array(n)
+        d[f"case{i}_shift"] = np.array(sh, np.uint32)
+        d[f"case{i}_in"] = x
+        d[f"case{i}_out"] = yr
+        d[f"case{i}_model_agrees"] = np.array(int(np.array_equal(ym, yr)))
+        if n <= 4096:
+            d[f"tw_{n}"] = np.array(model.pW, np.int16)
+    return d
+
+
+def fft1d_c2c_pymodel(ref):
+    gen = os.path.join(ref, "test", "fft_c7x", "FFTLIB_idat_gen")
+    fwd = load_module(os.path.join(gen, "FFTLIB_fft1d_i32fc_c32fc_o32fc", "fft1d_i32fc_c32fc_o32fc.py"),
+                      "ref_c2c_single").FFTLIB_fft1d_i32fc_c32fc_o32fc
+    inv = load_module(os.path.join(gen, "FFTLIB_ifft1d_i32fc_c32fc_o32fc", "ifft1d_i32fc_c32fc_o32fc.py"),
+                      "ref_ifft_single").FFTLIB_ifft1d_i32fc_c32fc_o32fc
+    sizes = [16, 60, 256, 1000, 4096]
+    d = {"sizes": np.array(sizes)}
+    for i, n in enumerate(sizes):
+        x = O.uniform_c2c(n, 1, 7000 + i)
+        z = O.as_complex(x, n, 1)[0]
+        yf = fwd(n).exec(z)
+        yi = inv(n).exec(z)
+        d[f"case{i}_in"] = x
+        d[f"case{i}_fwd"] = np.stack([yf.real, yf.imag], -1).ravel().astype(np.float32)
+        d[f"case{i}_inv"] = np.stack([yi.real, yi.imag], -1).ravel().astype(np.float32)
+    return d
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default="")
     a = ap.parse_args()
-    if not O.ref_available():
+    if not (O.ref_available() and O.ref1d_available()):
         O.build(a.ref)
-    np.savez_compressed(os.path.join(HERE, "r2c_extended.npz"),
-                        **extended(a.ref, "FFTLIB_fft1dBatched_i32f_c32fc_o32fc", "outmode", 1 << 20))
-    np.savez_compressed(os.path.join(HERE, "c2r_extended.npz"),
-                        **extended(a.ref, "FFTLIB_ifft1dBatched_i32fc_c32fc_o32f", "inMode", 1 << 20))
-    np.savez_compressed(os.path.join(HERE, "i16_pymodel.npz"), **i16_pymodel(a.ref))
-    np.savez_compressed(os.path.join(HERE, "c2c_pymodel.npz"), **c2c_pymodel(a.ref))
-    np.savez_compressed(os.path.join(HERE, "ref_cn.npz"), **ref_cn())
+    makers = {
+        "r2c_extended": lambda: extended(a.ref, "FFTLIB_fft1dBatched_i32f_c32fc_o32fc", "outmode", 1 << 20),
+        "c2r_extended": lambda: extended(a.ref, "FFTLIB_ifft1dBatched_i32fc_c32fc_o32f", "inMode", 1 << 20),
+        "i16_pymodel": lambda: i16_pymodel(a.ref),
+        "c2c_pymodel": lambda: c2c_pymodel(a.ref),
+        "ref_cn": ref_cn,
+        "fft1d_r2c_static": lambda: single_static(a.ref, "FFTLIB_fft1d_i32f_c32fc_o32fc"),
+        "fft1d_c2r_static": lambda: single_static(a.ref, "FFTLIB_ifft1d_i32fc_c32fc_o32f"),
+        "fft1d_i16_pymodel": lambda: fft1d_i16_pymodel(a.ref),
+        "fft1d_c2c_pymodel": lambda: fft1d_c2c_pymodel(a.ref),
+    }
+    only = [s for s in a.only.split(",") if s]
+    for name, make in makers.items():
+        if only and name not in only:
+            continue
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **make())
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(HERE, fn)))

@@ -157,6 +157,18 @@ def test_r2c_c2r_vs_fp64(gpu, n, mode):
     assert O.rel_l2(xr, x) <= REL_L2
 
 
+@pytest.mark.parametrize("n", [27648, 28800, 32000, 32768])
+def test_c2r_full_spectrum_longest_single_kernel(gpu, n):
+    """inMode 1 at the longest single-kernel half lengths (13824..16384),
+    whose staged full-spectrum row exceeds a CTA's shared memory: the split
+    runs as a pre-pass into pXFFT."""
+    x = O.real_signal(n, 2, seed=n + 3)
+    y = fftcall.r2c(x, n, 2, outmode=1)
+    assert O.rel_l2(O.as_complex(y, n, 2), O.fp64_r2c(x, n, 2, 1)) <= REL_L2
+    xr = fftcall.c2r(y, n, 2, inmode=1)
+    assert O.rel_l2(xr, O.fp64_c2r(y, n, 2, 1).ravel()) <= REL_L2
+
+
 @pytest.mark.parametrize("n,ch,mode", [(4096, 2, 0), (4096, 2, 1), (480, 3, 0), (250, 1, 1), (64, 4, 0), (6, 2, 0)])
 def test_r2c_c2r_vs_reference_cn(gpu, ref_cn, n, ch, mode):
     x = O.real_signal(n, ch, seed=4000 + n)
