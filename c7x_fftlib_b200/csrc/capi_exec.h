@@ -23,7 +23,7 @@ FFTLIB_STATUS read_record(void* pBlock, uint32_t kind, uint32_t n, PlanRecord* o
 FFTLIB_STATUS exec_c2c(float* pX, float* pY, uint32_t n, uint32_t c, bool inverse, ComplexPlan* plan);
 // FP32 real-input forward / real-output inverse over c channels of n reals
 // (outmode / inmode 0: n/2+1 bins per channel, 1: n bins). pXFFT is the
-// work buffer the four-step lengths (n/2 > kMaxSingleN) need.
+// work buffer the global-pass lengths (n/2 > kMaxSingleN) need.
 FFTLIB_STATUS exec_r2c(float* pX, float* pXFFT, float* pY, uint32_t n, uint32_t c, int outmode, ComplexPlan* plan);
 FFTLIB_STATUS exec_c2r(float* pX, float* pXFFT, float* pY, uint32_t n, uint32_t c, int inmode, ComplexPlan* plan);
 // int16 radix-4 transform with per-stage shifts (pW: the Q15 table of n).

@@ -92,15 +92,17 @@ FFTLIB_STATUS FFTLIB_b200_describePlan(uint32_t numPoints, char* buf, uint32_t l
     std::string s;
     EnginePlan e;
     if (!is_235(numPoints)) return FFTLIB_ERR_INVALID_DIMENSION;
-    uint32_t n1 = 0, n2 = 0;
+    int G = 0;
+    uint32_t R[kMaxGlobal];
     if (plan_engine(numPoints, &e)) {
         s = describe(e);
-    } else if (split_four_step(numPoints, &n1, &n2)) {
-        EnginePlan e1, e2;
-        plan_engine(n1, &e1);
-        plan_engine(n2, &e2);
-        s = "four-step " + std::to_string(n1) + "x" + std::to_string(n2) + " [" + describe(e1) + "] [" +
-            describe(e2) + "]";
+    } else if (split_global(numPoints, &G, R)) {
+        s = "global passes";
+        for (int g = 0; g < G; ++g) {
+            EnginePlan eg;
+            plan_engine(R[g], &eg);
+            s += (g ? " x " : " ") + std::to_string(R[g]) + " [" + describe(eg) + "]";
+        }
     } else {
         return FFTLIB_ERR_NOT_IMPLEMENTED;
     }
@@ -140,7 +142,7 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32f_c32fc_o32fc_kernelAsync(FFTLIB_F32* 
     FFTLIB_STATUS st = async_record(pBlock, REC_R2C, numPoints, &r);
     if (st != FFTLIB_SUCCESS) return st;
     if (outmode > 1) return FFTLIB_ERR_INVALID_OUTMODE;
-    if (r.plan->fourStep && !pXFFT) return FFTLIB_ERR_NULL_POINTER;
+    if (r.plan->multiPass && !pXFFT) return FFTLIB_ERR_NULL_POINTER;
     return launched(run_r2c(r.plan, pX, (float2*)pXFFT, (float2*)pY, numChannels, outmode, (cudaStream_t)stream),
                     "fft1dBatched r2c");
 }

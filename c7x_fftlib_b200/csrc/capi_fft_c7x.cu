@@ -162,13 +162,13 @@ FFTLIB_STATUS exec_r2c(float* pX, float* pXFFT, float* pY, uint32_t n, uint32_t 
         if (!plan) return cuda_fail(e, "plan creation");
     }
     DeviceScope scope(plan->device);
-    if (plan->fourStep && !pXFFT) {
+    if (plan->multiPass && !pXFFT) {
         set_error("pXFFT work buffer required for numPoints %u", n);
         return FFTLIB_ERR_NULL_POINTER;
     }
     const size_t nOut = outmode ? n : h + 1u;
     std::vector<ChannelBuf> bufs = {{pX, (size_t)n * sizeof(float), true, false},
-                                    {plan->fourStep ? pXFFT : nullptr, (size_t)h * sizeof(float2), false, false},
+                                    {plan->multiPass ? pXFFT : nullptr, (size_t)h * sizeof(float2), false, false},
                                     {pY, nOut * sizeof(float2), false, true}};
     cudaError_t e = run_channels(bufs, c, [&](const std::vector<void*>& d, uint32_t, uint32_t cnt, cudaStream_t s) {
         return run_r2c(plan, (float*)d[0], (float2*)d[1], (float2*)d[2], cnt, outmode, s);

@@ -88,8 +88,8 @@ cudaError_t enqueue(const MmaHandle* m, const float* x, const float* w, float* y
     if (m->path == PATH_TC && aligned)
         return launch_tc_dft(m->init.fftSize, reinterpret_cast<const float2*>(x), reinterpret_cast<float2*>(y), w,
                              batch, error_word().dev, s);
-    // above 16384 points the FFT uses pX as four-step scratch, as the
-    // fft1dBatched kernels do
+    // above 16384 points the FFT may use pX as scratch of its global passes,
+    // as the fft1dBatched kernels do
     return run_c2c(m->plan, const_cast<float2*>(reinterpret_cast<const float2*>(x)), reinterpret_cast<float2*>(y),
                    batch, false, s);
 }

@@ -62,10 +62,6 @@ struct FftArgs {
     float    scale;              // applied on store
     int32_t  batchMinor;         // thread layout: transform index fastest
     int32_t  staged;             // tile through shared memory on load/store
-    // four-step column step: output k of transform b is multiplied by
-    // twBig[b * k] = W_bigN^{b k}
-    const float2* twBig;
-    uint32_t bigN;
     // real-input kernels (N = h = half the real length)
     int32_t  ioMode;             // IoMode
     int32_t  realMode;           // r2c outmode / c2r inMode
@@ -78,6 +74,27 @@ struct FftArgs {
     uint32_t inMagic;            // fastdiv_magic(inCount)
     // error word (host-visible); kernels with bounded waits report here
     uint32_t* err;
+    // global Stockham pass (perCh != 0): transform b is column j = b mod
+    // perCh of channel c = b / perCh; it reads from c * inChStride +
+    // j * inBatch and writes to c * outChStride + (j / outGroup) *
+    // outGroupStride + (j mod outGroup) * outBatch (outGroup 0: j * outBatch)
+    uint32_t perCh;
+    uint32_t outGroup;
+    int64_t  inChStride, outChStride, outGroupStride;
+    // its input twiddle: element q of column j is multiplied by W_n^p,
+    // p = q (j mod twNs) twStep, as twLo[p mod 2^twLoBits] * twHi[p >> twLoBits]
+    const float2* twLo;
+    const float2* twHi;
+    uint32_t twLoBits;
+    uint32_t twNs;
+    uint32_t twStep;
+    // staged tiles of M transforms computed Mc at a time (T * Mc threads;
+    // 0: Mc = M); mMagic = fastdiv_magic(M)
+    uint32_t Mc;
+    uint32_t mMagic;
 };
+
+// Transforms one CTA computes at a time (its threads: T of them each).
+inline FFTB_HD uint32_t tile_group(const FftArgs& a) { return a.Mc && a.staged ? a.Mc : a.M; }
 
 } // namespace fftb200

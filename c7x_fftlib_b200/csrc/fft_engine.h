@@ -34,9 +34,11 @@ struct StaticEntry {
     cudaError_t (*launchPipelined)(const FftArgs&, cudaStream_t);
 };
 const std::vector<StaticEntry>& static_schedules();
+// maxThreads of the compiled fixed-size kernel for this schedule, or 0.
+int static_max_threads(uint32_t n, int emax, uint32_t T, int P, const int* R);
 
-// W[i] = exp(-2 pi i (i mod n) / n), i < count, computed in FP64.
-cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s);
+// W[i] = exp(-2 pi i (i stride mod n) / n), i < count, computed in FP64.
+cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s, uint32_t stride = 1);
 
 // Per-pass twiddle blocks: pass j occupies entries off[j] .. off[j] +
 // (R[j]-1)*Ns[j]; entry off + (q-1)*Ns + k = W_{Ns*R}^{q*k}, computed in FP64.

@@ -43,7 +43,7 @@ cudaError_t launch_generic(const FftArgs& a, cudaStream_t s)
     cudaError_t e = ensure_smem<EMAX, MAXT>(smem);
     if (e != cudaSuccess) return e;
     const uint32_t grid = (a.batch + a.M - 1) / a.M;
-    k_fft_stockham<EMAX, MAXT><<<grid, a.T * a.M, smem, s>>>(a);
+    k_fft_stockham<EMAX, MAXT><<<grid, a.T * tile_group(a), smem, s>>>(a);
     return cudaGetLastError();
 }
 

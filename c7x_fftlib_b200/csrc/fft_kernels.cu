@@ -10,14 +10,14 @@ extern template cudaError_t launch_generic<8, 1024>(const FftArgs&, cudaStream_t
 extern template cudaError_t launch_generic<16, 512>(const FftArgs&, cudaStream_t);
 extern template cudaError_t launch_generic<32, 512>(const FftArgs&, cudaStream_t);
 
-// W[i] = exp(-2 pi i (i mod n) / n) for i < count, evaluated in FP64 with
-// the angle reduced exactly in integers (sincospi of 2 r / n, r = i mod n)
-// and rounded once to FP32.
-__global__ void k_twiddle_f64(float2* __restrict__ w, uint32_t n, uint32_t count)
+// W[i] = exp(-2 pi i (i stride mod n) / n) for i < count, evaluated in FP64
+// with the angle reduced exactly in integers (sincospi of 2 r / n,
+// r = i stride mod n) and rounded once to FP32.
+__global__ void k_twiddle_f64(float2* __restrict__ w, uint32_t n, uint32_t count, uint32_t stride)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    const uint32_t r = i % n;
+    const uint32_t r = (uint32_t)(((uint64_t)i * stride) % n);
     double s, c;
     sincospi(2.0 * (double)r / (double)n, &s, &c);
     w[i] = make_float2((float)c, (float)(-s));
@@ -73,11 +73,22 @@ const StaticEntry* find_static(const FftArgs& a, int emax)
         if (e.n != a.N || e.emax != emax || e.T != a.T || e.P != (int)a.P) continue;
         bool same = true;
         for (int p = 0; p < e.P; ++p) same = same && (e.R[p] == a.pass[p].R);
-        if (same && a.T * a.M <= (uint32_t)e.maxThreads) return &e;
+        if (same && a.T * tile_group(a) <= (uint32_t)e.maxThreads) return &e;
     }
     return nullptr;
 }
 } // namespace
+
+int static_max_threads(uint32_t n, int emax, uint32_t T, int P, const int* R)
+{
+    for (const StaticEntry& e : static_schedules()) {
+        if (e.n != n || e.emax != emax || e.T != T || e.P != P) continue;
+        bool same = true;
+        for (int p = 0; p < P; ++p) same = same && (e.R[p] == R[p]);
+        if (same) return e.maxThreads;
+    }
+    return 0;
+}
 
 cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
 {
@@ -89,7 +100,7 @@ cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
         // the stage holds beside its padded exchange layout for N >= 64)
         const bool rowsOk = ((a.ioMode == IO_C2C || a.ioMode == IO_R2C_SPLIT) && a.inBatch == (int64_t)a.N) ||
                             (a.ioMode == IO_C2R_SPLIT && !a.realMode && a.inBatch == (int64_t)a.N + 1 && a.N >= 64u);
-        const bool pipelinable = st->launchPipelined && a.err && rowsOk && !a.batchMinor && !a.twBig &&
+        const bool pipelinable = st->launchPipelined && a.err && rowsOk && !a.batchMinor && !a.perCh &&
                                  a.inElem == 1 && a.outElem == 1 && ((uintptr_t)a.in & 15u) == 0 &&
                                  (a.N % 2u) == 0;
         if (pipelinable) {
@@ -114,10 +125,10 @@ cudaError_t launch_twiddle_passes(float2* w, const TwiddlePasses& tp, cudaStream
     return cudaGetLastError();
 }
 
-cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s)
+cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s, uint32_t stride)
 {
     if (count == 0) return cudaSuccess;
-    k_twiddle_f64<<<(count + 255) / 256, 256, 0, s>>>(w, n, count);
+    k_twiddle_f64<<<(count + 255) / 256, 256, 0, s>>>(w, n, count, stride);
     return cudaGetLastError();
 }
 

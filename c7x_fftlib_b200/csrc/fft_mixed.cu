@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(BLK) k_fft_mixed(const MixedGroup* __restrict_
         float2 v[EMAX];
         for (int p = 0; p < (int)a.P; ++p) {
             dispatch_radix<EMAX>(a.pass[p].R, [&](auto r) {
-                run_pass<EMAX, decltype(r)::value>(a, a.pass[p], p == 0, p + 1 == (int)a.P, T, v, sm, t, 0, active,
+                run_pass<EMAX, decltype(r)::value>(a, a.pass[p], p == 0, p + 1 == (int)a.P, T, v, sm, t, active,
                                                    rowIn, rowOut);
             });
         }

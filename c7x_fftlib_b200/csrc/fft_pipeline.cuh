@@ -232,10 +232,10 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
             if constexpr (P == 0) {
-                run_pass<S::EMAX, S::R[P]>(a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, gidx,
+                run_pass<S::EMAX, S::R[P]>(a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t,
                                            active, nullptr, rowOut, st + shift + m * (uint32_t)IC, refill);
             } else {
-                run_pass<S::EMAX, S::R[P]>(a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, gidx,
+                run_pass<S::EMAX, S::R[P]>(a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t,
                                            active, nullptr, rowOut);
             }
         });

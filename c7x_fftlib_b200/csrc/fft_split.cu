@@ -1,6 +1,6 @@
 // fft_split.cu -- stand-alone split passes of the real-input kernels, used
-// when the half-length complex transform is too long for one CTA (the
-// four-step path); shorter transforms fuse these into the FFT kernel.
+// when the half-length complex transform is too long for one CTA (global
+// passes); shorter transforms fuse these into the FFT kernel.
 //   r2c post-process: FFTLIB_fft1dBatched_i32f_c32fc_o32fc_cn.c:40-121
 //   c2r pre-process:  FFTLIB_ifft1dBatched_i32fc_c32fc_o32f_cn.c:35-83
 #include "fft_device.cuh"

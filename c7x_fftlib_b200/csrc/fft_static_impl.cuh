@@ -26,7 +26,7 @@ template <class S, int MAXT>
 cudaError_t launch_static(const FftArgs& a, cudaStream_t s)
 {
     const size_t smem = (size_t)a.M * a.slen * sizeof(float2);
-    if (a.T != (uint32_t)S::T || a.T * a.M > (uint32_t)MAXT) return cudaErrorInvalidConfiguration;
+    if (a.T != (uint32_t)S::T || a.T * tile_group(a) > (uint32_t)MAXT) return cudaErrorInvalidConfiguration;
     if (smem > 48u * 1024u) {
         static std::mutex mu;
         static size_t configured[64] = {};
@@ -41,7 +41,7 @@ cudaError_t launch_static(const FftArgs& a, cudaStream_t s)
         }
     }
     const uint32_t grid = (a.batch + a.M - 1) / a.M;
-    k_fft_static<S, MAXT><<<grid, a.T * a.M, smem, s>>>(a);
+    k_fft_static<S, MAXT><<<grid, a.T * tile_group(a), smem, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -105,11 +105,10 @@ FFT_DEV uint32_t swz_step(uint32_t swzBase, uint32_t idx0, uint32_t q, uint32_t 
 // raw: when not null, the first pass reads its input from this unpadded
 // shared-memory copy of the transform (filled by a bulk async copy).
 // afterGather runs right after the barrier that ends the pass's reads.
-// rowIn / rowOut: this lane's transform in HBM (first / last pass); b is its
-// index in the batch (four-step column twiddle).
+// rowIn / rowOut: this lane's transform in HBM (first / last pass).
 template <int EMAX, int R, class Hook = NoHook>
 FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, const bool last,
-                      const uint32_t T, float2 (&v)[EMAX], float2* sm, uint32_t t, uint32_t b, bool active,
+                      const uint32_t T, float2 (&v)[EMAX], float2* sm, uint32_t t, bool active,
                       const float2* rowIn, float2* rowOut, const float2* raw = nullptr,
                       Hook afterGather = Hook())
 {
@@ -165,9 +164,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
                 if (j < nb) {
                     static_for<R>([&](auto q) {
                         const uint32_t idx = j + (uint32_t)q * nb;
-                        float2 z = finish(a, v[i * R + q]);
-                        if (a.twBig) z = cmul(z, __ldg(&a.twBig[b * idx]));
-                        row[(int64_t)idx * a.outElem] = z;
+                        row[(int64_t)idx * a.outElem] = finish(a, v[i * R + q]);
                     });
                 }
             });
@@ -231,14 +228,76 @@ FFT_DEV void r2c_epilogue(const FftArgs& a, const float2* sm, uint32_t t, float2
     }
 }
 
-// Cooperative, coalesced copy of the CTA's contiguous input rows into the
-// per-transform shared-memory regions.
+// Offset (complex elements) of transform b's first input / output element.
+FFT_DEV int64_t row_in(const FftArgs& a, uint32_t b)
+{
+    if (a.perCh == 0u) return (int64_t)b * a.inBatch;
+    const uint32_t c = b / a.perCh;
+    return (int64_t)c * a.inChStride + (int64_t)(b - c * a.perCh) * a.inBatch;
+}
+
+FFT_DEV int64_t row_out(const FftArgs& a, uint32_t b)
+{
+    if (a.perCh == 0u) return (int64_t)b * a.outBatch;
+    const uint32_t c = b / a.perCh;
+    const uint32_t j = b - c * a.perCh;
+    int64_t off = (int64_t)c * a.outChStride;
+    if (a.outGroup) {
+        const uint32_t g = j / a.outGroup;
+        off += (int64_t)g * a.outGroupStride + (int64_t)(j - g * a.outGroup) * a.outBatch;
+    } else {
+        off += (int64_t)j * a.outBatch;
+    }
+    return off;
+}
+
+// Cooperative, coalesced copy of the CTA's input into the per-transform
+// shared-memory regions. Rows (inElem 1): the tile's transforms lie back to
+// back. Columns (inElem != 1, a full tile of M transforms inside one
+// channel, and inside one twNs block when the input twiddle is on):
+// element i of the tile's transforms is a run of M adjacent values.
 FFT_DEV void stage_in(const FftArgs& a, float2* smem, uint32_t b0)
 {
-    const uint32_t inCount = a.inCount, inMagic = a.inMagic, slen = a.slen;
+    const uint32_t inCount = a.inCount, slen = a.slen;
     const uint32_t nm = min(a.M, a.batch - b0);
     const uint32_t total = nm * inCount;
-    const float2* src = a.in + (int64_t)b0 * a.inBatch;
+    const float2* src = a.in + row_in(a, b0);
+    if (a.inElem != 1) {
+        // U loads in flight per thread before their shared-memory stores
+        constexpr int U = 4;
+        const uint32_t j0 = a.twLo ? (b0 % a.perCh) % a.twNs : 0u;
+        const uint32_t step = blockDim.x;
+        for (uint32_t e0 = threadIdx.x; e0 < total; e0 += U * step) {
+            float2 z[U], wl[U], wh[U];
+            static_for<U>([&](auto u) {
+                const uint32_t e = e0 + (uint32_t)u * step;
+                if (e < total) {
+                    const uint32_t i = fastdiv(e, a.M, a.mMagic);
+                    const uint32_t mm = e - i * a.M;
+                    z[u] = src[(int64_t)i * a.inElem + (int64_t)mm * a.inBatch];
+                    if (a.twLo) {
+                        const uint32_t p = i * (j0 + mm) * a.twStep;
+                        wl[u] = __ldg(&a.twLo[p & ((1u << a.twLoBits) - 1u)]);
+                        wh[u] = __ldg(&a.twHi[p >> a.twLoBits]);
+                    }
+                }
+            });
+            static_for<U>([&](auto u) {
+                const uint32_t e = e0 + (uint32_t)u * step;
+                if (e < total) {
+                    const uint32_t i = fastdiv(e, a.M, a.mMagic);
+                    const uint32_t mm = e - i * a.M;
+                    // (conjIn is applied when the first pass reads the tile;
+                    // passes with an input twiddle have conjIn 0)
+                    float2 v = z[u];
+                    if (a.twLo) v = cmul(v, cmul(wl[u], wh[u]));
+                    smem[mm * slen + smem_swz(i)] = v;
+                }
+            });
+        }
+        return;
+    }
+    const uint32_t inMagic = a.inMagic;
     for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
         const uint32_t mm = fastdiv(e, inCount, inMagic);
         const uint32_t i = e - mm * inCount;
@@ -246,12 +305,22 @@ FFT_DEV void stage_in(const FftArgs& a, float2* smem, uint32_t b0)
     }
 }
 
+// Counterpart of stage_in for the outputs (columns: a full tile inside one
+// outGroup block).
 FFT_DEV void stage_out(const FftArgs& a, const float2* smem, uint32_t b0)
 {
     const uint32_t slen = a.slen;
     const uint32_t nm = min(a.M, a.batch - b0);
     const uint32_t total = nm * a.N;
-    float2* dst = a.out + (int64_t)b0 * a.outBatch;
+    float2* dst = a.out + row_out(a, b0);
+    if (a.outElem != 1) {
+        for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
+            const uint32_t i = fastdiv(e, a.M, a.mMagic);
+            const uint32_t mm = e - i * a.M;
+            dst[(int64_t)i * a.outElem + (int64_t)mm * a.outBatch] = finish(a, smem[mm * slen + smem_swz(i)]);
+        }
+        return;
+    }
     for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
         const uint32_t mm = fastdiv(e, a.N, a.nMagic);
         const uint32_t i = e - mm * a.N;
@@ -274,33 +343,37 @@ FFT_DEV void lane_of(const FftArgs& a, uint32_t T, uint32_t* m, uint32_t* t)
 
 // Whole-transform body for the CTA's transforms b0 .. b0+M-1 (schedule read
 // from a.pass at run time).
+// A staged tile of M transforms is computed in groups of Mc (a uniform loop:
+// every thread takes part in every group's barriers).
+FFT_DEV uint32_t tile_groups(const FftArgs& a) { return a.M / tile_group(a); }
+
 template <int EMAX>
 FFT_DEV void fft_tile(const FftArgs& a, float2* smem, uint32_t b0)
 {
-    uint32_t m, t;
-    lane_of(a, a.T, &m, &t);
-    const uint32_t b = b0 + m;
-    const bool active = b < a.batch;
-    float2* sm = smem + m * a.slen;
-
+    uint32_t m0, t;
+    lane_of(a, a.T, &m0, &t);
     if (a.staged) {
         stage_in(a, smem, b0);
         __syncthreads();
     }
-    const float2* rowIn = a.in + (int64_t)b * a.inBatch;
-    float2* rowOut = a.out + (int64_t)b * a.outBatch;
-    float2 v[EMAX];
-    for (int p = 0; p < (int)a.P; ++p) {
-        dispatch_radix<EMAX>(a.pass[p].R, [&](auto r) {
-            run_pass<EMAX, decltype(r)::value>(a, a.pass[p], p == 0, p + 1 == (int)a.P, a.T, v, sm, t, b, active,
-                                               rowIn, rowOut);
-        });
+    const uint32_t groups = tile_groups(a), mc = tile_group(a);
+    for (uint32_t g = 0; g < groups; ++g) {
+        const uint32_t m = g * mc + m0;
+        const uint32_t b = b0 + m;
+        const bool active = b < a.batch;
+        float2* sm = smem + m * a.slen;
+        const float2* rowIn = a.in + row_in(a, b);
+        float2* rowOut = a.out + row_out(a, b);
+        float2 v[EMAX];
+        for (int p = 0; p < (int)a.P; ++p) {
+            dispatch_radix<EMAX>(a.pass[p].R, [&](auto r) {
+                run_pass<EMAX, decltype(r)::value>(a, a.pass[p], p == 0, p + 1 == (int)a.P, a.T, v, sm, t, active,
+                                                   rowIn, rowOut);
+            });
+        }
+        if (a.ioMode == IO_R2C_SPLIT) r2c_epilogue(a, sm, t, rowOut, active);
     }
-    if (a.ioMode == IO_R2C_SPLIT) {
-        r2c_epilogue(a, sm, t, rowOut, active);
-    } else if (a.staged) {
-        stage_out(a, smem, b0);
-    }
+    if (a.staged && a.ioMode != IO_R2C_SPLIT) stage_out(a, smem, b0);
 }
 
 // Compile-time schedule: length N, register capacity EMAX, T threads per
@@ -330,29 +403,30 @@ struct StaticSchedule {
 template <class S>
 FFT_DEV void fft_tile_static(const FftArgs& a, float2* smem, uint32_t b0)
 {
-    uint32_t m, t;
-    lane_of(a, (uint32_t)S::T, &m, &t);
-    const uint32_t b = b0 + m;
-    const bool active = b < a.batch;
-    float2* sm = smem + m * a.slen;
+    uint32_t m0, t;
+    lane_of(a, (uint32_t)S::T, &m0, &t);
     if (a.staged) {
         stage_in(a, smem, b0);
         __syncthreads();
     }
-    const float2* rowIn = a.in + (int64_t)b * a.inBatch;
-    float2* rowOut = a.out + (int64_t)b * a.outBatch;
-    float2 v[S::EMAX];
-    static_for<S::P>([&](auto p) {
-        constexpr int P = decltype(p)::value;
-        constexpr PassInfo pi = S::pass(P);
-        run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, b, active, rowIn,
-                                   rowOut);
-    });
-    if (a.ioMode == IO_R2C_SPLIT) {
-        r2c_epilogue(a, sm, t, rowOut, active);
-    } else if (a.staged) {
-        stage_out(a, smem, b0);
+    const uint32_t groups = tile_groups(a), mc = tile_group(a);
+    for (uint32_t g = 0; g < groups; ++g) {
+        const uint32_t m = g * mc + m0;
+        const uint32_t b = b0 + m;
+        const bool active = b < a.batch;
+        float2* sm = smem + m * a.slen;
+        const float2* rowIn = a.in + row_in(a, b);
+        float2* rowOut = a.out + row_out(a, b);
+        float2 v[S::EMAX];
+        static_for<S::P>([&](auto p) {
+            constexpr int P = decltype(p)::value;
+            constexpr PassInfo pi = S::pass(P);
+            run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, active, rowIn,
+                                       rowOut);
+        });
+        if (a.ioMode == IO_R2C_SPLIT) r2c_epilogue(a, sm, t, rowOut, active);
     }
+    if (a.staged && a.ioMode != IO_R2C_SPLIT) stage_out(a, smem, b0);
 }
 
 } // namespace fftb200

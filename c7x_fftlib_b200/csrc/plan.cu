@@ -299,19 +299,57 @@ cudaError_t make_pass_table(float2** p, const EnginePlan& e, cudaStream_t s)
     return launch_twiddle_passes(*p, tp, s);
 }
 
-// n = n1 * n2 with n1 <= n2, n1 as close to sqrt(n) as possible, both with
-// single-kernel schedules.
-bool split_four_step(uint32_t n, uint32_t* n1, uint32_t* n2)
+namespace {
+
+// Largest divisor of x that is at most cap.
+uint32_t largest_divisor(uint32_t x, uint32_t cap)
 {
-    const uint32_t root = (uint32_t)std::sqrt((double)n);
-    for (uint32_t d = root + 1; d >= 2; --d) {
-        if (n % d) continue;
-        const uint32_t e = n / d;
-        if (d > e || e > kMaxSingleN) continue;
-        EnginePlan a, b;
-        if (plan_engine(d, &a) && plan_engine(e, &b)) {
-            *n1 = d;
-            *n2 = e;
+    for (uint32_t d = std::min(x, cap); d > 1u; --d)
+        if (x % d == 0u) return d;
+    return 1u;
+}
+
+void split_dfs(uint32_t rest, int left, uint32_t* cur, int depth, double* best, int* bestG, uint32_t* bestR)
+{
+    if (left == 0) {
+        if (rest != 1u) return;
+        // balanced first (the largest radix bounds the tile size), then runs:
+        // pass i >= 1 tiles its columns in runs of a divisor of the product
+        // of the radices before it
+        uint32_t mx = 0, ns = 1;
+        double runs = 0.0;
+        for (int i = 0; i < depth; ++i) {
+            mx = std::max(mx, cur[i]);
+            if (i > 0) runs += 16.0 / (double)largest_divisor(ns, 16u);
+            ns *= cur[i];
+        }
+        const double score = (double)mx + runs;
+        if (score < *best) {
+            *best = score;
+            *bestG = depth;
+            for (int i = 0; i < depth; ++i) bestR[i] = cur[i];
+        }
+        return;
+    }
+    for (uint32_t d = 2; d <= std::min(rest, kMaxGlobalRadix); ++d) {
+        if (rest % d) continue;  // every divisor of a 2^a 3^b 5^c length is a single-kernel length
+        cur[depth] = d;
+        split_dfs(rest / d, left - 1, cur, depth + 1, best, bestG, bestR);
+    }
+}
+
+} // namespace
+
+bool split_global(uint32_t n, int* G, uint32_t* R)
+{
+    if (!is_235(n)) return false;
+    for (int g = 2; g <= kMaxGlobal; ++g) {
+        uint32_t cur[kMaxGlobal];
+        double best = 1e300;
+        int bestG = 0;
+        split_dfs(n, g, cur, 0, &best, &bestG, R);
+        if (bestG) {
+            *G = bestG;
             return true;
         }
     }
@@ -334,25 +372,36 @@ ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err)
         ComplexPlan* p = new ComplexPlan();
         p->device = dev;
         p->n = n;
+        cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, dev);
         if (n <= kMaxSingleN && plan_engine(n, &p->eng)) {
             EnginePlan tuned;
             if (autotune_enabled() && tune_schedule(n, 4096, 0, 0, &tuned)) p->eng = tuned;
             *err = make_pass_table(&p->tw, p->eng, s);
-        } else if (split_four_step(n, &p->n1, &p->n2)) {
-            p->fourStep = true;
-            plan_engine(p->n1, &p->eng1);
-            plan_engine(p->n2, &p->eng2);
-            *err = make_table(&p->tw, n, n, s);
-            if (*err == cudaSuccess) *err = make_pass_table(&p->tw1, p->eng1, s);
-            if (*err == cudaSuccess) *err = make_pass_table(&p->tw2, p->eng2, s);
+        } else if (split_global(n, &p->G, p->R)) {
+            p->multiPass = true;
+            // W_n^p = twLo[p mod L] twHi[p / L], L the power of two at or above sqrt(n)
+            uint32_t bits = 0;
+            while ((1ull << (2 * bits)) < n) ++bits;
+            p->twLoBits = bits;
+            const uint32_t lo = 1u << bits, hi = (n + lo - 1u) / lo;
+            *err = make_table(&p->twLo, n, lo, s);
+            if (*err == cudaSuccess) {
+                *err = cudaMalloc((void**)&p->twHi, sizeof(float2) * hi);
+                if (*err == cudaSuccess) *err = launch_twiddle(p->twHi, n, hi, s, lo);
+            }
+            for (int g = 0; g < p->G && *err == cudaSuccess; ++g) {
+                plan_engine(p->R[g], &p->engG[g]);
+                *err = make_pass_table(&p->twG[g], p->engG[g], s);
+            }
         } else {
             *err = cudaErrorInvalidValue;
         }
         if (*err == cudaSuccess) *err = cudaStreamSynchronize(s);
         if (*err != cudaSuccess) {
             cudaFree(p->tw);
-            cudaFree(p->tw1);
-            cudaFree(p->tw2);
+            for (float2* t : p->twG) cudaFree(t);
+            cudaFree(p->twLo);
+            cudaFree(p->twHi);
             delete p;
             g_plans.erase({dev, n});
             return nullptr;
@@ -381,8 +430,9 @@ void release_all_plans()
         if (!p) continue;
         cudaSetDevice(p->device);
         cudaFree(p->tw);
-        cudaFree(p->tw1);
-        cudaFree(p->tw2);
+        for (float2* t : p->twG) cudaFree(t);
+        cudaFree(p->twLo);
+        cudaFree(p->twHi);
         cudaFree(p->twSplit);
         delete p;
     }
@@ -396,47 +446,96 @@ void release_all_plans()
 
 namespace {
 
-// Four-step complex transform of each length-n row of `in` (overwritten)
-// into `out`: columns of the n1 x n2 view first (W_n fused into their
-// store), then rows, whose outputs land transposed at k1 + n1 * k2.
-cudaError_t run_four_step(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse,
-                          cudaStream_t s)
-{
-    const uint32_t n = p->n, n1 = p->n1, n2 = p->n2;
-    for (uint32_t c = 0; c < batch; ++c) {
-        float2* x = in + (size_t)c * n;
-        float2* y = out + (size_t)c * n;
-        FftArgs a = engine_args(p->eng1, p->tw1);
-        a.err = error_word().dev;
-        a.in = x;
-        a.out = x;
-        a.batch = n2;
-        a.inBatch = 1;
-        a.inElem = n2;
-        a.outBatch = 1;
-        a.outElem = n2;
-        a.batchMinor = 1;
-        a.conjIn = inverse ? 1 : 0;
-        a.twBig = p->tw;
-        a.bigN = n;
-        finalize_launch(a, p->eng1, false, false);
-        cudaError_t e = launch_fft(a, p->eng1.emax, s);
-        if (e != cudaSuccess) return e;
+constexpr uint32_t kMaxSmemBytes = 227u * 1024u;
 
-        FftArgs b = engine_args(p->eng2, p->tw2);
-        b.err = error_word().dev;
-        b.in = x;
-        b.out = y;
-        b.batch = n1;
-        b.inBatch = n2;
-        b.inElem = 1;
-        b.outBatch = 1;
-        b.outElem = n1;
-        b.conjOut = inverse ? 1 : 0;
-        b.scale = inverse ? 1.0f / (float)n : 1.0f;
-        finalize_launch(b, p->eng2, false, false);
-        e = launch_fft(b, p->eng2.emax, s);
+// Staged tile of one global pass: M columns of one channel (M divides
+// perCh, and ns when ns > 1, so a tile never straddles a channel or an
+// output group), loaded and stored as runs of M adjacent values through
+// shared memory and computed Mc columns at a time within the kernel's thread
+// limit (the fixed-size kernel's when the schedule has one). M is the
+// largest such divisor up to 16 that leaves two CTAs per SM room in shared
+// memory, smaller (not below 4) where that leaves fewer than 2 tiles per SM.
+void tile_global(FftArgs& a, const EnginePlan& e, uint32_t perCh, uint32_t ns, int sms)
+{
+    a.staged = 1;
+    a.batchMinor = 0;
+    a.perCh = perCh;
+    a.slen = smem_len(e.n);
+    a.inCount = e.n;
+    a.inMagic = fastdiv_magic(e.n);
+    const uint32_t bytesPer = a.slen * (uint32_t)sizeof(float2);
+    const uint32_t mMax = std::max(1u, std::min(16u, kMaxSmemBytes / 2u / bytesPer));
+    const uint32_t want = 2u * (uint32_t)std::max(sms, 1);
+    uint32_t M = 1;
+    for (uint32_t d = mMax; d >= 1u; --d) {
+        if (perCh % d || (ns > 1u && ns % d)) continue;
+        if (M == 1u) M = d;                    // the largest valid tile
+        if (d >= 4u && a.batch / d >= want) {  // prefer one that fills the device
+            M = d;
+            break;
+        }
+        if (d < 4u) break;
+    }
+    const int st = static_max_threads(e.n, e.emax, e.T, e.P, e.R);
+    const uint32_t cap = st ? (uint32_t)st : (uint32_t)engine_max_threads(e.emax);
+    uint32_t Mc = 1;
+    for (uint32_t d = M; d >= 1u; --d) {
+        if (M % d == 0u && e.T * d <= cap) {
+            Mc = d;
+            break;
+        }
+    }
+    a.M = M;
+    a.Mc = Mc;
+    a.mMagic = fastdiv_magic(M);
+}
+
+// Complex transform of `batch` rows of length n of `in` into `out` by G
+// global Stockham passes, one launch each for the whole batch. Pass g (radix
+// R, ns = product of the radices before it) runs the R-point sub-transform
+// of every column j < n/R: inputs in[j + q n/R], q < R, times
+// W_{ns R}^{q (j mod ns)} (pass g > 0), outputs to
+// out[(j / ns) ns R + (j mod ns) + q ns]. Both sides move runs of adjacent
+// columns; the last pass (ns = n/R) writes where it reads, so it may run in
+// place. Passes alternate between out and in (in is overwritten when G > 2)
+// and the last one lands in out.
+cudaError_t run_global(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse, cudaStream_t s)
+{
+    const uint32_t n = p->n;
+    const float2* src = in;
+    uint32_t ns = 1;
+    for (int g = 0; g < p->G; ++g) {
+        const uint32_t R = p->R[g], cols = n / R;
+        float2* dst = (g % 2 == 0 || g + 1 == p->G) ? out : in;
+        FftArgs a = engine_args(p->engG[g], p->twG[g]);
+        a.err = error_word().dev;
+        a.in = src;
+        a.out = dst;
+        a.batch = batch * cols;
+        a.inChStride = a.outChStride = n;
+        a.inBatch = 1;
+        a.inElem = cols;
+        a.outBatch = 1;
+        a.outElem = ns;
+        a.outGroup = ns;
+        a.outGroupStride = (int64_t)ns * R;
+        if (g > 0) {
+            a.twLo = p->twLo;
+            a.twHi = p->twHi;
+            a.twLoBits = p->twLoBits;
+            a.twNs = ns;
+            a.twStep = n / (ns * R);
+        }
+        a.conjIn = (g == 0 && inverse) ? 1 : 0;
+        if (g + 1 == p->G) {
+            a.conjOut = inverse ? 1 : 0;
+            a.scale = inverse ? 1.0f / (float)n : 1.0f;
+        }
+        tile_global(a, p->engG[g], cols, ns, p->sms);
+        cudaError_t e = launch_fft(a, p->engG[g].emax, s);
         if (e != cudaSuccess) return e;
+        src = dst;
+        ns *= R;
     }
     return cudaSuccess;
 }
@@ -446,7 +545,7 @@ cudaError_t run_four_step(const ComplexPlan* p, float2* in, float2* out, uint32_
 cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse, cudaStream_t s)
 {
     if (batch == 0) return cudaSuccess;
-    if (p->fourStep) return run_four_step(p, in, out, batch, inverse, s);
+    if (p->multiPass) return run_global(p, in, out, batch, inverse, s);
     const uint32_t n = p->n;
     FftArgs a = engine_args(p->eng, p->tw);
     a.err = error_word().dev;
@@ -468,9 +567,9 @@ cudaError_t run_r2c(const ComplexPlan* p, float* x, float2* scratch, float2* y, 
 {
     if (batch == 0) return cudaSuccess;
     const uint32_t h = p->n;
-    if (p->fourStep) {
+    if (p->multiPass) {
         if (!scratch) return cudaErrorInvalidValue;
-        cudaError_t e = run_four_step(p, (float2*)x, scratch, batch, false, s);
+        cudaError_t e = run_global(p, (float2*)x, scratch, batch, false, s);
         if (e != cudaSuccess) return e;
         return launch_r2c_post(scratch, y, p->twSplit, h, batch, outmode, s);
     }
@@ -505,7 +604,7 @@ bool c2r_staged_fits(uint32_t h, uint32_t inCount)
 bool c2r_needs_scratch(const ComplexPlan* p, int inmode)
 {
     const uint32_t h = p->n;
-    return p->fourStep || !c2r_staged_fits(h, inmode ? 2u * h : h + 1u);
+    return p->multiPass || !c2r_staged_fits(h, inmode ? 2u * h : h + 1u);
 }
 
 cudaError_t run_c2r(const ComplexPlan* p, const float2* x, float2* scratch, float* y, uint32_t batch, int inmode,
@@ -514,18 +613,18 @@ cudaError_t run_c2r(const ComplexPlan* p, const float2* x, float2* scratch, floa
     if (batch == 0) return cudaSuccess;
     const uint32_t h = p->n;
     const uint32_t inCount = inmode ? 2u * h : h + 1u;
-    if (!p->fourStep && !c2r_staged_fits(h, inCount)) {
+    if (!p->multiPass && !c2r_staged_fits(h, inCount)) {
         // split as a pre-pass into the work buffer, then the plain inverse
         if (!scratch) return cudaErrorInvalidValue;
         cudaError_t e = launch_c2r_pre(x, scratch, p->twSplit, h, batch, inmode, s);
         if (e != cudaSuccess) return e;
         return run_c2c(p, scratch, (float2*)y, batch, true, s);
     }
-    if (p->fourStep) {
+    if (p->multiPass) {
         if (!scratch) return cudaErrorInvalidValue;
         cudaError_t e = launch_c2r_pre(x, scratch, p->twSplit, h, batch, inmode, s);
         if (e != cudaSuccess) return e;
-        return run_four_step(p, scratch, (float2*)y, batch, true, s);
+        return run_global(p, scratch, (float2*)y, batch, true, s);
     }
     FftArgs a = engine_args(p->eng, p->tw);
     a.err = error_word().dev;

@@ -2,10 +2,11 @@
 // FFT kernels (internal to libfftlib_b200.so).
 //
 // A ComplexPlan describes one complex transform length n on one device:
-// either a single-kernel Stockham schedule (n <= kMaxSingleN) or a four-step
-// split n = n1 * n2 (column FFTs with the W_n twiddle fused into their store,
-// then row FFTs writing the transposed result). Its twiddle tables are
-// generated once on the device in FP64 and stay resident in HBM.
+// either a single-kernel Stockham schedule (n <= kMaxSingleN) or G global
+// Stockham passes (one kernel each, every kernel a batch of R-point
+// sub-transforms over strided columns with the pass twiddle fused into its
+// loads). Its twiddle tables are generated once on the device in FP64 and
+// stay resident in HBM.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -51,20 +52,27 @@ bool tune_schedule(uint32_t n, uint32_t batch, int emaxOnly, uint32_t maxT, Engi
 // True when $FFTLIB_B200_AUTOTUNE is set to a non-zero value.
 bool autotune_enabled();
 std::string describe(const EnginePlan& e);
-// Four-step split n = n1 * n2 (n1 <= n2, both single-kernel lengths).
-bool split_four_step(uint32_t n, uint32_t* n1, uint32_t* n2);
+// Global Stockham passes for n > kMaxSingleN: n = R[0] R[1] ... R[G-1],
+// each R <= kMaxGlobalRadix a single-kernel length, balanced and ordered so
+// that every pass after the first can tile its columns in runs of 8 or more.
+constexpr int kMaxGlobal = 4;
+constexpr uint32_t kMaxGlobalRadix = 1024;
+bool split_global(uint32_t n, int* G, uint32_t* R);
 
 struct ComplexPlan {
     int device = 0;
+    int sms = 0;                     // multiprocessors of the device
     uint32_t n = 0;
-    bool fourStep = false;
     EnginePlan eng;                  // single kernel
-    uint32_t n1 = 0, n2 = 0;         // four-step
-    EnginePlan eng1, eng2;
-    float2* tw = nullptr;            // single kernel: per-pass twiddle blocks;
-                                     // four-step: W_n, n entries (column step)
-    float2* tw1 = nullptr;           // per-pass blocks of the n1 schedule
-    float2* tw2 = nullptr;           // per-pass blocks of the n2 schedule
+    float2* tw = nullptr;            //   its per-pass twiddle blocks
+    bool multiPass = false;          // global Stockham passes
+    int G = 0;
+    uint32_t R[kMaxGlobal] = {};     //   their radices (sub-transform lengths)
+    EnginePlan engG[kMaxGlobal];     //   the sub-transform schedules
+    float2* twG[kMaxGlobal] = {};    //   and their per-pass blocks
+    float2* twLo = nullptr;          //   W_n^r, r < 2^twLoBits
+    float2* twHi = nullptr;          //   W_n^(2^twLoBits q), q < n / 2^twLoBits
+    uint32_t twLoBits = 0;
     float2* twSplit = nullptr;       // W_{2n}^i, i < n (real-input kernels)
 };
 
@@ -88,11 +96,11 @@ void finalize_launch(FftArgs& a, const EnginePlan& e, bool contiguousIn, bool co
 FftArgs engine_args(const EnginePlan& e, const float2* tw);
 
 // Launch sequences (device pointers, stream s, no synchronization).
-// run_c2c may overwrite `in` (four-step work buffer).
+// run_c2c may overwrite `in` (work buffer of the passes when G > 2).
 cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse,
                     cudaStream_t s);
 // h = p->n = numPoints / 2; x: batch x 2h reals; scratch: batch x h complex
-// (needed only for the four-step path); y: batch x (h+1) or x 2h bins.
+// (needed only for global passes); y: batch x (h+1) or x 2h bins.
 cudaError_t run_r2c(const ComplexPlan* p, float* x, float2* scratch, float2* y, uint32_t batch, int outmode,
                     cudaStream_t s);
 // x: batch x (h+1) or x 2h bins; y: batch x 2h reals. scratch (batch x h

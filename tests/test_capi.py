@@ -256,7 +256,7 @@ def test_planner_covers_every_235_length_up_to_16384():
         desc = F.describe_plan(n)
         m = re.match(r"N=(\d+) E=(\d+) T=(\d+) radices=([\dx]+)", desc)
         if m is None:
-            assert desc.startswith("four-step"), (n, desc)
+            assert desc.startswith("global passes"), (n, desc)
             continue
         radices = [int(r) for r in m.group(4).split("x")]
         assert int(np.prod(radices)) == n, (n, desc)

@@ -79,7 +79,7 @@ def test_c2c_vs_reference_cn(gpu, ref_cn):
 
 
 def test_round_trip_large(gpu):
-    """ifft1d(fft1d(x)) == x at 2^22 points (the four-step path), a
+    """ifft1d(fft1d(x)) == x at 2^22 points (three global passes), a
     size-independent check beyond the oracle's reach."""
     n = 1 << 22
     x = O.uniform_c2c(n, 1, seed=99)
