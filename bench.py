@@ -432,7 +432,71 @@ def secondary_configs(args):
                           "transforms_per_s": round(20000 / ms_graph * 1e3, 1)}
     mb.close()
     res["tc_dft"] = tc_dft_configs(args, steps)
+    res["fft1d_single"] = fft1d_single_configs(steps)
     return res
+
+
+def fft1d_single_configs(steps):
+    """Single-transform c2c (FFTLIB_fft1d_i32fc_c32fc_o32fc): the largest
+    single-kernel length, the reference test list's largest length and two
+    long lengths run as global passes. device_ms: the kernels alone (batched
+    async entry with one channel, device buffers, CUDA events); e2e_ms: the
+    synchronous FFTLIB_fft1d_i32fc_c32fc_o32fc_kernel on pinned host buffers
+    (copies in and out included), wall clock per call; ref_cn_ms: the
+    reference's natural-C single-transform kernel on one host core."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import c7x_fftlib_b200 as F
+    import oracle as O
+
+    stream = torch.cuda.Stream()
+    sp = F.ptr(stream.cuda_stream)
+    out = {}
+    base = F.KERNELS["1d_c2c"]
+    for n in (16384, 78125, 1 << 20, 1 << 24):
+        x = torch.rand(2 * n, device="cuda") * 2 - 1
+        y = torch.empty_like(x)
+        pb = F.pblock("c2c")
+        bb = F.bp(F.FFTLIB_FLOAT32, 2 * n)
+        F.check(F.fn(F.KERNELS["c2c"] + "_init")(F.ptr(x), bb, F.ptr(x), bb, F.ptr(y), bb, n, 1, pb))
+        k = F.fn("FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync")
+        ms = _time_launches(torch, stream, lambda: k(F.ptr(x), F.ptr(y), n, 1, pb, sp), max(steps, 20))
+        xh = torch.empty(2 * n, dtype=torch.float32, pin_memory=True)
+        yh = torch.empty(2 * n, dtype=torch.float32, pin_memory=True)
+        x0 = (torch.rand(2 * n) * 2 - 1)
+        pb1 = F.pblock("1d_c2c")
+        F.check(F.fn(base + "_init")(F.ptr(xh), bb, F.ptr(xh), bb, F.ptr(yh), bb, pb1))
+        reps = 20 if n <= (1 << 20) else 5
+        t_e2e = []
+        for _ in range(reps + 2):
+            xh.copy_(x0)  # the kernel may use pX as work buffer
+            t0 = time.perf_counter()
+            F.check(F.fn(base + "_kernel")(F.ptr(xh), bb, F.ptr(xh), bb, F.ptr(yh), bb, pb1))
+            t_e2e.append(time.perf_counter() - t0)
+        e2e_ms = float(np.median(t_e2e[2:])) * 1e3
+        got = yh.numpy().astype(np.float64)
+        want = np.fft.fft(x0.numpy().astype(np.float64).view(np.complex128))
+        rel = float(np.linalg.norm(got.view(np.complex128) - want) / np.linalg.norm(want))
+        entry = {"plan": F.describe_plan(n), "device_ms": round(ms, 5),
+                 "device_GBps": round(16.0 * n / ms / 1e6, 1), "e2e_ms": round(e2e_ms, 4),
+                 "h2d_d2h_bytes": 16 * n, "rel_l2_vs_fp64": rel}
+        if n <= 78125 and O.ref1d_available():
+            xr = x0.numpy()
+            w = O.ref_tw_gen_c2c(n)
+            t_ref = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                O.ref_fft1d_c2c_f32(xr, n, False, w)
+                t_ref.append(time.perf_counter() - t0)
+            entry["ref_cn_ms"] = round(float(np.median(t_ref)) * 1e3, 3)
+            entry["ref_cn_cores"] = 1
+            entry["e2e_speedup_vs_ref_cn"] = round(entry["ref_cn_ms"] / e2e_ms, 2)
+        out[str(n)] = entry
+        del x, y, xh, yh
+    return out
 
 
 def tc_flops(n: int) -> float:
