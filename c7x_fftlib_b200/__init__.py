@@ -27,6 +27,7 @@ FFTLIB_ERR_INVALID_DIMENSION = 4
 FFTLIB_ERR_NULL_POINTER = 5
 FFTLIB_ERR_NOT_IMPLEMENTED = 6
 FFTLIB_ERR_NOT_ALIGNED_PTRS_STRIDES = 8
+FFTLIB_ERR_INVALID_SHIFT = 12
 FFTLIB_ERR_INVALID_OUTMODE = 14
 
 # FFTLIB_data_type_e (src/common/FFTLIB_bufParams.h:22-42)
@@ -275,30 +276,36 @@ def fn(name: str):
 
 
 class DftMma:
-    """FFTLIB_FFT_fft_ixX_cxX_oxX_*: the DFT coordinator for FLOAT32
-    interleaved complex data (getSizes, twGen, init_checkParams, init, then
-    exec or the stream-ordered execAsync)."""
+    """FFTLIB_FFT_fft_ixX_cxX_oxX_*: the DFT coordinator (getSizes, twGen,
+    init_checkParams, init, then exec or the stream-ordered execAsync) for
+    FLOAT32 interleaved data or the reference's INT16 / INT32 data
+    (dtype, interleave and the five-entry shift vector as in its InitArgs)."""
 
-    def __init__(self, n: int, batch: int, func_style: int = FFTLIB_FUNCTION_OPTIMIZED, w_device=True):
+    def __init__(self, n: int, batch: int, func_style: int = FFTLIB_FUNCTION_OPTIMIZED, w_device=True,
+                 dtype: int = FFTLIB_FLOAT32, interleave: int = 1, shifts=None):
         import numpy as _np
 
         L = lib()
         M = "FFTLIB_FFT_fft_ixX_cxX_oxX_"
-        self.n, self.batch = n, batch
-        self.args = MmaInitArgs(func_style, n, batch, 1)
-        self.bx, self.bw, self.by = (BufParams(FFTLIB_FLOAT32, 0) for _ in range(3))
+        self.n, self.batch, self.dtype = n, batch, dtype
+        self.args = MmaInitArgs(func_style, n, batch, interleave)
+        for i, v in enumerate([] if shifts is None else list(shifts)):
+            self.args.shiftVector[i] = int(v)
+        self.bx, self.bw, self.by = (BufParams(dtype, 0) for _ in range(3))
         check(getattr(L, M + "getSizes")(C.byref(self.args), self.bx, self.bw, self.by), "getSizes")
         self.handle = C.create_string_buffer(getattr(L, M + "getHandleSize")(C.byref(self.args)))
         check(getattr(L, M + "init_checkParams")(self.handle, self.bx, self.bw, self.by, C.byref(self.args)),
               "init_checkParams")
         check(getattr(L, M + "init")(self.handle, self.bx, self.bw, self.by, C.byref(self.args)), "init")
-        self.w_host = _np.zeros(self.bw.dim_x, _np.float32)
+        np_dt = {FFTLIB_FLOAT32: _np.float32, FFTLIB_INT16: _np.int16, FFTLIB_INT32: _np.int32}[dtype]
+        self.w_host = _np.zeros(self.bw.dim_x, np_dt)
         check(getattr(L, M + "twGen")(C.byref(self.args), ptr(self.w_host), self.bw), "twGen")
         self.w = None
         if w_device:
             import torch
 
-            self.w = torch.empty(self.bw.dim_x, dtype=torch.float32, device="cuda")
+            t_dt = {FFTLIB_FLOAT32: torch.float32, FFTLIB_INT16: torch.int16, FFTLIB_INT32: torch.int32}[dtype]
+            self.w = torch.empty(self.bw.dim_x, dtype=t_dt, device="cuda")
             check(getattr(L, M + "twGen")(C.byref(self.args), ptr(self.w), self.bw), "twGen (device)")
 
     @property

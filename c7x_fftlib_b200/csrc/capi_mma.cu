@@ -1,10 +1,11 @@
 // capi_mma.cu -- FFTLIB_FFT_fft_ixX_cxX_oxX_*: the DFT coordinator of the
 // reference's src/fft_c7xmma/FFTLIB_FFT_fft_ixX_cxX_oxX/
-// FFTLIB_FFT_fft_ixX_cxX_oxX.cpp:7-282, for FLOAT32 data.
+// FFTLIB_FFT_fft_ixX_cxX_oxX.cpp:7-282.
 //
-// The reference picks dftSmall / dftLarge / highRadixDecompositions from
-// fftSize and batchSize (FFTLIB_FFT_fft_ixX_cxX_oxX.cpp:13-50) for its MMA
-// widths. Here init picks between two GPU paths:
+// INT16 / INT32 (the reference's types): the reference's own variant choice
+// (dftSmall / dftLarge / highRadixDecompositions, ..._oxX.cpp:13-50), tables
+// and arithmetic, bit-exact with its natural C (dft_int.cu).
+// FLOAT32 (added): init picks between two GPU paths:
 //   PATH_TC  -- funcStyle OPTIMIZED and fftSize a power of two in [8, 4096]:
 //               the split-precision tensor-core DFT (one DFT-GEMM up to 64,
 //               two DFT-GEMM stages with the twiddle fused between above);
@@ -13,6 +14,7 @@
 #include <string.h>
 
 #include "capi_common.h"
+#include "dft_int.h"
 #include "fft_c7xmma.h"
 #include "fftlib_b200_ext.h"
 #include "plan.h"
@@ -23,16 +25,32 @@ using namespace fftb200;
 namespace {
 
 constexpr uint32_t kMmaMagic = 0x32414D4Du;  // "MMA2"
-enum MmaPath : int32_t { PATH_NONE = 0, PATH_TC = 1, PATH_FFT = 2 };
+enum MmaPath : int32_t { PATH_NONE = 0, PATH_TC = 1, PATH_FFT = 2, PATH_INT = 3 };
 
 struct MmaHandle {
     uint32_t magic;
     int32_t path;
     int32_t device;
-    uint32_t reserved;
+    int32_t bits;       // PATH_INT: 16 or 32
     FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs init;
-    ComplexPlan* plan;  // CUDA-core FFT plan of fftSize
+    ComplexPlan* plan;  // CUDA-core FFT plan of fftSize (FLOAT32)
 };
+
+int int_bits(uint32_t type) { return type == FFTLIB_INT16 ? 16 : (type == FFTLIB_INT32 ? 32 : 0); }
+
+// INT16 / INT32 buffer sizes in elements (the reference's getSizes).
+FFTLIB_STATUS sizes_int(const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* a, int bits, uint32_t* x, uint32_t* w,
+                        uint32_t* y)
+{
+    const uint64_t xy = 2ull * a->fftSize * a->batchSize;
+    if (xy > 0xFFFFFFFFull) {
+        set_error("fftSize x batchSize x 2 = %llu exceeds the 32-bit dim_x", (unsigned long long)xy);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    *x = *y = (uint32_t)xy;
+    *w = int_dft_w_size(bits, a->fftSize, a->batchSize, a->interleave);
+    return FFTLIB_SUCCESS;
+}
 
 int32_t choose_path(const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* a)
 {
@@ -64,9 +82,10 @@ FFTLIB_STATUS sizes_f32(const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* a, uint32_t* 
     return FFTLIB_SUCCESS;
 }
 
-FFTLIB_STATUS not_float(uint32_t type)
+FFTLIB_STATUS unsupported_type(uint32_t type)
 {
-    set_error("data type %u: this library implements the coordinator for FLOAT32 (%d) only", type, FFTLIB_FLOAT32);
+    set_error("data type %u: the coordinator implements INT16 (%d), INT32 (%d) and FLOAT32 (%d)", type,
+              FFTLIB_INT16, FFTLIB_INT32, FFTLIB_FLOAT32);
     return FFTLIB_ERR_NOT_IMPLEMENTED;
 }
 
@@ -82,6 +101,9 @@ MmaHandle* handle_of(FFTLIB_kernelHandle h)
 
 cudaError_t enqueue(const MmaHandle* m, const float* x, const float* w, float* y, uint32_t batch, cudaStream_t s)
 {
+    if (m->path == PATH_INT)
+        return int_dft_launch(m->bits, m->init.fftSize, batch, m->init.interleave, m->init.shiftVector,
+                              const_cast<float*>(x), w, y, s);
     // the tensor-core kernels read and prefetch whole 16-byte lines; buffers
     // that are only 8-byte aligned take the FFT
     const bool aligned = (((uintptr_t)x | (uintptr_t)y) & 15u) == 0;
@@ -109,9 +131,10 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_getSizes(const FFTLIB_FFT_fft_ixX_cxX_o
                                                   FFTLIB_bufParams1D_t* bufParamsY)
 {
     if (!pKerInitArgs || !bufParamsX || !bufParamsW || !bufParamsY) return FFTLIB_ERR_NULL_POINTER;
-    if (bufParamsX->data_type != FFTLIB_FLOAT32) return not_float(bufParamsX->data_type);
+    const int bits = int_bits(bufParamsX->data_type);
+    if (!bits && bufParamsX->data_type != FFTLIB_FLOAT32) return unsupported_type(bufParamsX->data_type);
     uint32_t x, w, y;
-    const FFTLIB_STATUS st = sizes_f32(pKerInitArgs, &x, &w, &y);
+    const FFTLIB_STATUS st = bits ? sizes_int(pKerInitArgs, bits, &x, &w, &y) : sizes_f32(pKerInitArgs, &x, &w, &y);
     if (st != FFTLIB_SUCCESS) return st;
     bufParamsX->dim_x = x;
     bufParamsW->dim_x = w;
@@ -123,7 +146,25 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_twGen(const FFTLIB_FFT_fft_ixX_cxX_oxX_
                                                const FFTLIB_bufParams1D_t* bufParamsW)
 {
     if (!pKerInitArgs || !pW || !bufParamsW) return FFTLIB_ERR_NULL_POINTER;
-    if (bufParamsW->data_type != FFTLIB_FLOAT32) return not_float(bufParamsW->data_type);
+    const int bits = int_bits(bufParamsW->data_type);
+    if (bits) {
+        const uint32_t n = pKerInitArgs->fftSize, b = pKerInitArgs->batchSize, il = pKerInitArgs->interleave;
+        const uint32_t w = int_dft_w_size(bits, n, b, il);
+        if (bufParamsW->dim_x != w) {
+            set_error("bufParamsW->dim_x %u, expected %u", bufParamsW->dim_x, w);
+            return FFTLIB_ERR_INVALID_DIMENSION;
+        }
+        const size_t bytes = (size_t)w * (bits / 8);
+        if (!is_device_ptr(pW)) {
+            int_dft_twgen_host(bits, n, b, il, pW);
+            return FFTLIB_SUCCESS;
+        }
+        std::vector<unsigned char> tmp(bytes);
+        int_dft_twgen_host(bits, n, b, il, tmp.data());
+        const cudaError_t e = cudaMemcpy(pW, tmp.data(), bytes, cudaMemcpyHostToDevice);
+        return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen copy");
+    }
+    if (bufParamsW->data_type != FFTLIB_FLOAT32) return unsupported_type(bufParamsW->data_type);
     uint32_t x, w, y;
     FFTLIB_STATUS st = sizes_f32(pKerInitArgs, &x, &w, &y);
     if (st != FFTLIB_SUCCESS) return st;
@@ -161,10 +202,18 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_init_checkParams(FFTLIB_kernelHandle ha
                                                           const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs* pKerInitArgs)
 {
     if (!handle || !bufParamsX || !bufParamsW || !bufParamsY || !pKerInitArgs) return FFTLIB_ERR_NULL_POINTER;
-    if (bufParamsX->data_type != FFTLIB_FLOAT32) return not_float(bufParamsX->data_type);
+    const int bits = int_bits(bufParamsX->data_type);
+    if (!bits && bufParamsX->data_type != FFTLIB_FLOAT32) return unsupported_type(bufParamsX->data_type);
     uint32_t x, w, y;
-    const FFTLIB_STATUS st = sizes_f32(pKerInitArgs, &x, &w, &y);
+    const FFTLIB_STATUS st = bits ? sizes_int(pKerInitArgs, bits, &x, &w, &y) : sizes_f32(pKerInitArgs, &x, &w, &y);
     if (st != FFTLIB_SUCCESS) return st;
+    const int variant = bits ? int_dft_variant(bits, pKerInitArgs->fftSize, pKerInitArgs->batchSize,
+                                               pKerInitArgs->interleave)
+                             : 0;
+    // highRadix: at least 2 MMA points
+    // (FFTLIB_FFT_highRadixDecompositions_ixX_cxX_oxX.cpp:41-43)
+    if (variant == INT_HIGH_RADIX && pKerInitArgs->fftSize < 2u * (uint32_t)int_mma_size(bits))
+        return FFTLIB_ERR_INVALID_VALUE;
     if (bufParamsX->dim_x != x || bufParamsY->dim_x != y || bufParamsW->dim_x != w) {
         set_error("dim_x X/W/Y = %u/%u/%u, expected %u/%u/%u", bufParamsX->dim_x, bufParamsW->dim_x,
                   bufParamsY->dim_x, x, w, y);
@@ -172,6 +221,10 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_init_checkParams(FFTLIB_kernelHandle ha
     }
     if (bufParamsW->data_type != bufParamsX->data_type || bufParamsY->data_type != bufParamsX->data_type)
         return FFTLIB_ERR_INVALID_TYPE;
+    // dftLarge runs the LINALG matrix multiply, whose check bounds the shift
+    // by the accumulator width (FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX.cpp:41-56)
+    if (variant == INT_DFT_LARGE && (int8_t)pKerInitArgs->shiftVector[0] > (bits == 16 ? 64 : 128))
+        return FFTLIB_ERR_INVALID_SHIFT;
     return FFTLIB_SUCCESS;
 }
 
@@ -184,7 +237,27 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_init(FFTLIB_kernelHandle handle, FFTLIB
     (void)bufParamsY;
     MmaHandle* m = static_cast<MmaHandle*>(handle);
     memset(m, 0, sizeof(*m));
-    if (bufParamsX->data_type != FFTLIB_FLOAT32) return not_float(bufParamsX->data_type);
+    const int bits = int_bits(bufParamsX->data_type);
+    if (bits) {
+        const uint32_t n = pKerInitArgs->fftSize;
+        if (n == 0 || pKerInitArgs->batchSize == 0) return FFTLIB_ERR_INVALID_DIMENSION;
+        if (int_dft_variant(bits, n, pKerInitArgs->batchSize, pKerInitArgs->interleave) == INT_HIGH_RADIX &&
+            !int_high_radix_covered(bits, n)) {
+            set_error("INT%d fftSize %u: the high-radix decomposition needs d0 x %u^L points, d0 <= %u, L <= 4",
+                      bits, n, int_mma_size(bits) / 2, int_mma_size(bits) / 2);
+            return FFTLIB_ERR_NOT_IMPLEMENTED;
+        }
+        int dev = 0;
+        const cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+        m->init = *pKerInitArgs;
+        m->device = dev;
+        m->bits = bits;
+        m->path = PATH_INT;
+        m->magic = kMmaMagic;
+        return FFTLIB_SUCCESS;
+    }
+    if (bufParamsX->data_type != FFTLIB_FLOAT32) return unsupported_type(bufParamsX->data_type);
     uint32_t x, w, y;
     const FFTLIB_STATUS st = sizes_f32(pKerInitArgs, &x, &w, &y);
     if (st != FFTLIB_SUCCESS) return st;
@@ -218,11 +291,20 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_exec(FFTLIB_kernelHandle handle, void* 
     DeviceScope scope(m->device);
     const uint32_t n = m->init.fftSize;
     const void* w = pW;
-    if (m->path == PATH_TC) {
-        cudaError_t e = device_table(pW, tc_dft_w_floats(n) * sizeof(float), 2, &w);
+    const size_t elem = m->path == PATH_INT ? (size_t)m->bits / 8u : sizeof(float);
+    if (m->path == PATH_TC || m->path == PATH_INT) {
+        const size_t wbytes = m->path == PATH_TC
+                                  ? tc_dft_w_floats(n) * sizeof(float)
+                                  : (size_t)int_dft_w_size(m->bits, n, m->init.batchSize, m->init.interleave) * elem;
+        cudaError_t e = device_table(pW, wbytes, 2, &w);
         if (e != cudaSuccess) return cuda_fail(e, "computational matrix copy");
     }
-    const size_t bytes = (size_t)n * 2u * sizeof(float);
+    if (m->path == PATH_INT && pX == pY &&
+        int_dft_variant(m->bits, n, m->init.batchSize, m->init.interleave) == INT_HIGH_RADIX) {
+        set_error("the high-radix path works in pX and needs pY != pX");
+        return FFTLIB_ERR_INVALID_VALUE;
+    }
+    const size_t bytes = (size_t)n * 2u * elem;
     std::vector<ChannelBuf> bufs = {{pX, bytes, true, false}, {pY, bytes, false, true}};
     cudaError_t e = run_channels(bufs, m->init.batchSize,
                                  [&](const std::vector<void*>& d, uint32_t, uint32_t cnt, cudaStream_t s) {
@@ -239,6 +321,11 @@ FFTLIB_STATUS FFTLIB_b200_FFT_fft_execAsync(FFTLIB_kernelHandle handle, void* pX
     if (!pX || !pW || !pY) return FFTLIB_ERR_NULL_POINTER;
     if (!is_device_ptr(pX) || !is_device_ptr(pY) || !is_device_ptr(pW)) {
         set_error("execAsync needs device buffers");
+        return FFTLIB_ERR_INVALID_VALUE;
+    }
+    if (m->path == PATH_INT && pX == pY &&
+        int_dft_variant(m->bits, m->init.fftSize, m->init.batchSize, m->init.interleave) == INT_HIGH_RADIX) {
+        set_error("the high-radix path works in pX and needs pY != pX");
         return FFTLIB_ERR_INVALID_VALUE;
     }
     DeviceScope scope(m->device);

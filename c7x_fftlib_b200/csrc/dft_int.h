@@ -1,0 +1,45 @@
+// dft_int.h -- integer (INT16 / INT32) paths of the DFT coordinator
+// FFTLIB_FFT_fft_ixX_cxX_oxX (internal to libfftlib_b200.so).
+//
+// Bit-exact with the reference's natural-C arithmetic:
+//   dftSmall  (fftSize <= MMA/2)  Y = round_shift(X W), W the block-diagonal
+//             real embedding with row stride MMA
+//             (src/fft_c7xmma/FFTLIB_FFT_dftSmall_ixX_cxX_oxX/..._cn.cpp:18-46);
+//   dftLarge  (fftSize == MMA, or 2 MMA with a large batch) the same product
+//             with the dense 2N x 2N embedding, through the LINALG matrix
+//             multiply (src/linalg_c7xmma/FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX/..._cn.cpp:27-62);
+//   highRadix (larger) decimation stages of radix d0 then MMA/2, each an
+//             exact complex DFT rounded by its shift, times a twiddle
+//             rounded by bits - 1, then MMA/2-point DFTs stored in digit-
+//             reversed order (..._highRadixDecompositions_ixX_cxX_oxX_cn.cpp:20-455).
+// MMA = 32 for INT16 and 16 for INT32, the C7120 widths. Products and sums
+// are exact (64-bit for INT16, 128-bit for INT32); results are saturated as
+// the reference does, including its 128-bit saturation of non-negative
+// values (FFTLIB_utility.h:546-566, only the low 64 bits are tested).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fftb200 {
+
+enum IntVariant : int32_t { INT_DFT_SMALL = 1, INT_DFT_LARGE = 2, INT_HIGH_RADIX = 3 };
+
+int int_mma_size(int bits);
+// The reference's variant choice (FFTLIB_FFT_fft_ixX_cxX_oxX.cpp:13-50).
+int int_dft_variant(int bits, uint32_t n, uint32_t batch, uint32_t interleave);
+// Caller-table elements, as the reference's getSizes reports them.
+uint32_t int_dft_w_size(int bits, uint32_t n, uint32_t batch, uint32_t interleave);
+// highRadix lengths this path computes: n = d0 R^L with d0 <= R = MMA/2 the
+// first-stage factor and at most four decimation stages (the reference's
+// loop structure has no fifth).
+bool int_high_radix_covered(int bits, uint32_t n);
+// The caller's table (twGen) into host memory of the data type.
+void int_dft_twgen_host(int bits, uint32_t n, uint32_t batch, uint32_t interleave, void* w);
+
+// Enqueues the transform of `batch` rows on device buffers. highRadix works
+// in place on x (overwritten, as in the reference) and needs x != y.
+cudaError_t int_dft_launch(int bits, uint32_t n, uint32_t batch, uint32_t interleave, const uint32_t* shifts,
+                           void* x, const void* w, void* y, cudaStream_t s);
+
+} // namespace fftb200

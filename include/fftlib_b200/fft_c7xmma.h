@@ -4,12 +4,28 @@
  * FFTLIB_FFT_fft_ixX_cxX_oxX.h:37-234 (same names, InitArgs layout, call
  * order and status codes).
  *
- * Data types. The reference implements INT16 and INT32 only and answers
+ * Data types. The reference implements INT16 and INT32 and answers
  * FFTLIB_ERR_NOT_IMPLEMENTED for anything else. This library implements
- * FLOAT32 (interleaved complex) on the GPU and answers
- * FFTLIB_ERR_NOT_IMPLEMENTED for INT16, INT32 and non-interleaved data.
+ * INT16 and INT32 exactly as the reference does, and adds FLOAT32
+ * (interleaved complex); other types answer FFTLIB_ERR_NOT_IMPLEMENTED.
  *
- * Paths (chosen by init, from InitArgs):
+ * INT16 / INT32 (interleaved or planar, both as in the reference): the
+ * reference's variant choice for its C7120 MMA widths (32 for INT16, 16 for
+ * INT32; FFTLIB_FFT_fft_ixX_cxX_oxX.cpp:13-50), its getSizes and twGen
+ * tables, and its natural-C arithmetic bit for bit, on the GPU:
+ *   fftSize <= MMA/2          dftSmall: Y = round_shift(X W, shiftVector[0])
+ *   fftSize == MMA (or 2 MMA  dftLarge: the same product through the dense
+ *     with a large batch)     2N x 2N embedding
+ *   larger                    highRadixDecompositions: decimation stages
+ *                             (shiftVector[0..3]) and a final MMA/2-point
+ *                             DFT stage (shiftVector[4]).
+ * highRadix covers fftSize = d0 (MMA/2)^L with d0 <= MMA/2 and L <= 4 (the
+ * reference's stage structure; init answers FFTLIB_ERR_NOT_IMPLEMENTED for
+ * other lengths, where the reference's loops do not compute a DFT). As in
+ * the reference, highRadix uses pX as its work buffer (pX is overwritten and
+ * must differ from pY).
+ *
+ * FLOAT32 paths (chosen by init, from InitArgs):
  *   funcStyle OPTIMIZED, fftSize a power of two in [8, 4096]:
  *     split-precision tensor-core DFT. fftSize <= 64 is one DFT-GEMM (the
  *     reference's dftSmall / dftLarge variants); larger sizes are two
@@ -102,7 +118,8 @@ FFTLIB_STATUS FFTLIB_b200_FFT_fft_execAsync(FFTLIB_kernelHandle handle, void *pX
 /* Synchronizes `stream` and reports a device-side failure of earlier
  * execAsync calls (FFTLIB_ERR_FAILURE, text in FFTLIB_b200_lastError). */
 FFTLIB_STATUS FFTLIB_b200_FFT_fft_sync(void *stream);
-/* Which path init chose: 1 = tensor-core DFT, 2 = CUDA-core FFT, 0 = none. */
+/* Which path init chose: 1 = tensor-core DFT, 2 = CUDA-core FFT (FLOAT32),
+ * 3 = the integer path (INT16 / INT32), 0 = none. */
 int32_t FFTLIB_b200_FFT_fft_path(FFTLIB_kernelHandle handle);
 
 #if defined(__GNUC__)

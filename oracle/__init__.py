@@ -429,6 +429,86 @@ def ref_fft1d_c2c_i16(x, n, shifts, w=None):
 
 
 # --------------------------------------------------------------------------
+# Integer DFT coordinator (FFTLIB_FFT_fft_ixX_cxX_oxX, INT16 / INT32):
+# oracle/mma_int_oracle.c, values carried in int32 arrays
+# --------------------------------------------------------------------------
+
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+def _mma_lib():
+    L = lib()
+    if not getattr(L, "_mma_bound", False):
+        L.orc_mma_variant.argtypes = [C.c_int, _u32, _u32, _u32]
+        L.orc_mma_w_size.argtypes = [C.c_int, _u32, _u32, _u32]
+        L.orc_mma_w_size.restype = _u32
+        L.orc_mma_twgen.argtypes = [C.c_int, _u32, _u32, _u32, _i32p]
+        L.orc_mma_exec.argtypes = [C.c_int, _u32, _u32, _u32, _u32p, _i32p, _i32p, _i32p]
+        L.orc_mma_w1.argtypes = [C.c_int, _u32, _i32p]
+        L._mma_bound = True
+    return L
+
+
+def mma_variant(bits: int, n: int, batch: int, interleave: int) -> int:
+    """1 dftSmall, 2 dftLarge, 3 highRadixDecompositions."""
+    return _mma_lib().orc_mma_variant(bits, n, batch, interleave)
+
+
+def mma_twgen(bits: int, n: int, batch: int, interleave: int) -> np.ndarray:
+    L = _mma_lib()
+    w = np.zeros(L.orc_mma_w_size(bits, n, batch, interleave), np.int32)
+    L.orc_mma_twgen(bits, n, batch, interleave, w)
+    return w.astype(np.int16 if bits == 16 else np.int32)
+
+
+def mma_w1(bits: int, n: int) -> np.ndarray:
+    """The highRadix internal table (MMA x MMA entries)."""
+    L = _mma_lib()
+    mma = 32 if bits == 16 else 16
+    w = np.zeros(mma * mma, np.int32)
+    L.orc_mma_w1(bits, n, w)
+    return w.astype(np.int16 if bits == 16 else np.int32)
+
+
+def ref_mma_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libref_mma.so"))
+
+
+def ref_mma_exec(bits: int, n: int, batch: int, interleave: int, shifts, x, w=None) -> np.ndarray:
+    """The reference's natural-C integer DFT (dftSmall / LINALG / highRadix
+    _cn) through oracle/mma_ref_driver.cpp, with this oracle's tables."""
+    dt = np.int16 if bits == 16 else np.int32
+    if w is None:
+        w = mma_twgen(bits, n, batch, interleave)
+    sh = np.zeros(5, np.uint32)
+    sh[: len(shifts)] = shifts
+    v = mma_variant(bits, n, batch, interleave)
+    xin = np.ascontiguousarray(x, dt).copy()
+    y = np.zeros(2 * n * batch, dt)
+    w1 = mma_w1(bits, n)
+    L = ref_lib("mma")
+    rc = L.ref_mma_exec(C.c_int(bits), C.c_int(v), _u32(n), _u32(batch), _u32(interleave), _vp(sh),
+                        _vp(np.ascontiguousarray(w, dt)), _vp(w1), _vp(xin), _vp(y))
+    if rc:
+        raise ValueError(f"reference integer DFT returned {rc}")
+    return y
+
+
+def mma_exec(bits: int, n: int, batch: int, interleave: int, shifts, x, w=None) -> np.ndarray:
+    L = _mma_lib()
+    if w is None:
+        w = mma_twgen(bits, n, batch, interleave)
+    sh = np.zeros(5, np.uint32)
+    sh[: len(shifts)] = shifts
+    y = np.zeros(2 * n * batch, np.int32)
+    rc = L.orc_mma_exec(bits, n, batch, interleave, sh, np.ascontiguousarray(w, np.int32),
+                        np.ascontiguousarray(x, np.int32), y)
+    if rc:
+        raise ValueError(f"oracle integer DFT does not cover N={n}")
+    return y.astype(np.int16 if bits == 16 else np.int32)
+
+
+# --------------------------------------------------------------------------
 # Seeded synthetic inputs (splitmix64-free: numpy PCG64 with a fixed seed)
 # --------------------------------------------------------------------------
 

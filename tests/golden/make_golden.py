@@ -35,6 +35,11 @@ fixtures themselves):
 * ``fft1d_c2c_pymodel.npz`` -- outputs of the reference's Python generators
   of the single-transform c2c and ifft c2c on seeded inputs.
 
+* ``mma_int_static.npz`` -- the DFT coordinator's committed static INT16 /
+  INT32 cases (test/fft_c7xmma/FFTLIB_FFT_fft_ixX_cxX_oxX/
+  FFTLIB_FFT_fft_ixX_cxX_oxX_idat.c): input, output, shift vector and
+  (bits, batchSize, fftSize, interleave) per case.
+
 ``--only NAME[,NAME]`` regenerates just the named fixtures (file stems).
 """
 from __future__ import annotations
@@ -286,6 +291,30 @@ def fft1d_c2c_pymodel(ref):
     return d
 
 
+MMA_ARRAY_RE = re.compile(r"static\s+(?:int16_t|int32_t|uint32_t)\s+(\w+)\[[^\]]*\]\s*=\s*\{([^}]*)\}", re.S)
+MMA_ROW_RE = re.compile(r"\{STATIC,\s*staticRefInput(\d+),\s*staticRefOut\d+,\s*shiftVector\d+,\s*"
+                        r"FFTLIB_INT(16|32),\s*(\d+),\s*(\d+),\s*(\d+),")
+
+
+def mma_int_static(ref):
+    path = os.path.join(ref, "test", "fft_c7xmma", "FFTLIB_FFT_fft_ixX_cxX_oxX", "FFTLIB_FFT_fft_ixX_cxX_oxX_idat.c")
+    with open(path) as f:
+        text = f.read()
+    arr = {name: np.array([int(v, 0) for v in re.findall(r"-?0x[0-9a-fA-F]+|-?\d+", body)], np.int64)
+           for name, body in MMA_ARRAY_RE.findall(text)}
+    d, ids = {}, []
+    for cid, bits, batch, n, il in MMA_ROW_RE.findall(text):
+        cid, bits = int(cid), int(bits)
+        dt = np.int16 if bits == 16 else np.int32
+        ids.append(cid)
+        d[f"meta_{cid}"] = np.array([bits, int(batch), int(n), int(il)])
+        d[f"in_{cid}"] = arr[f"staticRefInput{cid}"].astype(dt)
+        d[f"out_{cid}"] = arr[f"staticRefOut{cid}"].astype(dt)
+        d[f"shift_{cid}"] = arr[f"shiftVector{cid}"].astype(np.uint32)
+    d["ids"] = np.array(ids)
+    return d
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -303,6 +332,7 @@ def main():
         "fft1d_c2r_static": lambda: single_static(a.ref, "FFTLIB_ifft1d_i32fc_c32fc_o32f"),
         "fft1d_i16_pymodel": lambda: fft1d_i16_pymodel(a.ref),
         "fft1d_c2c_pymodel": lambda: fft1d_c2c_pymodel(a.ref),
+        "mma_int_static": lambda: mma_int_static(a.ref),
     }
     only = [s for s in a.only.split(",") if s]
     for name, make in makers.items():

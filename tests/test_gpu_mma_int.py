@@ -1,0 +1,99 @@
+"""Bit-exact parity of the coordinator's integer paths (INT16 / INT32) on
+the GPU against the integer oracle and the reference's own natural C, and
+the reference test's 50-LSB tolerance against its committed vectors
+(FFTLIB_FFT_fft_ixX_cxX_oxX_d.c:159-170)."""
+import os
+
+import numpy as np
+import pytest
+
+import c7x_fftlib_b200 as F
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+DT = {16: F.FFTLIB_INT16, 32: F.FFTLIB_INT32}
+NP = {16: np.int16, 32: np.int32}
+
+CASES = [(4, 3, 1), (8, 2, 0), (16, 4, 1), (16, 1, 0), (32, 8, 1), (32, 4, 0), (64, 4, 1), (64, 8, 0), (64, 32, 1),
+         (64, 16, 0), (64, 16, 1), (128, 2, 1), (256, 3, 0), (1024, 2, 1), (4096, 2, 1), (512, 1, 1), (80, 2, 1),
+         (16, 1000, 1), (32, 777, 0), (256, 300, 1), (65536, 1, 1)]
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def run(torch, bits, n, batch, il, shifts, x, on_device=True, stream=False):
+    d = F.DftMma(n, batch, dtype=DT[bits], interleave=il, shifts=shifts, w_device=on_device)
+    if on_device:
+        X = torch.from_numpy(np.ascontiguousarray(x, NP[bits])).cuda()
+        Y = torch.zeros_like(X)
+        if stream:
+            s = torch.cuda.current_stream()
+            d.exec_async(X, Y, F.ptr(s.cuda_stream))
+            F.check(F.lib().FFTLIB_b200_FFT_fft_sync(F.ptr(s.cuda_stream)), "sync")
+        else:
+            d.exec(X, Y)
+        return Y.cpu().numpy()
+    X = np.array(x, NP[bits])
+    Y = np.zeros_like(X)
+    d.exec(X, Y, w=d.w_host)
+    return Y
+
+
+def _rand(bits, size, seed, full):
+    mx = (1 << (bits - 1)) - 1
+    lo, hi = (-mx - 1, mx) if full else (-1000, 1000)
+    return np.random.default_rng(seed).integers(lo, hi + 1, size)
+
+
+@pytest.mark.parametrize("bits", [16, 32])
+@pytest.mark.parametrize("n,batch,il", CASES)
+def test_bit_exact_with_oracle_and_reference_cn(torch_cuda, bits, n, batch, il):
+    if bits == 32 and n in (80, 65536):
+        pytest.skip("not a d0 x 8^L length within four stages")
+    for seed, full in ((1, False), (2, True)):
+        x = _rand(bits, 2 * n * batch, 7 * n + seed, full)
+        for sh in ([1, 1, 1, 1, 1], [4, 4, 4, 4, 4], [0, 0, 0, 0, 0], [bits - 1] * 5, [0, 3, 1, 2, 5]):
+            y = run(torch_cuda, bits, n, batch, il, sh, x)
+            want = O.mma_exec(bits, n, batch, il, sh, x)
+            assert np.array_equal(y, want), (bits, n, batch, il, sh, full)
+            if O.ref_mma_available() and n * batch <= 8192:
+                assert np.array_equal(y, O.ref_mma_exec(bits, n, batch, il, sh, x))
+
+
+@pytest.mark.parametrize("bits,n,batch,il", [(16, 16, 8, 1), (16, 64, 4, 0), (16, 1024, 2, 1), (32, 32, 4, 1),
+                                              (32, 64, 8, 0)])
+def test_host_buffers_and_stream_entry(torch_cuda, bits, n, batch, il):
+    x = _rand(bits, 2 * n * batch, 11 * n, True)
+    sh = [2, 2, 2, 2, 2]
+    want = O.mma_exec(bits, n, batch, il, sh, x)
+    assert np.array_equal(run(torch_cuda, bits, n, batch, il, sh, x, on_device=False), want)
+    assert np.array_equal(run(torch_cuda, bits, n, batch, il, sh, x, stream=True), want)
+
+
+def test_reference_committed_vectors(torch_cuda):
+    d = np.load(os.path.join(GOLDEN, "mma_int_static.npz"))
+    for cid in d["ids"]:
+        bits, batch, n, il = (int(v) for v in d[f"meta_{cid}"])
+        sh = d[f"shift_{cid}"]
+        y = run(torch_cuda, bits, n, batch, il, sh, d[f"in_{cid}"])
+        assert np.array_equal(y, O.mma_exec(bits, n, batch, il, sh, d[f"in_{cid}"])), cid
+        assert np.abs(y.astype(np.int64) - d[f"out_{cid}"].astype(np.int64)).max() <= 50, cid
+
+
+def test_high_radix_needs_distinct_buffers(torch_cuda):
+    import torch
+
+    d = F.DftMma(64, 4, dtype=F.FFTLIB_INT16, interleave=1)
+    X = torch.zeros(2 * 64 * 4, dtype=torch.int16, device="cuda")
+    st = F.lib().FFTLIB_FFT_fft_ixX_cxX_oxX_exec(d.handle, F.ptr(X), F.ptr(d.w), F.ptr(X))
+    assert st == F.FFTLIB_ERR_INVALID_VALUE
+    assert d.path == 3

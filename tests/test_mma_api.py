@@ -37,8 +37,7 @@ def test_status_codes():
     assert _sizes(0, 4)[0] == F.FFTLIB_ERR_INVALID_DIMENSION
     assert _sizes(64, 0)[0] == F.FFTLIB_ERR_INVALID_DIMENSION
     assert _sizes(64, 4, interleave=0)[0] == F.FFTLIB_ERR_NOT_IMPLEMENTED
-    assert _sizes(64, 4, dtype=F.FFTLIB_INT16)[0] == F.FFTLIB_ERR_NOT_IMPLEMENTED
-    assert _sizes(64, 4, dtype=F.FFTLIB_INT32)[0] == F.FFTLIB_ERR_NOT_IMPLEMENTED
+    assert _sizes(64, 4, dtype=F.FFTLIB_UINT32)[0] == F.FFTLIB_ERR_NOT_IMPLEMENTED
     L = F.lib()
     a = F.MmaInitArgs(1, 64, 4, 1)
     bx, bw, by = F.BufParams(F.FFTLIB_FLOAT32, 512), F.BufParams(F.FFTLIB_FLOAT32, 128 * 128), \
