@@ -433,7 +433,63 @@ def secondary_configs(args):
     mb.close()
     res["tc_dft"] = tc_dft_configs(args, steps)
     res["fft1d_single"] = fft1d_single_configs(steps)
+    res["int_dft"] = int_dft_configs(steps)
     return res
+
+
+def int_dft_configs(steps):
+    """The coordinator's integer paths (INT16 / INT32, bit-exact with the
+    reference's natural C), on device buffers through execAsync: dftSmall,
+    dftLarge and highRadix lengths with the rows of the tensor-core DFT
+    configuration (2^20 rows up to 64 points, 16 M points per launch above).
+    Bytes: one read and one write of 2 N values per row. ref_cn: the
+    reference's natural C on one host core over 256 rows of the same data."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import c7x_fftlib_b200 as F
+    import oracle as O
+
+    stream = torch.cuda.Stream()
+    sp = F.ptr(stream.cuda_stream)
+    out = {}
+    for bits, n, rows in ((16, 16, 1 << 20), (16, 32, 1 << 20), (16, 256, 1 << 16), (16, 1024, 1 << 14),
+                          (32, 8, 1 << 20), (32, 16, 1 << 20), (32, 64, 1 << 18)):
+        dt = F.FFTLIB_INT16 if bits == 16 else F.FFTLIB_INT32
+        tdt = torch.int16 if bits == 16 else torch.int32
+        sh = [bits - 1] * 5 if n <= (32 if bits == 16 else 16) else [2, 2, 2, 2, 4]
+        d = F.DftMma(n, rows, dtype=dt, interleave=1, shifts=sh)
+        lim = (1 << (bits - 1)) - 1
+        x0 = torch.randint(-lim, lim, (2 * n * rows,), dtype=torch.int64, device="cuda").to(tdt)
+        x = x0.clone()
+        y = torch.empty_like(x)
+        ms = _time_launches(torch, stream, lambda: d.exec_async(x, y, sp), max(steps, 10))
+        F.check(F.lib().FFTLIB_b200_FFT_fft_sync(sp), "sync")
+        # bit-exact spot check against the oracle (highRadix overwrote x: rerun on a fresh copy)
+        x.copy_(x0)
+        d.exec_async(x, y, sp)
+        F.check(F.lib().FFTLIB_b200_FFT_fft_sync(sp), "sync")
+        k = min(rows, 64)
+        xs = x0[: 2 * n * k].cpu().numpy()
+        want = O.mma_exec(bits, n, k, 1, sh, xs)
+        exact = bool(np.array_equal(y[: 2 * n * k].cpu().numpy(), want))
+        entry = {"variant": O.mma_variant(bits, n, rows, 1), "rows": rows, "ms": round(ms, 4),
+                 "GBps": round(2.0 * 2 * n * rows * (bits // 8) / ms / 1e6, 1),
+                 "rows_per_s": round(rows / ms * 1e3, 1), "bit_exact_sample": exact}
+        if O.ref_mma_available():
+            kr = 256
+            xr = x0[: 2 * n * kr].cpu().numpy()
+            t0 = time.perf_counter()
+            O.ref_mma_exec(bits, n, kr, 1, sh, xr)
+            t_ref = time.perf_counter() - t0
+            entry["ref_cn_rows_per_s"] = round(kr / t_ref, 1)
+            entry["ref_cn_cores"] = 1
+            entry["speedup_vs_ref_cn"] = round(entry["rows_per_s"] / entry["ref_cn_rows_per_s"], 1)
+        out[f"int{bits}_n{n}"] = entry
+        del x, x0, y
+    return out
 
 
 def fft1d_single_configs(steps):
@@ -638,6 +694,17 @@ def run_case(args):
 
         def launch():
             k(F.ptr(x), F.ptr(wd), F.ptr(y), F.ptr(sh), ns, n, batch, pb, sp)
+    elif kind in ("int16", "int32"):  # the coordinator's integer path, interleaved
+        bits = int(kind[3:])
+        dt = F.FFTLIB_INT16 if bits == 16 else F.FFTLIB_INT32
+        tdt = torch.int16 if bits == 16 else torch.int32
+        nbytes = 2.0 * 2 * n * batch * (bits // 8)
+        d = F.DftMma(n, batch, dtype=dt, interleave=1, shifts=[2, 2, 2, 2, 4])
+        x = torch.randint(-1000, 1000, (2 * n * batch,), dtype=torch.int64, device="cuda").to(tdt)
+        y = torch.empty_like(x)
+
+        def launch():
+            d.exec_async(x, y, sp)
     elif kind == "mixed":  # mixed:COUNT:SEED -- the uneven-length batch, one graph launch
         lengths = np.sort(mixed_lengths(n, seed=batch))[::-1].copy()
         total = int(lengths.sum())

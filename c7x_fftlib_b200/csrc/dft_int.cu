@@ -4,6 +4,7 @@
 // results depend on every rounding step, so the data never leaves integers.
 #include <math.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -80,36 +81,77 @@ __device__ __forceinline__ typename IntT<T>::Acc mul(T a, T b)
     return (typename IntT<T>::Acc)((long long)a * (long long)b);
 }
 
+// acc + a b, exact: one 32 x 32 -> 64-bit multiply-add for INT16 data, a
+// 64-bit product added into the 128-bit sum for INT32.
+__device__ __forceinline__ long long mac(long long acc, int16_t a, int16_t b)
+{
+    long long d;
+    asm("mad.wide.s32 %0, %1, %2, %3;" : "=l"(d) : "r"((int)a), "r"((int)b), "l"(acc));
+    return d;
+}
+__device__ __forceinline__ __int128 mac(__int128 acc, int32_t a, int32_t b)
+{
+    long long p;
+    asm("mul.wide.s32 %0, %1, %2;" : "=l"(p) : "r"(a), "r"(b));
+    return acc + (__int128)p;
+}
+
 // ---- dftSmall / dftLarge: Y = round_shift(X W) -------------------------------
 
-// Each CTA stages W (n2 x n2 of the caller's table, row stride ld) and up to
-// kGemmRows rows of X in shared memory, then every thread forms exact dot
-// products of its outputs. In place when x == y (a CTA reads its rows first).
+// Persistent CTAs: each stages W (n2 x n2 of the caller's table, row stride
+// ld) in shared memory once, then walks tiles of kGemmRows rows of X, stored
+// transposed so that element k of 4 consecutive rows is one vector; every
+// thread forms the exact dot products of one output column for 4 rows (one
+// W load and one vector X load per 4 multiply-adds). In place when x == y
+// (a tile is read completely before it is written).
 constexpr uint32_t kGemmRows = 32;
+
+template <class T> struct Vec4;
+template <> struct Vec4<int16_t> { using type = short4; };
+template <> struct Vec4<int32_t> { using type = int4; };
 
 template <class T>
 __global__ void __launch_bounds__(256) k_int_gemm(const T* x, const T* __restrict__ w, T* y, uint32_t n2,
                                                   uint32_t ld, uint32_t rows, uint32_t shift)
 {
+    using V = typename Vec4<T>::type;
     extern __shared__ __align__(16) unsigned char s_raw[];
     T* ws = reinterpret_cast<T*>(s_raw);
-    T* xs = ws + n2 * n2;
-    const uint32_t r0 = blockIdx.x * kGemmRows;
-    const uint32_t nr = min(kGemmRows, rows - r0);
+    T* xt = ws + n2 * n2;  // [k][row], kGemmRows rows
     for (uint32_t e = threadIdx.x; e < n2 * n2; e += blockDim.x) {
         const uint32_t k = e / n2;
         ws[e] = w[k * ld + (e - k * n2)];
     }
-    const T* xr = x + (size_t)r0 * n2;
-    for (uint32_t e = threadIdx.x; e < nr * n2; e += blockDim.x) xs[e] = xr[e];
-    __syncthreads();
-    T* yr = y + (size_t)r0 * n2;
-    for (uint32_t e = threadIdx.x; e < nr * n2; e += blockDim.x) {
-        const uint32_t r = e / n2, j = e - r * n2;
-        typename IntT<T>::Acc acc = 0;
-        const T* a = xs + r * n2;
-        for (uint32_t k = 0; k < n2; ++k) acc += mul<T>(a[k], ws[k * n2 + j]);
-        yr[e] = shift_round<T>(acc, shift);
+    const V* xv = reinterpret_cast<const V*>(xt);
+    const uint32_t tiles = (rows + kGemmRows - 1) / kGemmRows;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t r0 = tile * kGemmRows;
+        const uint32_t nr = min(kGemmRows, rows - r0);
+        const T* xr = x + (size_t)r0 * n2;
+        __syncthreads();  // the previous tile's reads of xt are done
+        for (uint32_t e = threadIdx.x; e < kGemmRows * n2; e += blockDim.x) {
+            const uint32_t r = e / n2, k = e - r * n2;
+            xt[k * kGemmRows + r] = r < nr ? xr[e] : (T)0;
+        }
+        __syncthreads();
+        T* yr = y + (size_t)r0 * n2;
+        for (uint32_t e = threadIdx.x; e < (kGemmRows / 4) * n2; e += blockDim.x) {
+            const uint32_t g = e / n2, j = e - g * n2;  // rows 4g..4g+3, column j
+            typename IntT<T>::Acc a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+            for (uint32_t k = 0; k < n2; ++k) {
+                const T wk = ws[k * n2 + j];
+                const V v = xv[k * (kGemmRows / 4) + g];
+                a0 = mac(a0, v.x, wk);
+                a1 = mac(a1, v.y, wk);
+                a2 = mac(a2, v.z, wk);
+                a3 = mac(a3, v.w, wk);
+            }
+            const uint32_t r = 4 * g;
+            if (r < nr) yr[(size_t)r * n2 + j] = shift_round<T>(a0, shift);
+            if (r + 1 < nr) yr[(size_t)(r + 1) * n2 + j] = shift_round<T>(a1, shift);
+            if (r + 2 < nr) yr[(size_t)(r + 2) * n2 + j] = shift_round<T>(a2, shift);
+            if (r + 3 < nr) yr[(size_t)(r + 3) * n2 + j] = shift_round<T>(a3, shift);
+        }
     }
 }
 
@@ -151,8 +193,8 @@ __global__ void __launch_bounds__(256) k_int_stage(T* buf, uint32_t n, uint32_t 
         for (uint32_t m = 0; m < R; ++m) {
             if (m < rad) {
                 const T c0 = f[2 * m], c1 = f[2 * m + 1];
-                yi += mul<T>(c0, ai[m]) + mul<T>(c1, ar[m]);
-                yr += mul<T>(c0, ar[m]) + mul<T>(c1, neg_sat<T>(ai[m]));
+                yi = mac(mac(yi, c0, ai[m]), c1, ar[m]);
+                yr = mac(mac(yr, c0, ar[m]), c1, neg_sat<T>(ai[m]));
             }
         }
         const T tr = shift_round<T>(yr, shift), ti = shift_round<T>(yi, shift);
@@ -208,8 +250,8 @@ __global__ void __launch_bounds__(256) k_int_final(const T* buf, T* y, uint32_t 
         const T* di = D + (2u * l + 1u) * MMA;
 #pragma unroll
         for (uint32_t q = 0; q < R; ++q) {
-            xr += mul<T>(dr[2 * q], ai[q]) + mul<T>(dr[2 * q + 1], ar[q]);
-            xi += mul<T>(di[2 * q], ai[q]) + mul<T>(di[2 * q + 1], ar[q]);
+            xr = mac(mac(xr, dr[2 * q], ai[q]), dr[2 * q + 1], ar[q]);
+            xi = mac(mac(xi, di[2 * q], ai[q]), di[2 * q + 1], ar[q]);
         }
         const uint32_t p = l * G + dst0;
         const T vr = shift_round<T>(xr, shift), vi = shift_round<T>(xi, shift);
@@ -315,12 +357,19 @@ cudaError_t launch_typed(uint32_t n, uint32_t batch, uint32_t interleave, const 
     const int v = int_dft_variant(bits, n, batch, interleave);
     if (v == INT_DFT_SMALL || v == INT_DFT_LARGE) {
         const uint32_t n2 = 2u * n, ld = v == INT_DFT_SMALL ? MMA : n2;
-        const size_t smem = (size_t)(n2 * n2 + kGemmRows * n2) * sizeof(T);
+        const size_t smem = (size_t)(n2 * n2 + kGemmRows * n2) * sizeof(T);  // x tile 16-byte aligned: n2 is even
         if (smem > 48u * 1024u) {
             cudaError_t e = cudaFuncSetAttribute(k_int_gemm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
-        k_int_gemm<T><<<(batch + kGemmRows - 1) / kGemmRows, 256, smem, s>>>(x, w, y, n2, ld, batch, shifts[0]);
+        int dev = 0, sms = 0, per = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_int_gemm<T>, 256, smem);
+        if (e != cudaSuccess) return e;
+        const uint32_t tiles = (batch + kGemmRows - 1) / kGemmRows;
+        const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)std::max(1, per * sms));
+        k_int_gemm<T><<<grid, 256, smem, s>>>(x, w, y, n2, ld, batch, shifts[0]);
         return cudaGetLastError();
     }
     if (!int_high_radix_covered(bits, n) || x == y) return cudaErrorInvalidValue;
