@@ -29,8 +29,12 @@ FFTLIB_ERR_NOT_IMPLEMENTED = 6
 FFTLIB_ERR_NOT_ALIGNED_PTRS_STRIDES = 8
 FFTLIB_ERR_INVALID_SHIFT = 12
 FFTLIB_ERR_INVALID_OUTMODE = 14
+FFTLIB_ERR_MATRIX_MATRIX_MULTIPLY_UNSUPPORTED_INPUT_TYPE = 10000
+FFTLIB_ERR_MATRIX_MATRIX_MULTIPLY_UNSUPPORTED_OUTPUT_TYPE = 10001
+FFTLIB_ERR_MATRIX_MATRIX_MULTIPLY_UNSUPPORTED_TYPE_COMBINATION = 10002
 
 # FFTLIB_data_type_e (src/common/FFTLIB_bufParams.h:22-42)
+FFTLIB_INT8 = 0
 FFTLIB_INT16 = 1
 FFTLIB_INT32 = 2
 FFTLIB_UINT32 = 8
@@ -70,6 +74,33 @@ class MmaInitArgs(C.Structure):
     _fields_ = [("funcStyle", C.c_int8), ("fftSize", C.c_uint32), ("batchSize", C.c_uint32),
                 ("interleave", C.c_uint32), ("shiftVector", C.c_uint32 * 5)]
 
+
+class DftVariantInitArgs(C.Structure):
+    """FFTLIB_FFT_dftSmall_ixX_cxX_oxX_InitArgs and FFTLIB_FFT_dftLarge_ixX_cxX_oxX_InitArgs
+    (..._dftSmall_ixX_cxX_oxX.h:40-62, ..._dftLarge_ixX_cxX_oxX.h:42-64: one shift).
+    The highRadixDecompositions InitArgs has the coordinator's layout (five shifts)."""
+    _fields_ = [("funcStyle", C.c_int8), ("fftSize", C.c_uint32), ("batchSize", C.c_uint32),
+                ("interleave", C.c_uint32), ("shiftVector", C.c_uint32 * 1)]
+
+
+class BufParams2D(C.Structure):
+    """FFTLIB_bufParams2D_t (src/common/FFTLIB_bufParams.h:69-78): stride_y in bytes."""
+    _fields_ = [("data_type", C.c_uint32), ("dim_x", C.c_uint32), ("dim_y", C.c_uint32), ("stride_y", C.c_int32)]
+
+
+class LinalgInitArgs(C.Structure):
+    """FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX_InitArgs
+    (src/linalg_c7xmma/FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX/..._oxX.h:48-51)."""
+    _fields_ = [("funcStyle", C.c_int8), ("shift", C.c_int8)]
+
+
+# the coordinator's variants as separate kernels: name prefix and InitArgs type
+DFT_VARIANTS = {
+    "dftSmall": ("FFTLIB_FFT_dftSmall_ixX_cxX_oxX_", DftVariantInitArgs),
+    "dftLarge": ("FFTLIB_FFT_dftLarge_ixX_cxX_oxX_", DftVariantInitArgs),
+    "highRadix": ("FFTLIB_FFT_highRadixDecompositions_ixX_cxX_oxX_", MmaInitArgs),
+}
+LINALG = "FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX_"
 
 # paths the coordinator's init picks (FFTLIB_b200_FFT_fft_path)
 MMA_PATH_TC = 1
@@ -178,6 +209,29 @@ def lib() -> C.CDLL:
     getattr(L, M + "exec_checkParams").argtypes = [_vp, _vp, _vp, _vp]
     for f in ("getSizes", "twGen", "init", "init_checkParams", "exec", "exec_checkParams"):
         getattr(L, M + f).restype = C.c_int
+    for prefix, args_t in DFT_VARIANTS.values():
+        _va = C.POINTER(args_t)
+        getattr(L, prefix + "getHandleSize").argtypes = [_va]
+        getattr(L, prefix + "getHandleSize").restype = C.c_int32
+        getattr(L, prefix + "getSizes").argtypes = [_va, _bpp, _bpp, _bpp]
+        getattr(L, prefix + "twGen").argtypes = [_va, _vp, _bpp]
+        getattr(L, prefix + "init").argtypes = [_vp, _bpp, _bpp, _bpp, _va]
+        getattr(L, prefix + "init_checkParams").argtypes = [_vp, _bpp, _bpp, _bpp, _va]
+        getattr(L, prefix + "exec").argtypes = [_vp, _vp, _vp, _vp]
+        getattr(L, prefix + "exec_checkParams").argtypes = [_vp, _vp, _vp, _vp]
+        for f in ("getSizes", "twGen", "init", "init_checkParams", "exec", "exec_checkParams"):
+            getattr(L, prefix + f).restype = C.c_int
+    _la, _b2 = C.POINTER(LinalgInitArgs), C.POINTER(BufParams2D)
+    getattr(L, LINALG + "getHandleSize").argtypes = [_la]
+    getattr(L, LINALG + "getHandleSize").restype = C.c_int32
+    getattr(L, LINALG + "init").argtypes = [_vp, _b2, _b2, _b2, _la]
+    getattr(L, LINALG + "init_checkParams").argtypes = [_vp, _b2, _b2, _b2, _la]
+    getattr(L, LINALG + "exec").argtypes = [_vp, _vp, _vp, _vp]
+    getattr(L, LINALG + "exec_checkParams").argtypes = [_vp, _vp, _vp, _vp]
+    for f in ("init", "init_checkParams", "exec", "exec_checkParams"):
+        getattr(L, LINALG + f).restype = C.c_int
+    L.FFTLIB_b200_LINALG_matrixMatrixMultiply_execAsync.argtypes = [_vp, _vp, _vp, _vp, _vp]
+    L.FFTLIB_b200_LINALG_matrixMatrixMultiply_execAsync.restype = C.c_int
     L.FFTLIB_b200_FFT_fft_execAsync.argtypes = [_vp, _vp, _vp, _vp, _vp]
     L.FFTLIB_b200_FFT_fft_execAsync.restype = C.c_int
     L.FFTLIB_b200_FFT_fft_sync.argtypes = [_vp]
@@ -282,14 +336,18 @@ class DftMma:
     (dtype, interleave and the five-entry shift vector as in its InitArgs)."""
 
     def __init__(self, n: int, batch: int, func_style: int = FFTLIB_FUNCTION_OPTIMIZED, w_device=True,
-                 dtype: int = FFTLIB_FLOAT32, interleave: int = 1, shifts=None):
+                 dtype: int = FFTLIB_FLOAT32, interleave: int = 1, shifts=None, variant: str | None = None):
+        """variant None: the coordinator; "dftSmall", "dftLarge" or "highRadix":
+        that kernel on its own (FFTLIB_FFT_<variant>_ixX_cxX_oxX_*)."""
         import numpy as _np
 
         L = lib()
-        M = "FFTLIB_FFT_fft_ixX_cxX_oxX_"
+        M, args_t = ("FFTLIB_FFT_fft_ixX_cxX_oxX_", MmaInitArgs) if variant is None else DFT_VARIANTS[variant]
+        self.prefix = M
         self.n, self.batch, self.dtype = n, batch, dtype
-        self.args = MmaInitArgs(func_style, n, batch, interleave)
-        for i, v in enumerate([] if shifts is None else list(shifts)):
+        self.args = args_t(func_style, n, batch, interleave)
+        nsh = len(self.args.shiftVector)
+        for i, v in enumerate([] if shifts is None else list(shifts)[:nsh]):
             self.args.shiftVector[i] = int(v)
         self.bx, self.bw, self.by = (BufParams(dtype, 0) for _ in range(3))
         check(getattr(L, M + "getSizes")(C.byref(self.args), self.bx, self.bw, self.by), "getSizes")
@@ -314,8 +372,38 @@ class DftMma:
 
     def exec(self, x, y, w=None):
         w = self.w if w is None else w
-        check(lib().FFTLIB_FFT_fft_ixX_cxX_oxX_exec(self.handle, ptr(x), ptr(w), ptr(y)), "exec")
+        check(getattr(lib(), self.prefix + "exec")(self.handle, ptr(x), ptr(w), ptr(y)), "exec")
 
     def exec_async(self, x, y, stream=None, w=None):
         w = self.w if w is None else w
         check(lib().FFTLIB_b200_FFT_fft_execAsync(self.handle, ptr(x), ptr(w), ptr(y), stream), "execAsync")
+
+
+class MatMul:
+    """FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX_*: C = shiftAndRound(A B)
+    for INT8 / INT16 / INT32 (init_checkParams, init, then exec or the
+    stream-ordered execAsync). Strides are row strides in elements (default:
+    dense rows)."""
+
+    ELEM = {FFTLIB_INT8: 1, FFTLIB_INT16: 2, FFTLIB_INT32: 4}
+
+    def __init__(self, m: int, k: int, n: int, dtype: int, shift: int = 0,
+                 func_style: int = FFTLIB_FUNCTION_OPTIMIZED, lda=None, ldb=None, ldc=None):
+        L = lib()
+        es = self.ELEM.get(dtype, 1)
+        self.m, self.k, self.n, self.dtype = m, k, n, dtype
+        self.args = LinalgInitArgs(func_style, shift)
+        self.a = BufParams2D(dtype, k, m, (k if lda is None else lda) * es)
+        self.b = BufParams2D(dtype, n, k, (n if ldb is None else ldb) * es)
+        self.c = BufParams2D(dtype, n, m, (n if ldc is None else ldc) * es)
+        self.handle = C.create_string_buffer(getattr(L, LINALG + "getHandleSize")(C.byref(self.args)))
+        check(getattr(L, LINALG + "init_checkParams")(self.handle, self.a, self.b, self.c, C.byref(self.args)),
+              "init_checkParams")
+        check(getattr(L, LINALG + "init")(self.handle, self.a, self.b, self.c, C.byref(self.args)), "init")
+
+    def exec(self, a, b, c):
+        check(getattr(lib(), LINALG + "exec")(self.handle, ptr(a), ptr(b), ptr(c)), "exec")
+
+    def exec_async(self, a, b, c, stream=None):
+        check(lib().FFTLIB_b200_LINALG_matrixMatrixMultiply_execAsync(self.handle, ptr(a), ptr(b), ptr(c), stream),
+              "execAsync")

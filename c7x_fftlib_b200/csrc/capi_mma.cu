@@ -16,6 +16,7 @@
 #include "capi_common.h"
 #include "dft_int.h"
 #include "fft_c7xmma.h"
+#include "fft_c7xmma_variants.h"
 #include "fftlib_b200_ext.h"
 #include "plan.h"
 #include "tc_dft.h"
@@ -32,9 +33,15 @@ struct MmaHandle {
     int32_t path;
     int32_t device;
     int32_t bits;       // PATH_INT: 16 or 32
+    int32_t variant;    // PATH_INT: the variant fixed by a variant's init (0: the coordinator's rule)
     FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs init;
     ComplexPlan* plan;  // CUDA-core FFT plan of fftSize (FLOAT32)
 };
+
+int variant_of(const MmaHandle* m)
+{
+    return m->variant ? m->variant : int_dft_variant(m->bits, m->init.fftSize, m->init.batchSize, m->init.interleave);
+}
 
 int int_bits(uint32_t type) { return type == FFTLIB_INT16 ? 16 : (type == FFTLIB_INT32 ? 32 : 0); }
 
@@ -93,7 +100,7 @@ MmaHandle* handle_of(FFTLIB_kernelHandle h)
 {
     MmaHandle* m = static_cast<MmaHandle*>(h);
     if (!m || m->magic != kMmaMagic || m->path == PATH_NONE) {
-        set_error("handle was not set up by FFTLIB_FFT_fft_ixX_cxX_oxX_init");
+        set_error("handle was not set up by the init of the coordinator or of one of its variants");
         return nullptr;
     }
     return m;
@@ -102,8 +109,8 @@ MmaHandle* handle_of(FFTLIB_kernelHandle h)
 cudaError_t enqueue(const MmaHandle* m, const float* x, const float* w, float* y, uint32_t batch, cudaStream_t s)
 {
     if (m->path == PATH_INT)
-        return int_dft_launch(m->bits, m->init.fftSize, batch, m->init.interleave, m->init.shiftVector,
-                              const_cast<float*>(x), w, y, s);
+        return int_dft_launch_v(m->bits, variant_of(m), m->init.fftSize, batch, m->init.interleave,
+                                m->init.shiftVector, const_cast<float*>(x), w, y, s);
     // the tensor-core kernels read and prefetch whole 16-byte lines; buffers
     // that are only 8-byte aligned take the FFT
     const bool aligned = (((uintptr_t)x | (uintptr_t)y) & 15u) == 0;
@@ -293,14 +300,12 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_exec(FFTLIB_kernelHandle handle, void* 
     const void* w = pW;
     const size_t elem = m->path == PATH_INT ? (size_t)m->bits / 8u : sizeof(float);
     if (m->path == PATH_TC || m->path == PATH_INT) {
-        const size_t wbytes = m->path == PATH_TC
-                                  ? tc_dft_w_floats(n) * sizeof(float)
-                                  : (size_t)int_dft_w_size(m->bits, n, m->init.batchSize, m->init.interleave) * elem;
+        const size_t wbytes = m->path == PATH_TC ? tc_dft_w_floats(n) * sizeof(float)
+                                                 : (size_t)int_dft_w_size_v(m->bits, variant_of(m), n) * elem;
         cudaError_t e = device_table(pW, wbytes, 2, &w);
         if (e != cudaSuccess) return cuda_fail(e, "computational matrix copy");
     }
-    if (m->path == PATH_INT && pX == pY &&
-        int_dft_variant(m->bits, n, m->init.batchSize, m->init.interleave) == INT_HIGH_RADIX) {
+    if (m->path == PATH_INT && pX == pY && variant_of(m) == INT_HIGH_RADIX) {
         set_error("the high-radix path works in pX and needs pY != pX");
         return FFTLIB_ERR_INVALID_VALUE;
     }
@@ -323,8 +328,7 @@ FFTLIB_STATUS FFTLIB_b200_FFT_fft_execAsync(FFTLIB_kernelHandle handle, void* pX
         set_error("execAsync needs device buffers");
         return FFTLIB_ERR_INVALID_VALUE;
     }
-    if (m->path == PATH_INT && pX == pY &&
-        int_dft_variant(m->bits, m->init.fftSize, m->init.batchSize, m->init.interleave) == INT_HIGH_RADIX) {
+    if (m->path == PATH_INT && pX == pY && variant_of(m) == INT_HIGH_RADIX) {
         set_error("the high-radix path works in pX and needs pY != pX");
         return FFTLIB_ERR_INVALID_VALUE;
     }
@@ -346,5 +350,222 @@ int32_t FFTLIB_b200_FFT_fft_path(FFTLIB_kernelHandle handle)
     const MmaHandle* m = static_cast<const MmaHandle*>(handle);
     return (m && m->magic == kMmaMagic) ? m->path : PATH_NONE;
 }
+
+uint8_t FFTLIB_FFT_twData[32 * 32 * 3 * sizeof(int16_t)];
+
+} // extern "C"
+
+// ---- the variants on their own (fft_c7xmma_variants.h) ----------------------------
+//
+// The same handle, tables and kernels as the coordinator, with the variant
+// fixed by which init was called. The checks follow each variant's
+// init_checkParams (src/fft_c7xmma/FFTLIB_FFT_dftSmall_ixX_cxX_oxX/
+// FFTLIB_FFT_dftSmall_ixX_cxX_oxX.cpp:13-52, ..._dftLarge_ixX_cxX_oxX.cpp:13-75,
+// ..._highRadixDecompositions_ixX_cxX_oxX.cpp:14-66) and getSizes
+// (c71/..._ci.cpp: dftSmall 74-106, dftLarge 43-75, highRadix 1975-2025).
+namespace {
+
+template <class VArgs>
+FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs coordinator_args(const VArgs* a)
+{
+    FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs c;
+    memset(&c, 0, sizeof(c));
+    c.funcStyle = a->funcStyle;
+    c.fftSize = a->fftSize;
+    c.batchSize = a->batchSize;
+    c.interleave = a->interleave;
+    for (size_t i = 0; i < sizeof(a->shiftVector) / sizeof(a->shiftVector[0]); ++i) c.shiftVector[i] = a->shiftVector[i];
+    return c;
+}
+
+// getSizes of one variant: X, W and Y elements.
+FFTLIB_STATUS variant_sizes(int variant, const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs& a, uint32_t type, uint32_t* x,
+                            uint32_t* w, uint32_t* y)
+{
+    const int bits = int_bits(type);
+    if (!bits) {
+        set_error("data type %u: the DFT variants implement INT16 (%d) and INT32 (%d)", type, FFTLIB_INT16,
+                  FFTLIB_INT32);
+        return FFTLIB_ERR_NOT_IMPLEMENTED;
+    }
+    const uint32_t mma = (uint32_t)int_mma_size(bits), n = a.fftSize;
+    if (variant == INT_DFT_SMALL && n > mma / 2) {
+        set_error("dftSmall: fftSize %u above MMA/2 = %u", n, mma / 2);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    if (variant == INT_DFT_LARGE && n <= mma / 2) {
+        set_error("dftLarge: fftSize %u not above MMA/2 = %u", n, mma / 2);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    const uint64_t xy = 2ull * n * a.batchSize;
+    if (xy > 0xFFFFFFFFull || (variant == INT_DFT_LARGE && 4ull * n * n > 0xFFFFFFFFull)) {
+        set_error("fftSize %u x batchSize %u exceeds the 32-bit dim_x", n, a.batchSize);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    *x = *y = (uint32_t)xy;
+    *w = int_dft_w_size_v(bits, variant, n);
+    return FFTLIB_SUCCESS;
+}
+
+FFTLIB_STATUS variant_get_sizes(int variant, const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs& a,
+                                FFTLIB_bufParams1D_t* bx, FFTLIB_bufParams1D_t* bw, FFTLIB_bufParams1D_t* by)
+{
+    if (!bx || !bw || !by) return FFTLIB_ERR_NULL_POINTER;
+    uint32_t x, w, y;
+    const FFTLIB_STATUS st = variant_sizes(variant, a, bx->data_type, &x, &w, &y);
+    if (st != FFTLIB_SUCCESS) return st;
+    bx->dim_x = x;
+    bw->dim_x = w;
+    by->dim_x = y;
+    return FFTLIB_SUCCESS;
+}
+
+FFTLIB_STATUS variant_tw_gen(int variant, const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs& a, void* pW,
+                             const FFTLIB_bufParams1D_t* bw)
+{
+    if (!pW || !bw) return FFTLIB_ERR_NULL_POINTER;
+    uint32_t x, w, y;
+    const FFTLIB_STATUS st = variant_sizes(variant, a, bw->data_type, &x, &w, &y);
+    if (st != FFTLIB_SUCCESS) return st;
+    if (bw->dim_x != w) {
+        set_error("bufParamsW->dim_x %u, expected %u", bw->dim_x, w);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    const int bits = int_bits(bw->data_type);
+    if (!is_device_ptr(pW)) {
+        int_dft_twgen_host_v(bits, variant, a.fftSize, a.batchSize, a.interleave, pW);
+        return FFTLIB_SUCCESS;
+    }
+    std::vector<unsigned char> tmp((size_t)w * (bits / 8));
+    int_dft_twgen_host_v(bits, variant, a.fftSize, a.batchSize, a.interleave, tmp.data());
+    const cudaError_t e = cudaMemcpy(pW, tmp.data(), tmp.size(), cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen copy");
+}
+
+FFTLIB_STATUS variant_check(int variant, FFTLIB_kernelHandle handle, const FFTLIB_bufParams1D_t* bx,
+                            const FFTLIB_bufParams1D_t* bw, const FFTLIB_bufParams1D_t* by,
+                            const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs& a)
+{
+    if (!handle) return FFTLIB_ERR_NULL_POINTER;
+    if (!bx || !bw || !by) return FFTLIB_ERR_NULL_POINTER;
+    uint32_t x, w, y;
+    const FFTLIB_STATUS st = variant_sizes(variant, a, bx->data_type, &x, &w, &y);
+    if (st != FFTLIB_SUCCESS) return st;
+    const int bits = int_bits(bx->data_type);
+    if (variant == INT_HIGH_RADIX && a.fftSize < 2u * (uint32_t)int_mma_size(bits)) {
+        set_error("highRadix: fftSize %u below 2 MMA = %d", a.fftSize, 2 * int_mma_size(bits));
+        return FFTLIB_ERR_INVALID_VALUE;
+    }
+    if (bx->dim_x != x || by->dim_x != y || bw->dim_x != w) {
+        set_error("dim_x X/W/Y = %u/%u/%u, expected %u/%u/%u", bx->dim_x, bw->dim_x, by->dim_x, x, w, y);
+        return FFTLIB_ERR_INVALID_DIMENSION;
+    }
+    if (bw->data_type != bx->data_type || by->data_type != bx->data_type) return FFTLIB_ERR_INVALID_TYPE;
+    // dftLarge: the LINALG multiply's own check (its shift is int8_t)
+    if (variant == INT_DFT_LARGE && (int8_t)a.shiftVector[0] > (bits == 16 ? 64 : 128))
+        return FFTLIB_ERR_INVALID_SHIFT;
+    return FFTLIB_SUCCESS;
+}
+
+FFTLIB_STATUS variant_init(int variant, FFTLIB_kernelHandle handle, const FFTLIB_bufParams1D_t* bx,
+                           const FFTLIB_FFT_fft_ixX_cxX_oxX_InitArgs& a)
+{
+    if (!handle || !bx) return FFTLIB_ERR_NULL_POINTER;
+    MmaHandle* m = static_cast<MmaHandle*>(handle);
+    memset(m, 0, sizeof(*m));
+    uint32_t x, w, y;
+    const FFTLIB_STATUS st = variant_sizes(variant, a, bx->data_type, &x, &w, &y);
+    if (st != FFTLIB_SUCCESS) return st;
+    const int bits = int_bits(bx->data_type);
+    const uint32_t n = a.fftSize;
+    if (n == 0 || a.batchSize == 0) return FFTLIB_ERR_INVALID_DIMENSION;
+    if (variant == INT_HIGH_RADIX) {
+        if (n < 2u * (uint32_t)int_mma_size(bits)) {
+            set_error("highRadix: fftSize %u below 2 MMA = %d", n, 2 * int_mma_size(bits));
+            return FFTLIB_ERR_INVALID_VALUE;
+        }
+        if (!int_high_radix_covered(bits, n)) {
+            set_error("INT%d fftSize %u: the high-radix decomposition needs d0 x %u^L points, d0 <= %u, L <= 4",
+                      bits, n, int_mma_size(bits) / 2, int_mma_size(bits) / 2);
+            return FFTLIB_ERR_NOT_IMPLEMENTED;
+        }
+        // the reference's init leaves the internal table in FFTLIB_FFT_twData
+        int_dft_w1_host(bits, n, FFTLIB_FFT_twData);
+    }
+    int dev = 0;
+    const cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    m->init = a;
+    m->device = dev;
+    m->bits = bits;
+    m->variant = variant;
+    m->path = PATH_INT;
+    m->magic = kMmaMagic;
+    return FFTLIB_SUCCESS;
+}
+
+} // namespace
+
+extern "C" {
+
+#define FFTLIB_B200_DFT_VARIANT(NAME, VARIANT, INIT_CONST, EXEC_X_CONST, EXEC_W_CONST)                              \
+    int32_t FFTLIB_FFT_##NAME##_getHandleSize(FFTLIB_FFT_##NAME##_InitArgs* pKerInitArgs)                            \
+    {                                                                                                                \
+        (void)pKerInitArgs;                                                                                          \
+        return (int32_t)sizeof(MmaHandle);                                                                           \
+    }                                                                                                                \
+    FFTLIB_STATUS FFTLIB_FFT_##NAME##_getSizes(const FFTLIB_FFT_##NAME##_InitArgs* pKerInitArgs,                     \
+                                               FFTLIB_bufParams1D_t* bufParamsX, FFTLIB_bufParams1D_t* bufParamsW,    \
+                                               FFTLIB_bufParams1D_t* bufParamsY)                                     \
+    {                                                                                                                \
+        if (!pKerInitArgs) return FFTLIB_ERR_NULL_POINTER;                                                           \
+        return variant_get_sizes(VARIANT, coordinator_args(pKerInitArgs), bufParamsX, bufParamsW, bufParamsY);      \
+    }                                                                                                                \
+    FFTLIB_STATUS FFTLIB_FFT_##NAME##_twGen(const FFTLIB_FFT_##NAME##_InitArgs* pKerInitArgs, void* pW,              \
+                                            const FFTLIB_bufParams1D_t* bufParamsW)                                  \
+    {                                                                                                                \
+        if (!pKerInitArgs) return FFTLIB_ERR_NULL_POINTER;                                                           \
+        return variant_tw_gen(VARIANT, coordinator_args(pKerInitArgs), pW, bufParamsW);                              \
+    }                                                                                                                \
+    FFTLIB_STATUS FFTLIB_FFT_##NAME##_init_checkParams(                                                              \
+        FFTLIB_kernelHandle handle, const FFTLIB_bufParams1D_t* bufParamsX, const FFTLIB_bufParams1D_t* bufParamsW,  \
+        const FFTLIB_bufParams1D_t* bufParamsY, const FFTLIB_FFT_##NAME##_InitArgs* pKerInitArgs)                    \
+    {                                                                                                                \
+        if (!pKerInitArgs) return FFTLIB_ERR_NULL_POINTER;                                                           \
+        return variant_check(VARIANT, handle, bufParamsX, bufParamsW, bufParamsY, coordinator_args(pKerInitArgs));   \
+    }                                                                                                                \
+    FFTLIB_STATUS FFTLIB_FFT_##NAME##_init(FFTLIB_kernelHandle handle, INIT_CONST FFTLIB_bufParams1D_t* bufParamsX,  \
+                                           INIT_CONST FFTLIB_bufParams1D_t* bufParamsW,                              \
+                                           INIT_CONST FFTLIB_bufParams1D_t* bufParamsY,                              \
+                                           INIT_CONST FFTLIB_FFT_##NAME##_InitArgs* pKerInitArgs)                    \
+    {                                                                                                                \
+        (void)bufParamsW;                                                                                            \
+        (void)bufParamsY;                                                                                            \
+        if (!pKerInitArgs) return FFTLIB_ERR_NULL_POINTER;                                                           \
+        return variant_init(VARIANT, handle, bufParamsX, coordinator_args(pKerInitArgs));                            \
+    }                                                                                                                \
+    FFTLIB_STATUS FFTLIB_FFT_##NAME##_exec_checkParams(FFTLIB_kernelHandle handle, const void* pX, const void* pW,   \
+                                                       const void* pY)                                               \
+    {                                                                                                                \
+        (void)handle;                                                                                                \
+        return (!pX || !pW || !pY) ? FFTLIB_ERR_NULL_POINTER : FFTLIB_SUCCESS;                                       \
+    }                                                                                                                \
+    FFTLIB_STATUS FFTLIB_FFT_##NAME##_exec(FFTLIB_kernelHandle handle, EXEC_X_CONST void* pX,                        \
+                                           EXEC_W_CONST void* pW, void* pY)                                          \
+    {                                                                                                                \
+        const MmaHandle* m = handle_of(handle);                                                                      \
+        if (!m) return FFTLIB_ERR_NULL_POINTER;                                                                      \
+        if (m->variant != VARIANT) {                                                                                 \
+            set_error("handle was set up for another DFT variant");                                                  \
+            return FFTLIB_ERR_INVALID_VALUE;                                                                         \
+        }                                                                                                            \
+        return FFTLIB_FFT_fft_ixX_cxX_oxX_exec(handle, const_cast<void*>(pX), const_cast<void*>(pW), pY);            \
+    }
+
+FFTLIB_B200_DFT_VARIANT(dftSmall_ixX_cxX_oxX, INT_DFT_SMALL, , , )
+FFTLIB_B200_DFT_VARIANT(dftLarge_ixX_cxX_oxX, INT_DFT_LARGE, const, const, const)
+FFTLIB_B200_DFT_VARIANT(highRadixDecompositions_ixX_cxX_oxX, INT_HIGH_RADIX, , , )
+
+#undef FFTLIB_B200_DFT_VARIANT
 
 } // extern "C"

@@ -20,6 +20,11 @@ namespace {
 constexpr double kTablePi = 3.141592654;
 
 template <class T> struct IntT;
+template <> struct IntT<int8_t> {  // the LINALG multiply's INT8 data, int32 sums
+    using Acc = int32_t;
+    static constexpr int kBits = 8;
+    static constexpr uint32_t kMma = 64;
+};
 template <> struct IntT<int16_t> {
     using Acc = long long;
     static constexpr int kBits = 16;
@@ -82,7 +87,13 @@ __device__ __forceinline__ typename IntT<T>::Acc mul(T a, T b)
 }
 
 // acc + a b, exact: one 32 x 32 -> 64-bit multiply-add for INT16 data, a
-// 64-bit product added into the 128-bit sum for INT32.
+// 64-bit product added into the 128-bit sum for INT32. INT8 products are
+// summed in 32 bits, wrapping where the reference's int32 sum would overflow
+// (undefined behaviour in its C).
+__device__ __forceinline__ int32_t mac(int32_t acc, int8_t a, int8_t b)
+{
+    return (int32_t)((uint32_t)acc + (uint32_t)((int32_t)a * (int32_t)b));
+}
 __device__ __forceinline__ long long mac(long long acc, int16_t a, int16_t b)
 {
     long long d;
@@ -105,8 +116,10 @@ __device__ __forceinline__ __int128 mac(__int128 acc, int32_t a, int32_t b)
 // W load and one vector X load per 4 multiply-adds). In place when x == y
 // (a tile is read completely before it is written).
 constexpr uint32_t kGemmRows = 32;
+constexpr size_t kIntGemmMaxSmem = 200u * 1024u;
 
 template <class T> struct Vec4;
+template <> struct Vec4<int8_t> { using type = char4; };
 template <> struct Vec4<int16_t> { using type = short4; };
 template <> struct Vec4<int32_t> { using type = int4; };
 
@@ -153,6 +166,79 @@ __global__ void __launch_bounds__(256) k_int_gemm(const T* x, const T* __restric
             if (r + 3 < nr) yr[(size_t)(r + 3) * n2 + j] = shift_round<T>(a3, shift);
         }
     }
+}
+
+// ---- general matrix multiply: C = round_shift(A B) ---------------------------------
+
+// The LINALG multiply (..._matrixMatrixMultiply_ixX_ixX_oxX_cn.cpp:27-62) for
+// any M x K by K x N with row strides in elements. A CTA owns a 64 x 64 tile
+// of C and walks K in steps of 32: the A slice is stored transposed in shared
+// memory ([k][m]) so that four rows of one column k are one vector, the B
+// slice row by row; each of the 256 threads keeps the exact sums of a 4 x 4
+// block of C. Ragged edges are zero-filled on load and skipped on store.
+constexpr uint32_t kMmTile = 64, kMmK = 32, kMmPad = 4;
+
+template <class T>
+__global__ void __launch_bounds__(256) k_int_mm(const T* __restrict__ a, size_t lda, const T* __restrict__ b,
+                                                size_t ldb, T* __restrict__ c, size_t ldc, uint32_t M, uint32_t K,
+                                                uint32_t N, uint32_t shift)
+{
+    using V = typename Vec4<T>::type;
+    using Acc = typename IntT<T>::Acc;
+    __shared__ __align__(16) T as[kMmK][kMmTile + kMmPad];
+    __shared__ __align__(16) T bs[kMmK][kMmTile + kMmPad];
+    const uint32_t tx = threadIdx.x % 16u, ty = threadIdx.x / 16u;
+    const size_t m0 = (size_t)blockIdx.x * kMmTile;
+    const uint32_t n0 = blockIdx.y * kMmTile;
+    Acc acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+    for (uint32_t k0 = 0; k0 < K; k0 += kMmK) {
+        for (uint32_t e = threadIdx.x; e < kMmTile * kMmK; e += blockDim.x) {
+            const uint32_t r = e / kMmK, k = e % kMmK;  // A: consecutive threads along k
+            const size_t m = m0 + r;
+            as[k][r] = (m < M && k0 + k < K) ? a[m * lda + k0 + k] : (T)0;
+            const uint32_t kb = e / kMmTile, n = e % kMmTile;  // B: consecutive threads along n
+            bs[kb][n] = (k0 + kb < K && n0 + n < N) ? b[(size_t)(k0 + kb) * ldb + n0 + n] : (T)0;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (uint32_t k = 0; k < kMmK; ++k) {
+            const V av = *reinterpret_cast<const V*>(&as[k][4u * ty]);
+            const V bv = *reinterpret_cast<const V*>(&bs[k][4u * tx]);
+            const T ar[4] = {av.x, av.y, av.z, av.w}, br[4] = {bv.x, bv.y, bv.z, bv.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = mac(acc[i][j], ar[i], br[j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const size_t m = m0 + 4u * ty + i;
+        if (m >= M) break;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t n = n0 + 4u * tx + j;
+            if (n < N) c[m * ldc + n] = shift_round<T>(acc[i][j], shift);
+        }
+    }
+}
+
+template <class T>
+cudaError_t matmul_typed(uint32_t M, uint32_t K, uint32_t N, const void* a, size_t lda, const void* b, size_t ldb,
+                         void* c, size_t ldc, uint32_t shift, cudaStream_t s)
+{
+    if (M == 0 || N == 0) return cudaSuccess;
+    const uint64_t gx = ((uint64_t)M + kMmTile - 1) / kMmTile, gy = ((uint64_t)N + kMmTile - 1) / kMmTile;
+    if (gx > 0x7FFFFFFFull || gy > 65535ull) return cudaErrorInvalidValue;
+    k_int_mm<T><<<dim3((unsigned)gx, (unsigned)gy), 256, 0, s>>>(static_cast<const T*>(a), lda,
+                                                                 static_cast<const T*>(b), ldb, static_cast<T*>(c),
+                                                                 ldc, M, K, N, shift);
+    return cudaGetLastError();
 }
 
 // ---- highRadix -----------------------------------------------------------------
@@ -346,7 +432,7 @@ const void* device_w1(int bits, uint32_t n, cudaError_t* err)
 }
 
 template <class T>
-cudaError_t launch_typed(uint32_t n, uint32_t batch, uint32_t interleave, const uint32_t* shifts, void* xv,
+cudaError_t launch_typed(int v, uint32_t n, uint32_t batch, uint32_t interleave, const uint32_t* shifts, void* xv,
                          const void* wv, void* yv, cudaStream_t s)
 {
     constexpr int bits = IntT<T>::kBits;
@@ -354,10 +440,23 @@ cudaError_t launch_typed(uint32_t n, uint32_t batch, uint32_t interleave, const 
     T* x = static_cast<T*>(xv);
     T* y = static_cast<T*>(yv);
     const T* w = static_cast<const T*>(wv);
-    const int v = int_dft_variant(bits, n, batch, interleave);
     if (v == INT_DFT_SMALL || v == INT_DFT_LARGE) {
         const uint32_t n2 = 2u * n, ld = v == INT_DFT_SMALL ? MMA : n2;
-        const size_t smem = (size_t)(n2 * n2 + kGemmRows * n2) * sizeof(T);  // x tile 16-byte aligned: n2 is even
+        const size_t smem = ((size_t)n2 * n2 + kGemmRows * n2) * sizeof(T);  // x tile 16-byte aligned: n2 is even
+        if (smem > kIntGemmMaxSmem) {
+            // a table too large to stay in shared memory: the tiled multiply,
+            // whose CTAs read rows that others write, so in place goes
+            // through a temporary output
+            if (x != y) return matmul_typed<T>(batch, n2, n2, x, n2, w, ld, y, n2, shifts[0], s);
+            const size_t bytes = (size_t)batch * n2 * sizeof(T);
+            void* tmp = nullptr;
+            cudaError_t e = cudaMallocAsync(&tmp, bytes, s);
+            if (e != cudaSuccess) return e;
+            e = matmul_typed<T>(batch, n2, n2, x, n2, w, ld, tmp, n2, shifts[0], s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(y, tmp, bytes, cudaMemcpyDeviceToDevice, s);
+            const cudaError_t f = cudaFreeAsync(tmp, s);
+            return e != cudaSuccess ? e : f;
+        }
         if (smem > 48u * 1024u) {
             cudaError_t e = cudaFuncSetAttribute(k_int_gemm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
@@ -419,8 +518,13 @@ int int_dft_variant(int bits, uint32_t n, uint32_t batch, uint32_t interleave)
 
 uint32_t int_dft_w_size(int bits, uint32_t n, uint32_t batch, uint32_t interleave)
 {
+    return int_dft_w_size_v(bits, int_dft_variant(bits, n, batch, interleave), n);
+}
+
+uint32_t int_dft_w_size_v(int bits, int variant, uint32_t n)
+{
     const uint32_t mma = (uint32_t)int_mma_size(bits), r = mma / 2;
-    switch (int_dft_variant(bits, n, batch, interleave)) {
+    switch (variant) {
     case INT_DFT_SMALL: return mma * mma;
     case INT_DFT_LARGE: return 4u * n * n;
     default: {
@@ -450,14 +554,18 @@ bool int_high_radix_covered(int bits, uint32_t n)
 
 void int_dft_twgen_host(int bits, uint32_t n, uint32_t batch, uint32_t interleave, void* w)
 {
+    int_dft_twgen_host_v(bits, int_dft_variant(bits, n, batch, interleave), n, batch, interleave, w);
+}
+
+void int_dft_twgen_host_v(int bits, int v, uint32_t n, uint32_t batch, uint32_t interleave, void* w)
+{
     const uint32_t mma = (uint32_t)int_mma_size(bits), r = mma / 2;
-    const size_t total = int_dft_w_size(bits, n, batch, interleave);
-    auto set = [&](size_t i, int32_t v) {
-        if (bits == 16) put<int16_t>(w, i, v);
-        else put<int32_t>(w, i, v);
+    const size_t total = int_dft_w_size_v(bits, v, n);
+    auto set = [&](size_t i, int32_t val) {
+        if (bits == 16) put<int16_t>(w, i, val);
+        else put<int32_t>(w, i, val);
     };
     for (size_t i = 0; i < total; ++i) set(i, 0);
-    const int v = int_dft_variant(bits, n, batch, interleave);
     if (v == INT_DFT_SMALL) {
         // r/n block-diagonal copies of the 2n x 2n real embedding, row stride MMA
         // (planar: only the copies j < batch, as the reference generates them)
@@ -533,9 +641,37 @@ void int_dft_twgen_host(int bits, uint32_t n, uint32_t batch, uint32_t interleav
 cudaError_t int_dft_launch(int bits, uint32_t n, uint32_t batch, uint32_t interleave, const uint32_t* shifts,
                            void* x, const void* w, void* y, cudaStream_t s)
 {
+    return int_dft_launch_v(bits, int_dft_variant(bits, n, batch, interleave), n, batch, interleave, shifts, x, w, y,
+                            s);
+}
+
+cudaError_t int_dft_launch_v(int bits, int variant, uint32_t n, uint32_t batch, uint32_t interleave,
+                             const uint32_t* shifts, void* x, const void* w, void* y, cudaStream_t s)
+{
     if (batch == 0) return cudaSuccess;
-    return bits == 16 ? launch_typed<int16_t>(n, batch, interleave, shifts, x, w, y, s)
-                      : launch_typed<int32_t>(n, batch, interleave, shifts, x, w, y, s);
+    return bits == 16 ? launch_typed<int16_t>(variant, n, batch, interleave, shifts, x, w, y, s)
+                      : launch_typed<int32_t>(variant, n, batch, interleave, shifts, x, w, y, s);
+}
+
+void int_dft_w1_host(int bits, uint32_t n, void* out)
+{
+    std::vector<int32_t> w1;
+    fill_w1(bits, n, w1);
+    for (size_t i = 0; i < w1.size(); ++i) {
+        if (bits == 16) put<int16_t>(out, i, w1[i]);
+        else put<int32_t>(out, i, w1[i]);
+    }
+}
+
+cudaError_t int_matmul_launch(int bits, uint32_t M, uint32_t K, uint32_t N, const void* a, size_t lda, const void* b,
+                              size_t ldb, void* c, size_t ldc, uint32_t shift, cudaStream_t s)
+{
+    switch (bits) {
+    case 8: return matmul_typed<int8_t>(M, K, N, a, lda, b, ldb, c, ldc, shift, s);
+    case 16: return matmul_typed<int16_t>(M, K, N, a, lda, b, ldb, c, ldc, shift, s);
+    case 32: return matmul_typed<int32_t>(M, K, N, a, lda, b, ldb, c, ldc, shift, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 } // namespace fftb200

@@ -42,4 +42,23 @@ void int_dft_twgen_host(int bits, uint32_t n, uint32_t batch, uint32_t interleav
 cudaError_t int_dft_launch(int bits, uint32_t n, uint32_t batch, uint32_t interleave, const uint32_t* shifts,
                            void* x, const void* w, void* y, cudaStream_t s);
 
+// The same with the variant given (the public dftSmall / dftLarge /
+// highRadixDecompositions entry points): dftSmall needs n <= MMA/2,
+// dftLarge any n (its table is the dense 2n x 2n embedding; one that does
+// not fit in shared memory runs the tiled multiply, which needs x != y),
+// highRadix a covered length.
+uint32_t int_dft_w_size_v(int bits, int variant, uint32_t n);
+void int_dft_twgen_host_v(int bits, int variant, uint32_t n, uint32_t batch, uint32_t interleave, void* w);
+cudaError_t int_dft_launch_v(int bits, int variant, uint32_t n, uint32_t batch, uint32_t interleave,
+                             const uint32_t* shifts, void* x, const void* w, void* y, cudaStream_t s);
+// The highRadix internal table of n (MMA x MMA entries of the data type).
+void int_dft_w1_host(int bits, uint32_t n, void* out);
+
+// The LINALG matrix multiply C = round_shift(A B), A M x K, B K x N, C M x N,
+// row strides in elements, bits 8 (int32 sums), 16 (int64) or 32 (128-bit)
+// (src/linalg_c7xmma/FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX/..._cn.cpp:27-62).
+// C must not overlap A or B.
+cudaError_t int_matmul_launch(int bits, uint32_t M, uint32_t K, uint32_t N, const void* a, size_t lda, const void* b,
+                              size_t ldb, void* c, size_t ldc, uint32_t shift, cudaStream_t s);
+
 } // namespace fftb200

@@ -9,6 +9,8 @@
 #include "fftlib_b200/fft_c7x.h"
 #include "fftlib_b200/fft1d_c7x.h"
 #include "fftlib_b200/fft_c7xmma.h"
+#include "fftlib_b200/fft_c7xmma_variants.h"
+#include "fftlib_b200/linalg_c7xmma.h"
 #include "fftlib_b200/fftlib_b200_ext.h"
 
 #endif

@@ -87,6 +87,14 @@ typedef struct {
    uint32_t dim_x;     /* width in elements */
 } FFTLIB_bufParams1D_t;
 
+/* reference: src/common/FFTLIB_bufParams.h:69-78 */
+typedef struct {
+   uint32_t data_type; /* FFTLIB_data_type_e */
+   uint32_t dim_x;     /* width in elements */
+   uint32_t dim_y;     /* height in elements */
+   int32_t stride_y;   /* row stride in bytes */
+} FFTLIB_bufParams2D_t;
+
 /* Bytes per element of a FFTLIB_data_type_e value. */
 static inline int32_t FFTLIB_sizeof(uint32_t type)
 {

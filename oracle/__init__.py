@@ -445,8 +445,17 @@ def _mma_lib():
         L.orc_mma_twgen.argtypes = [C.c_int, _u32, _u32, _u32, _i32p]
         L.orc_mma_exec.argtypes = [C.c_int, _u32, _u32, _u32, _u32p, _i32p, _i32p, _i32p]
         L.orc_mma_w1.argtypes = [C.c_int, _u32, _i32p]
+        L.orc_mma_w_size_v.argtypes = [C.c_int, C.c_int, _u32]
+        L.orc_mma_w_size_v.restype = _u32
+        L.orc_mma_twgen_v.argtypes = [C.c_int, C.c_int, _u32, _u32, _u32, _i32p]
+        L.orc_mma_exec_v.argtypes = [C.c_int, C.c_int, _u32, _u32, _u32, _u32p, _i32p, _i32p, _i32p]
+        L.orc_linalg_mm.argtypes = [C.c_int, _u32, _u32, _u32, _i32p, C.c_uint64, _i32p, C.c_uint64, _i32p,
+                                    C.c_uint64, C.c_int32]
         L._mma_bound = True
     return L
+
+
+_INT_DT = {8: np.int8, 16: np.int16, 32: np.int32}
 
 
 def mma_variant(bits: int, n: int, batch: int, interleave: int) -> int:
@@ -454,10 +463,13 @@ def mma_variant(bits: int, n: int, batch: int, interleave: int) -> int:
     return _mma_lib().orc_mma_variant(bits, n, batch, interleave)
 
 
-def mma_twgen(bits: int, n: int, batch: int, interleave: int) -> np.ndarray:
+def mma_twgen(bits: int, n: int, batch: int, interleave: int, variant: int | None = None) -> np.ndarray:
+    """The caller's table of the coordinator (variant None: its rule) or of
+    one variant (1 dftSmall, 2 dftLarge, 3 highRadix)."""
     L = _mma_lib()
-    w = np.zeros(L.orc_mma_w_size(bits, n, batch, interleave), np.int32)
-    L.orc_mma_twgen(bits, n, batch, interleave, w)
+    v = mma_variant(bits, n, batch, interleave) if variant is None else variant
+    w = np.zeros(L.orc_mma_w_size_v(bits, v, n), np.int32)
+    L.orc_mma_twgen_v(bits, v, n, batch, interleave, w)
     return w.astype(np.int16 if bits == 16 else np.int32)
 
 
@@ -474,15 +486,16 @@ def ref_mma_available() -> bool:
     return os.path.exists(os.path.join(REF_DIR, "libref_mma.so"))
 
 
-def ref_mma_exec(bits: int, n: int, batch: int, interleave: int, shifts, x, w=None) -> np.ndarray:
+def ref_mma_exec(bits: int, n: int, batch: int, interleave: int, shifts, x, w=None,
+                 variant: int | None = None) -> np.ndarray:
     """The reference's natural-C integer DFT (dftSmall / LINALG / highRadix
     _cn) through oracle/mma_ref_driver.cpp, with this oracle's tables."""
     dt = np.int16 if bits == 16 else np.int32
+    v = mma_variant(bits, n, batch, interleave) if variant is None else variant
     if w is None:
-        w = mma_twgen(bits, n, batch, interleave)
+        w = mma_twgen(bits, n, batch, interleave, v)
     sh = np.zeros(5, np.uint32)
     sh[: len(shifts)] = shifts
-    v = mma_variant(bits, n, batch, interleave)
     xin = np.ascontiguousarray(x, dt).copy()
     y = np.zeros(2 * n * batch, dt)
     w1 = mma_w1(bits, n)
@@ -494,18 +507,51 @@ def ref_mma_exec(bits: int, n: int, batch: int, interleave: int, shifts, x, w=No
     return y
 
 
-def mma_exec(bits: int, n: int, batch: int, interleave: int, shifts, x, w=None) -> np.ndarray:
+def mma_exec(bits: int, n: int, batch: int, interleave: int, shifts, x, w=None,
+             variant: int | None = None) -> np.ndarray:
     L = _mma_lib()
+    v = mma_variant(bits, n, batch, interleave) if variant is None else variant
     if w is None:
-        w = mma_twgen(bits, n, batch, interleave)
+        w = mma_twgen(bits, n, batch, interleave, v)
     sh = np.zeros(5, np.uint32)
     sh[: len(shifts)] = shifts
     y = np.zeros(2 * n * batch, np.int32)
-    rc = L.orc_mma_exec(bits, n, batch, interleave, sh, np.ascontiguousarray(w, np.int32),
-                        np.ascontiguousarray(x, np.int32), y)
+    rc = L.orc_mma_exec_v(bits, v, n, batch, interleave, sh, np.ascontiguousarray(w, np.int32),
+                          np.ascontiguousarray(x, np.int32), y)
     if rc:
         raise ValueError(f"oracle integer DFT does not cover N={n}")
     return y.astype(np.int16 if bits == 16 else np.int32)
+
+
+def linalg_mm(bits: int, a: np.ndarray, b: np.ndarray, shift: int, c_shape=None, ldc=None) -> np.ndarray:
+    """The LINALG multiply C = shiftAndRound(A B, shift) (oracle/mma_int_oracle.c).
+    a, b: 2-D arrays whose row strides (in elements, from their strides) may
+    exceed their widths. Returns C as a dense M x N array of the data type."""
+    L = _mma_lib()
+    M, K = a.shape
+    K2, N = b.shape
+    assert K == K2
+    a32 = np.ascontiguousarray(a, np.int32)
+    b32 = np.ascontiguousarray(b, np.int32)
+    c = np.zeros((M, N), np.int32)
+    L.orc_linalg_mm(bits, M, K, N, a32, max(K, 1), b32, max(N, 1), c, max(N, 1), int(shift))
+    return c.astype(_INT_DT[bits])
+
+
+def ref_linalg_mm(bits: int, a: np.ndarray, b: np.ndarray, shift: int) -> np.ndarray:
+    """The reference's own LINALG _cn (oracle/_ref/libref_mma.so)."""
+    dt = _INT_DT[bits]
+    M, K = a.shape
+    N = b.shape[1]
+    A = np.ascontiguousarray(a, dt)
+    B = np.ascontiguousarray(b, dt)
+    Cm = np.zeros((M, N), dt)
+    L = ref_lib("mma")
+    rc = L.ref_linalg_exec(C.c_int(bits), C.c_int32(M), C.c_int32(K), C.c_int32(N), _vp(A), C.c_int32(max(K, 1)),
+                           _vp(B), C.c_int32(max(N, 1)), _vp(Cm), C.c_int32(max(N, 1)), C.c_int32(shift))
+    if rc:
+        raise ValueError(f"reference LINALG returned {rc}")
+    return Cm
 
 
 # --------------------------------------------------------------------------

@@ -17,7 +17,8 @@
  *                    576-594, 643-661 (shiftAndRound), 672-722 (table entries)
  *   dftSmall         .../FFTLIB_FFT_dftSmall_ixX_cxX_oxX_cn.cpp:18-46; getSizes/twGen
  *                    .../c71/FFTLIB_FFT_dftSmall_ixX_cxX_oxX_ci.cpp:74-212
- *   dftLarge         src/linalg_c7xmma/FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX/..._cn.cpp:27-62;
+ *   dftLarge and the LINALG matrix multiply (INT8 too)
+ *                    src/linalg_c7xmma/FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX/..._cn.cpp:27-62;
  *                    getSizes/twGen .../c71/FFTLIB_FFT_dftLarge_ixX_cxX_oxX_ci.cpp:43-156
  *   highRadix        .../FFTLIB_FFT_highRadixDecompositions_ixX_cxX_oxX_cn.cpp:20-455;
  *                    getSizes/twGen .../c71/..._ci.cpp:1975-2168
@@ -33,7 +34,11 @@ typedef __int128 i128;
 static const double MMA_PI = 3.141592654;
 
 static int mma_size(int bits) { return bits == 16 ? 32 : 16; }
-static int64_t mma_max(int bits) { return bits == 16 ? 32767 : 2147483647; }
+static int64_t mma_max(int bits) { return ((int64_t)1 << (bits - 1)) - 1; }
+
+/* Arithmetic right shift of the exact sum; counts past its width give the
+ * sign (the reference's shift of its accumulator is undefined there). */
+static i128 mma_sra(i128 x, uint32_t k) { return k >= 127u ? (x < 0 ? -1 : 0) : x >> k; }
 
 /* Saturate to the data type. The reference's 128-bit saturation
  * (FFTLIB_utility.h:546-566) tests only the low 64 bits of a non-negative
@@ -56,7 +61,7 @@ static int32_t mma_shift_round(i128 x, uint32_t shift, int bits)
 {
     const uint32_t s = shift & 0xFFu;
     if (s == 0) return mma_sat(x, bits);
-    return mma_sat(((x >> (s - 1)) + 1) >> 1, bits);
+    return mma_sat(mma_sra(mma_sra(x, s - 1) + 1, 1), bits);
 }
 
 /* Negation that maps the most negative value to the most positive. */
@@ -98,11 +103,11 @@ static uint32_t stage0_factor(uint32_t fftSize, uint32_t r)
     return f;
 }
 
-/* Caller's table size (elements), as getSizes reports it. */
-uint32_t orc_mma_w_size(int bits, uint32_t fftSize, uint32_t batchSize, uint32_t interleave)
+/* Caller's table size (elements) of a variant, as its getSizes reports it. */
+uint32_t orc_mma_w_size_v(int bits, int variant, uint32_t fftSize)
 {
     const uint32_t mma = (uint32_t)mma_size(bits), r = mma / 2;
-    switch (orc_mma_variant(bits, fftSize, batchSize, interleave)) {
+    switch (variant) {
     case 1: return mma * mma;
     case 2: return 4u * fftSize * fftSize;
     default: {
@@ -117,13 +122,17 @@ uint32_t orc_mma_w_size(int bits, uint32_t fftSize, uint32_t batchSize, uint32_t
     }
 }
 
-/* The caller's table (twGen), int values in int32 slots. */
-void orc_mma_twgen(int bits, uint32_t fftSize, uint32_t batchSize, uint32_t interleave, int32_t *W)
+uint32_t orc_mma_w_size(int bits, uint32_t fftSize, uint32_t batchSize, uint32_t interleave)
+{
+    return orc_mma_w_size_v(bits, orc_mma_variant(bits, fftSize, batchSize, interleave), fftSize);
+}
+
+/* The caller's table (twGen) of a variant, int values in int32 slots. */
+void orc_mma_twgen_v(int bits, int v, uint32_t fftSize, uint32_t batchSize, uint32_t interleave, int32_t *W)
 {
     const uint32_t mma = (uint32_t)mma_size(bits), r = mma / 2;
     const uint32_t n = fftSize;
-    const int v = orc_mma_variant(bits, fftSize, batchSize, interleave);
-    memset(W, 0, sizeof(int32_t) * orc_mma_w_size(bits, fftSize, batchSize, interleave));
+    memset(W, 0, sizeof(int32_t) * orc_mma_w_size_v(bits, v, fftSize));
     if (v == 1) {
         /* block-diagonal copies of the 2N x 2N real embedding, row stride MMA */
         const uint32_t copies = r / n;
@@ -277,18 +286,23 @@ void orc_mma_w1(int bits, uint32_t fftSize, int32_t *W1)
         }
 }
 
-/* Returns 0 on success, 1 for a length the decomposition does not cover. */
-int orc_mma_exec(int bits, uint32_t fftSize, uint32_t batchSize, uint32_t interleave, const uint32_t *shifts,
-                 const int32_t *W, const int32_t *x, int32_t *y)
+void orc_mma_twgen(int bits, uint32_t fftSize, uint32_t batchSize, uint32_t interleave, int32_t *W)
+{
+    orc_mma_twgen_v(bits, orc_mma_variant(bits, fftSize, batchSize, interleave), fftSize, batchSize, interleave, W);
+}
+
+/* One variant's transform. Returns 0 on success, 1 for a length the
+ * decomposition does not cover. */
+int orc_mma_exec_v(int bits, int v, uint32_t fftSize, uint32_t batchSize, uint32_t interleave,
+                   const uint32_t *shifts, const int32_t *W, const int32_t *x, int32_t *y)
 {
     const uint32_t mma = (uint32_t)mma_size(bits), r = mma / 2, n = fftSize;
-    const int v = orc_mma_variant(bits, fftSize, batchSize, interleave);
     if (v == 1) {
         mma_gemm(bits, 2u * n, batchSize, mma, shifts[0], W, x, y);
         return 0;
     }
     if (v == 2) {
-        mma_gemm(bits, 2u * n, batchSize, 2u * n, shifts[(0)], W, x, y);
+        mma_gemm(bits, 2u * n, batchSize, 2u * n, shifts[0], W, x, y);
         return 0;
     }
     if (n < 2u * mma) return 1;
@@ -362,4 +376,32 @@ int orc_mma_exec(int bits, uint32_t fftSize, uint32_t batchSize, uint32_t interl
     free(re2);
     free(im2);
     return 0;
+}
+
+int orc_mma_exec(int bits, uint32_t fftSize, uint32_t batchSize, uint32_t interleave, const uint32_t *shifts,
+                 const int32_t *W, const int32_t *x, int32_t *y)
+{
+    return orc_mma_exec_v(bits, orc_mma_variant(bits, fftSize, batchSize, interleave), fftSize, batchSize, interleave,
+                          shifts, W, x, y);
+}
+
+/* The LINALG matrix multiply (src/linalg_c7xmma/FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX/
+ * ..._cn.cpp:27-62): C[m][n] = shiftAndRound(sum_k A[m][k] B[k][n], shift) for
+ * bits = 8, 16 or 32, row strides in elements, values in int32 slots. The
+ * shift is the InitArgs int8_t, passed on as the uint8_t of shiftAndRound.
+ * INT8 sums are kept in 32 bits with two's-complement wrap (the reference's
+ * int32 accumulator; its overflow is undefined in C). */
+void orc_linalg_mm(int bits, uint32_t M, uint32_t K, uint32_t N, const int32_t *A, uint64_t lda, const int32_t *B,
+                   uint64_t ldb, int32_t *Cm, uint64_t ldc, int32_t shift)
+{
+    const uint32_t s = (uint32_t)(uint8_t)(int8_t)shift;
+    for (uint32_t m = 0; m < M; ++m)
+        for (uint32_t n = 0; n < N; ++n) {
+            i128 acc = 0;
+            for (uint32_t k = 0; k < K; ++k) {
+                acc += (i128)((int64_t)A[m * lda + k] * (int64_t)B[k * ldb + n]);
+                if (bits == 8) acc = (i128)(int32_t)(uint32_t)(uint64_t)acc;
+            }
+            Cm[m * ldc + n] = mma_shift_round(acc, s, bits);
+        }
 }

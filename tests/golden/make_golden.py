@@ -296,8 +296,11 @@ MMA_ROW_RE = re.compile(r"\{STATIC,\s*staticRefInput(\d+),\s*staticRefOut\d+,\s*
                         r"FFTLIB_INT(16|32),\s*(\d+),\s*(\d+),\s*(\d+),")
 
 
-def mma_int_static(ref):
-    path = os.path.join(ref, "test", "fft_c7xmma", "FFTLIB_FFT_fft_ixX_cxX_oxX", "FFTLIB_FFT_fft_ixX_cxX_oxX_idat.c")
+def mma_int_static(ref, kernel="FFTLIB_FFT_fft_ixX_cxX_oxX", max_points=None):
+    """The reference test's committed integer in/out vectors and shift vectors of
+    the coordinator (or of one variant, `kernel`); cases with more than
+    `max_points` complex points in total are left out to keep the fixture small."""
+    path = os.path.join(ref, "test", "fft_c7xmma", kernel, kernel + "_idat.c")
     with open(path) as f:
         text = f.read()
     arr = {name: np.array([int(v, 0) for v in re.findall(r"-?0x[0-9a-fA-F]+|-?\d+", body)], np.int64)
@@ -305,6 +308,8 @@ def mma_int_static(ref):
     d, ids = {}, []
     for cid, bits, batch, n, il in MMA_ROW_RE.findall(text):
         cid, bits = int(cid), int(bits)
+        if max_points is not None and int(batch) * int(n) > max_points:
+            continue
         dt = np.int16 if bits == 16 else np.int32
         ids.append(cid)
         d[f"meta_{cid}"] = np.array([bits, int(batch), int(n), int(il)])
@@ -333,6 +338,10 @@ def main():
         "fft1d_i16_pymodel": lambda: fft1d_i16_pymodel(a.ref),
         "fft1d_c2c_pymodel": lambda: fft1d_c2c_pymodel(a.ref),
         "mma_int_static": lambda: mma_int_static(a.ref),
+        "mma_dft_small_static": lambda: mma_int_static(a.ref, "FFTLIB_FFT_dftSmall_ixX_cxX_oxX"),
+        "mma_dft_large_static": lambda: mma_int_static(a.ref, "FFTLIB_FFT_dftLarge_ixX_cxX_oxX"),
+        "mma_high_radix_static": lambda: mma_int_static(a.ref, "FFTLIB_FFT_highRadixDecompositions_ixX_cxX_oxX",
+                                                        max_points=4096),
     }
     only = [s for s in a.only.split(",") if s]
     for name, make in makers.items():

@@ -23,9 +23,12 @@ def declared_functions():
     for h in glob.glob(os.path.join(ROOT, "include", "**", "*.h"), recursive=True):
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        for m in re.finditer(r"^\s*(?:FFTLIB_STATUS|void|int|const char \*)\s*\**\s*(\w+)\s*\(", text, re.M):
+        for m in re.finditer(r"^\s*(?:FFTLIB_STATUS|void|int32_t|uint32_t|int|const char \*)\s+\**\s*(\w+)\s*\(",
+                             text, re.M):
             if m.group(1) != "FFTLIB_sizeof":
                 names.add(m.group(1))
+        for m in re.finditer(r"^\s*extern\s+\w+\s+(\w+)\s*\[", text, re.M):
+            names.add(m.group(1))
     return sorted(names)
 
 
