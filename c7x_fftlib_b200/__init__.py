@@ -243,6 +243,11 @@ def lib() -> C.CDLL:
     for fn in ("tw_gen_r2c", "split_factor_gen_r2c", "ifft_c2r_tw_gen", "ifft_c2r_split_factor_gen"):
         getattr(L, fn).argtypes = [_vp, C.c_int32]
         getattr(L, fn).restype = None
+        getattr(L, "FFTLIB_b200_" + fn + "_device").argtypes = [_vp, C.c_int32, _vp]
+        getattr(L, "FFTLIB_b200_" + fn + "_device").restype = C.c_int
+    for fn in ("tw_gen_c2c_device", "tw_gen_i16_device"):
+        getattr(L, "FFTLIB_b200_" + fn).argtypes = [_vp, _u32, _vp]
+        getattr(L, "FFTLIB_b200_" + fn).restype = C.c_int
     _lib = L
     return L
 

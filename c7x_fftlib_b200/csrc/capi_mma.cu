@@ -19,6 +19,7 @@
 #include "fft_c7xmma_variants.h"
 #include "fftlib_b200_ext.h"
 #include "plan.h"
+#include "tables.h"
 #include "tc_dft.h"
 
 using namespace fftb200;
@@ -123,6 +124,27 @@ cudaError_t enqueue(const MmaHandle* m, const float* x, const float* w, float* y
                    batch, false, s);
 }
 
+// The caller's integer table of `elems` entries: host memory from the host
+// generator; device memory from the device generator for the dense dftLarge
+// matrix (4 n^2 entries), else from the host one and one copy.
+FFTLIB_STATUS int_tw_gen(int bits, int variant, uint32_t n, uint32_t batch, uint32_t il, void* pW, uint32_t elems)
+{
+    if (!is_device_ptr(pW)) {
+        int_dft_twgen_host_v(bits, variant, n, batch, il, pW);
+        return FFTLIB_SUCCESS;
+    }
+    cudaError_t e;
+    if (variant == INT_DFT_LARGE) {
+        e = dft_large_matrix_device(pW, bits, n, il, cudaStreamPerThread);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
+        return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen");
+    }
+    std::vector<unsigned char> tmp((size_t)elems * (bits / 8));
+    int_dft_twgen_host_v(bits, variant, n, batch, il, tmp.data());
+    e = cudaMemcpy(pW, tmp.data(), tmp.size(), cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen copy");
+}
+
 } // namespace
 
 extern "C" {
@@ -161,15 +183,7 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_twGen(const FFTLIB_FFT_fft_ixX_cxX_oxX_
             set_error("bufParamsW->dim_x %u, expected %u", bufParamsW->dim_x, w);
             return FFTLIB_ERR_INVALID_DIMENSION;
         }
-        const size_t bytes = (size_t)w * (bits / 8);
-        if (!is_device_ptr(pW)) {
-            int_dft_twgen_host(bits, n, b, il, pW);
-            return FFTLIB_SUCCESS;
-        }
-        std::vector<unsigned char> tmp(bytes);
-        int_dft_twgen_host(bits, n, b, il, tmp.data());
-        const cudaError_t e = cudaMemcpy(pW, tmp.data(), bytes, cudaMemcpyHostToDevice);
-        return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen copy");
+        return int_tw_gen(bits, int_dft_variant(bits, n, b, il), n, b, il, pW, w);
     }
     if (bufParamsW->data_type != FFTLIB_FLOAT32) return unsupported_type(bufParamsW->data_type);
     uint32_t x, w, y;
@@ -195,11 +209,9 @@ FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_twGen(const FFTLIB_FFT_fft_ixX_cxX_oxX_
         FFTLIB_b200_tw_gen_c2c(out, n);
         return FFTLIB_SUCCESS;
     }
-    float* tmp = new float[2u * (size_t)n];
-    FFTLIB_b200_tw_gen_c2c(tmp, n);
-    cudaError_t e = cudaMemcpy(out, tmp, 2u * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
-    delete[] tmp;
-    return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen copy");
+    cudaError_t e = stage_twiddles_device(out, n, false, cudaStreamPerThread);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
+    return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen");
 }
 
 FFTLIB_STATUS FFTLIB_FFT_fft_ixX_cxX_oxX_init_checkParams(FFTLIB_kernelHandle handle,
@@ -431,15 +443,7 @@ FFTLIB_STATUS variant_tw_gen(int variant, const FFTLIB_FFT_fft_ixX_cxX_oxX_InitA
         set_error("bufParamsW->dim_x %u, expected %u", bw->dim_x, w);
         return FFTLIB_ERR_INVALID_DIMENSION;
     }
-    const int bits = int_bits(bw->data_type);
-    if (!is_device_ptr(pW)) {
-        int_dft_twgen_host_v(bits, variant, a.fftSize, a.batchSize, a.interleave, pW);
-        return FFTLIB_SUCCESS;
-    }
-    std::vector<unsigned char> tmp((size_t)w * (bits / 8));
-    int_dft_twgen_host_v(bits, variant, a.fftSize, a.batchSize, a.interleave, tmp.data());
-    const cudaError_t e = cudaMemcpy(pW, tmp.data(), tmp.size(), cudaMemcpyHostToDevice);
-    return e == cudaSuccess ? FFTLIB_SUCCESS : cuda_fail(e, "twGen copy");
+    return int_tw_gen(int_bits(bw->data_type), variant, a.fftSize, a.batchSize, a.interleave, pW, w);
 }
 
 FFTLIB_STATUS variant_check(int variant, FFTLIB_kernelHandle handle, const FFTLIB_bufParams1D_t* bx,

@@ -108,6 +108,25 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_destroy(FFTLIB_b200_mixedHandle handle);
 void FFTLIB_b200_tw_gen_c2c(FFTLIB_F32 *pW, uint32_t numPoints);
 void FFTLIB_b200_tw_gen_i16(int16_t *pW, uint32_t numPoints);
 
+/* The same generators on the GPU, for callers that keep no host copy of the
+ * tables: the reference's formulas with pi truncated to 3.141592654 and the
+ * same order of double operations, so the tables are bit-identical to the
+ * host generators' (FFTLIB_b200_tw_gen_c2c / _i16 above; tw_gen_r2c,
+ * split_factor_gen_r2c, ifft_c2r_tw_gen, ifft_c2r_split_factor_gen of
+ * fft_c7x.h). The buffer is device memory of the host generator's size;
+ * entries the host generator leaves unwritten are left unwritten. Enqueued
+ * on `stream` (a cudaStream_t). FFTLIB_ERR_INVALID_VALUE for host memory,
+ * FFTLIB_ERR_INVALID_DIMENSION for a negative numPoints, and for a Q15
+ * numPoints that is not a power of two (the int16 kernel's lengths; for
+ * others the host generator's stage blocks overlap and its table depends on
+ * its write order). */
+FFTLIB_STATUS FFTLIB_b200_tw_gen_c2c_device(FFTLIB_F32 *pW, uint32_t numPoints, void *stream);
+FFTLIB_STATUS FFTLIB_b200_tw_gen_i16_device(int16_t *pW, uint32_t numPoints, void *stream);
+FFTLIB_STATUS FFTLIB_b200_tw_gen_r2c_device(FFTLIB_F32 *pW, int32_t numPoints, void *stream);
+FFTLIB_STATUS FFTLIB_b200_split_factor_gen_r2c_device(FFTLIB_F32 *pSFactor, int32_t numPoints, void *stream);
+FFTLIB_STATUS FFTLIB_b200_ifft_c2r_tw_gen_device(FFTLIB_F32 *pW, int32_t numPoints, void *stream);
+FFTLIB_STATUS FFTLIB_b200_ifft_c2r_split_factor_gen_device(FFTLIB_F32 *pSFactor, int32_t numPoints, void *stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

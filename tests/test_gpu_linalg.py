@@ -42,7 +42,9 @@ def test_bit_exact_device(torch_cuda, bits, m, k, n):
         a, b = _mats(bits, m, k, n, 7 * m + k + n + bits, full)
         for sh in (0, 1, bits - 1, bits + 3):
             mm = F.MatMul(m, k, n, DT[bits], shift=sh)
-            A, B = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+            # an empty A or B (k = 0) still needs a non-NULL buffer, as in the reference
+            A = torch.from_numpy(a).cuda() if a.size else torch.zeros(1, dtype=torch.from_numpy(a).dtype).cuda()
+            B = torch.from_numpy(b).cuda() if b.size else torch.zeros(1, dtype=A.dtype).cuda()
             Cd = torch.zeros((m, n), dtype=A.dtype, device="cuda")
             mm.exec(A, B, Cd)
             want = O.linalg_mm(bits, a, b, sh)
