@@ -434,6 +434,7 @@ def secondary_configs(args):
     res["tc_dft"] = tc_dft_configs(args, steps)
     res["fft1d_single"] = fft1d_single_configs(steps)
     res["int_dft"] = int_dft_configs(steps)
+    res["linalg"] = linalg_configs(steps)
     return res
 
 
@@ -489,6 +490,54 @@ def int_dft_configs(steps):
             entry["speedup_vs_ref_cn"] = round(entry["rows_per_s"] / entry["ref_cn_rows_per_s"], 1)
         out[f"int{bits}_n{n}"] = entry
         del x, x0, y
+    return out
+
+
+def linalg_configs(steps):
+    """The integer matrix multiply FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX
+    (bit-exact with the reference's natural C) on device buffers through
+    execAsync: a square 4096^3 product and the DFT-shaped 2^20 x 64 x 64, for
+    INT8, INT16 and INT32. MAC/s counts the M K N multiply-adds; bytes: A, B
+    and C once. ref_cn: the reference's natural C on one host core over the
+    first 16 rows of A."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import c7x_fftlib_b200 as F
+    import oracle as O
+
+    stream = torch.cuda.Stream()
+    sp = F.ptr(stream.cuda_stream)
+    out = {}
+    types = {8: (F.FFTLIB_INT8, torch.int8), 16: (F.FFTLIB_INT16, torch.int16), 32: (F.FFTLIB_INT32, torch.int32)}
+    for bits in (8, 16, 32):
+        dt, tdt = types[bits]
+        lim = (1 << (bits - 1)) - 1
+        for m, k, n in ((4096, 4096, 4096), (1 << 20, 64, 64)):
+            a = torch.randint(-lim, lim, (m, k), dtype=torch.int64, device="cuda").to(tdt)
+            b = torch.randint(-lim, lim, (k, n), dtype=torch.int64, device="cuda").to(tdt)
+            c = torch.empty((m, n), dtype=tdt, device="cuda")
+            shift = 2 * bits - 1
+            mm = F.MatMul(m, k, n, dt, shift=shift)
+            ms = _time_launches(torch, stream, lambda: mm.exec_async(a, b, c, sp), max(steps, 5))
+            torch.cuda.synchronize()
+            rs = 16
+            a_s, b_h = a[:rs].cpu().numpy(), b.cpu().numpy()
+            exact = bool(np.array_equal(c[:rs].cpu().numpy(), O.linalg_mm(bits, a_s, b_h, shift)))
+            entry = {"m": m, "k": k, "n": n, "ms": round(ms, 4),
+                     "TMACps": round(m * k * n / ms / 1e9, 3),
+                     "GBps": round((m * k + k * n + m * n) * (bits // 8) / ms / 1e6, 1),
+                     "bit_exact_sample": exact}
+            if O.ref_mma_available():
+                t0 = time.perf_counter()
+                O.ref_linalg_mm(bits, a_s, b_h, shift)
+                t_ref = time.perf_counter() - t0
+                entry["ref_cn_TMACps_1core"] = round(rs * k * n / t_ref / 1e12, 6)
+                entry["speedup_vs_ref_cn"] = round(entry["TMACps"] / entry["ref_cn_TMACps_1core"], 1)
+            out[f"int{bits}_{m}x{k}x{n}"] = entry
+            del a, b, c
     return out
 
 
