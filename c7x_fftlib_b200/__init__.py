@@ -236,6 +236,8 @@ def lib() -> C.CDLL:
     L.FFTLIB_b200_FFT_fft_execAsync.restype = C.c_int
     L.FFTLIB_b200_FFT_fft_sync.argtypes = [_vp]
     L.FFTLIB_b200_FFT_fft_sync.restype = C.c_int
+    L.FFTLIB_b200_FFT_setIntTensorCores.argtypes = [C.c_int32]
+    L.FFTLIB_b200_FFT_setIntTensorCores.restype = None
     L.FFTLIB_b200_FFT_fft_path.argtypes = [_vp]
     L.FFTLIB_b200_FFT_fft_path.restype = C.c_int32
     L.FFTLIB_b200_tw_gen_c2c.argtypes = [_vp, _u32]

@@ -365,6 +365,8 @@ int32_t FFTLIB_b200_FFT_fft_path(FFTLIB_kernelHandle handle)
 
 uint8_t FFTLIB_FFT_twData[32 * 32 * 3 * sizeof(int16_t)];
 
+void FFTLIB_b200_FFT_setIntTensorCores(int32_t enable) { int_set_tensor_cores(enable != 0); }
+
 } // extern "C"
 
 // ---- the variants on their own (fft_c7xmma_variants.h) ----------------------------

@@ -54,6 +54,16 @@ cudaError_t int_dft_launch_v(int bits, int variant, uint32_t n, uint32_t batch, 
 // The highRadix internal table of n (MMA x MMA entries of the data type).
 void int_dft_w1_host(int bits, uint32_t n, void* out);
 
+// The INT16 dftSmall / dftLarge product on the tensor cores (dft_int_tc.cu):
+// rows of n2 = 2N values, n2 dividing 128; x 8-byte aligned.
+bool int16_tc_supported(uint32_t n2, const void* x, const void* y);
+cudaError_t launch_int16_tc(const int16_t* x, int16_t* y, const int16_t* w, uint32_t n2, uint32_t ld, uint32_t rows,
+                            uint32_t shift, cudaStream_t s);
+// Whether the INT16 products use the tensor cores when they can (default
+// on; the CUDA-core kernel gives the same bits).
+void int_set_tensor_cores(bool on);
+bool int_tensor_cores();
+
 // The LINALG matrix multiply C = round_shift(A B), A M x K, B K x N, C M x N,
 // row strides in elements, bits 8 (int32 sums), 16 (int64) or 32 (128-bit)
 // (src/linalg_c7xmma/FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX/..._cn.cpp:27-62).

@@ -1,0 +1,370 @@
+// dft_int_tc.cu -- the INT16 dftSmall / dftLarge product Y = round_shift(X W)
+// on the tensor cores (tcgen05.mma kind::i8), bit-exact with the reference's
+// natural C (src/fft_c7xmma/FFTLIB_FFT_dftSmall_ixX_cxX_oxX/..._cn.cpp:18-46,
+// src/linalg_c7xmma/FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX/..._cn.cpp:27-62).
+//
+// Exactness. Every INT16 value v is taken in offset binary, v' = v + 32768 =
+// 256 h + l with bytes h, l in [0, 255], so each product of two values is four
+// u8 x u8 products, summed exactly in the tensor core's 32-bit accumulators:
+//   hh = sum h_x h_w,  mid = sum (h_x l_w + l_x h_w),  ll = sum l_x l_w
+//   sum x w = 2^16 hh + 2^8 mid + ll - 2^15 (sum x' + sum w') + K 2^30,
+// evaluated in 64 bits by the epilogue (K = 128, the products' length); the
+// sums are below 2^24, far from the accumulators' range.
+//
+// Layout (the FP32 one-stage kernel's, tc_dft_small.cuh). Rows of 128 INT16
+// values (a "super-row": 128 / 2N consecutive transforms) are multiplied by a
+// 128 x 128 block-diagonal matrix, 128 / 2N copies of the 2N x 2N table; the
+// matrix is the A operand (M = 128 output values) and 64 super-rows the B
+// operand (N = 64), so a warp of the epilogue writes 32 consecutive outputs of
+// a super-row with one store. The zero entries of the block-diagonal matrix
+// are offset like the others, which the correction term accounts for.
+//
+// Roles per CTA (one persistent CTA per SM): 8 loader warps (HBM -> offset
+// bytes -> swizzled K-major shared memory, and the super-row sums), 8
+// epilogue warps (three accumulators -> 64-bit combination -> shift, round,
+// saturate -> HBM) and one warp that allocates tensor memory and issues the
+// 16 MMAs of a tile. Four operand buffers in shared memory and two
+// accumulator buffers in tensor memory (3 x 64 columns each); the next tile
+// of the CTA is prefetched into L2. Every wait is bounded and a wait that
+// gives up sets kErrTcTimeout in the launch's error word.
+#include <mutex>
+
+#include "dft_int.h"
+#include "int_arith.cuh"
+#include "plan.h"
+#include "tc_dft.cuh"
+
+namespace fftb200 {
+
+namespace {
+
+struct IntTc {
+    static constexpr int TS = 64;  // super-rows per tile = MMA N
+    static constexpr int NB = 4;   // operand tile buffers (shared memory)
+    static constexpr int NA = 2;   // accumulator buffers (tensor memory)
+    static constexpr int RS = 8;   // super-row sum slots: a slot is rewritten NB + NA tiles after its epilogue
+    static constexpr int LW = 8, EW = 8;
+    static constexpr int MMA_WARP = LW + EW;
+    static constexpr int THREADS = 32 * (MMA_WARP + 1);
+    static constexpr int RPW = TS / LW;  // super-rows per loader warp per tile
+    // 128-byte K-major rows (KMajor counts 16-bit units: 64 of them)
+    using LA = KMajor<128, 64>;  // matrix limb: 128 output values x 128 input values
+    using LB = KMajor<TS, 64>;   // data limb: TS super-rows x 128 input values
+    static constexpr uint32_t W_LIMB = LA::BYTES;  // 16 KB
+    static constexpr uint32_t X_LIMB = LB::BYTES;  // 8 KB
+    static constexpr uint32_t TILE = 2 * X_LIMB;
+    static constexpr uint32_t OFF_W = NB * TILE;
+    static constexpr uint32_t OFF_CS = OFF_W + 2 * W_LIMB;  // 128 column sums of the offset matrix
+    static constexpr uint32_t OFF_RS = OFF_CS + 4u * 128u;  // RS x TS super-row sums
+    static constexpr uint32_t OFF_BAR = (OFF_RS + 4u * RS * TS + 7u) & ~7u;
+    static constexpr int NBARS = 2 * NB + 2 * NA + 1;
+    static constexpr uint32_t OFF_MISC = OFF_BAR + 8u * NBARS;
+    static constexpr uint32_t SMEM = OFF_MISC + 16u + 1024u;
+    static constexpr uint32_t ACC = 3 * TS;  // hh, mid, ll columns of one buffer
+    static constexpr uint32_t TMEM_COLS = 512;
+    // A_FULL/S_FREE per operand buffer, D_FULL/D_FREE per accumulator buffer
+    static constexpr int A_FULL = 0, S_FREE = NB, D_FULL = 2 * NB, D_FREE = 2 * NB + NA, DRAIN = 2 * NB + 2 * NA;
+    static_assert(NA * ACC <= TMEM_COLS, "tensor memory");
+    static_assert(RS >= NB + NA, "super-row sum slots");
+    static_assert(SMEM <= 227u * 1024u, "shared memory per CTA");
+};
+
+// Instruction descriptor: S32 accumulator, unsigned 8-bit A and B, both
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t umma_idesc_u8(int n)
+{
+    return (2u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+// D (+)= A . B, unsigned 8-bit A and B from shared memory, S32 accumulator.
+FFT_DEV void tc_mma_u8(uint32_t d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n"
+        "  .reg .pred p;\n"
+        "  setp.ne.b32 p, %4, 0;\n"
+        "  tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n"
+        "}\n" ::"r"(d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// 16 consecutive 32-bit columns of this thread's tensor-memory lane.
+FFT_DEV void tmem_ld16_s32(uint32_t taddr, int32_t (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])::"memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = (int32_t)r[i];
+}
+
+// w entry (k, l) of the block-diagonal 128 x 128 matrix built from the 2N x 2N
+// table (row stride ld), plus the 32768 offset.
+__device__ __forceinline__ uint32_t offset_entry(const int16_t* __restrict__ w, uint32_t n2, uint32_t ld, int k,
+                                                 int l)
+{
+    int32_t v = 0;
+    if ((uint32_t)k / n2 == (uint32_t)l / n2) v = w[(size_t)((uint32_t)k % n2) * ld + (uint32_t)l % n2];
+    return (uint32_t)(v + 32768);
+}
+
+__global__ void __launch_bounds__(IntTc::THREADS, 1)
+    k_int16_tc(const int16_t* x, int16_t* y, const int16_t* __restrict__ w, uint32_t n2, uint32_t ld, uint64_t comps,
+               uint32_t shift, uint32_t* err)
+{
+    using S = IntTc;
+    constexpr int TS = S::TS, NB = S::NB, NA = S::NA, RS = S::RS;
+    extern __shared__ unsigned char int_tc_smem_raw[];
+    unsigned char* sm = int_tc_smem_raw + ((1024u - (smem_addr(int_tc_smem_raw) & 1023u)) & 1023u);
+    const uint32_t sbase = smem_addr(sm);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + S::OFF_BAR);
+    uint32_t* misc = reinterpret_cast<uint32_t*>(sm + S::OFF_MISC);
+    volatile uint32_t* abortFlag = misc + 1;
+    int32_t* colsum = reinterpret_cast<int32_t*>(sm + S::OFF_CS);
+    int32_t* rowsum = reinterpret_cast<int32_t*>(sm + S::OFF_RS);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t superRows = (comps + 127u) / 128u;
+    const uint32_t numTiles = (uint32_t)((superRows + TS - 1) / TS);
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S::NBARS; ++i) mbar_init(&bars[i], 1);
+        misc[1] = 0;
+        fence_mbarrier_init();
+    }
+    if (warp == S::MMA_WARP) {
+        tmem_alloc(&misc[0], S::TMEM_COLS);
+        tmem_relinquish();
+    }
+    // the matrix operand: row l (output value), 16-byte chunk j = input
+    // values 16 j .. 16 j + 15, high and low bytes in two limbs
+    {
+        unsigned char* hi = sm + S::OFF_W;
+        unsigned char* lo = hi + S::W_LIMB;
+        for (int it = threadIdx.x; it < 128 * 8; it += blockDim.x) {
+            const int l = it >> 3, j = it & 7;
+            uint32_t h[4] = {0u, 0u, 0u, 0u}, q[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                const uint32_t u = offset_entry(w, n2, ld, 16 * j + e, l);
+                h[e >> 2] |= (u >> 8) << (8 * (e & 3));
+                q[e >> 2] |= (u & 255u) << (8 * (e & 3));
+            }
+            const uint32_t off = S::LA::chunk(l, j);
+            *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<uint4*>(lo + off) = make_uint4(q[0], q[1], q[2], q[3]);
+        }
+        for (int l = threadIdx.x; l < 128; l += blockDim.x) {
+            int32_t s = 0;
+            for (int k = 0; k < 128; ++k) s += (int32_t)offset_entry(w, n2, ld, k, l);
+            colsum[l] = s;
+        }
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = misc[0];
+
+    if (warp < S::LW) {
+        // ================= loaders =================
+        // lane l holds values 4l .. 4l+3 of a super-row (8 bytes); the next
+        // tile of this CTA is pulled into L2 while this one is converted
+        const int j = threadIdx.x;
+        auto prefetch = [&](uint32_t tl) {
+            if (j != 0 || tl >= numTiles) return;
+            const uint64_t first = (uint64_t)tl * TS * 128u;
+            const uint64_t cnt = min((uint64_t)TS * 128u, comps - first);
+            if ((((uintptr_t)(x + first)) & 15u) != 0 || (cnt * 2u) % 16u != 0) return;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(x + first), "r"((uint32_t)(cnt * 2u))
+                         : "memory");
+        };
+        prefetch(blockIdx.x);
+        uint32_t i = 0;
+        for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
+            prefetch(tile + gridDim.x);
+            const int b = (int)(i % NB);
+            const uint32_t u = i / NB, slot = i % RS;
+            const uint64_t base = (uint64_t)tile * TS * 128u;
+            uint2 v[S::RPW];
+#pragma unroll
+            for (int k = 0; k < S::RPW; ++k) {
+                const uint64_t e0 = base + (uint64_t)(warp * S::RPW + k) * 128u + 4u * lane;
+                if (e0 + 4u <= comps) {
+                    v[k] = *reinterpret_cast<const uint2*>(x + e0);
+                } else {
+                    uint16_t t[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) t[c] = e0 + c < comps ? (uint16_t)x[e0 + c] : (uint16_t)0;
+                    v[k] = make_uint2((uint32_t)t[0] | ((uint32_t)t[1] << 16), (uint32_t)t[2] | ((uint32_t)t[3] << 16));
+                }
+            }
+            bool bad = false;
+            if (u >= 1 && j == 0) bad = !tc_wait(&bars[S::S_FREE + b], (u - 1) & 1u, abortFlag, err);
+            if (group_sync_or(1, 32 * S::LW, bad)) break;
+            unsigned char* hiB = sm + b * S::TILE;
+            unsigned char* loB = hiB + S::X_LIMB;
+#pragma unroll
+            for (int k = 0; k < S::RPW; ++k) {
+                const int r = warp * S::RPW + k;
+                // offset binary: v + 32768 flips the sign bit of each 16-bit value;
+                // high bytes are bytes 1 and 3 of each word, low bytes 0 and 2
+                const uint32_t a = v[k].x ^ 0x80008000u, c = v[k].y ^ 0x80008000u;
+                const uint32_t hb = __byte_perm(a, c, 0x7531u);
+                const uint32_t lb = __byte_perm(a, c, 0x6420u);
+                int32_t s = (int32_t)(256u * __dp4a(hb, 0x01010101u, 0u) + __dp4a(lb, 0x01010101u, 0u));
+#pragma unroll
+                for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                const uint32_t off = S::LB::chunk(r, lane >> 2) + (uint32_t)(lane & 3) * 4u;
+                *reinterpret_cast<uint32_t*>(hiB + off) = hb;
+                *reinterpret_cast<uint32_t*>(loB + off) = lb;
+                if (lane == 0) rowsum[slot * TS + r] = s;
+            }
+            fence_proxy_async_smem();
+            group_sync(1, 32 * S::LW);
+            if (j == 0) mbar_arrive(&bars[S::A_FULL + b]);
+        }
+    } else if (warp == S::MMA_WARP) {
+        // ================= MMA issue =================
+        if (lane == 0) {
+            constexpr uint32_t idesc = umma_idesc_u8(TS);
+            constexpr int KS = 128 / 32;  // 32 bytes of K per instruction
+            const uint32_t wHi = sbase + S::OFF_W, wLo = wHi + S::W_LIMB;
+            uint32_t i = 0;
+            for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
+                const int b = (int)(i % NB), a = (int)(i % NA);
+                const uint32_t u = i / NB, ua = i / NA;
+                if (!tc_wait(&bars[S::A_FULL + b], u & 1u, abortFlag, err)) break;
+                if (ua >= 1 && !tc_wait(&bars[S::D_FREE + a], (ua - 1) & 1u, abortFlag, err)) break;
+                tc_fence_after();
+                const uint32_t xHi = sbase + b * S::TILE, xLo = xHi + S::X_LIMB;
+                const uint32_t d = tmem + (uint32_t)a * S::ACC;
+#pragma unroll
+                for (int s = 0; s < KS; ++s)
+                    tc_mma_u8(d, S::LA::desc(wHi, 0, s), S::LB::desc(xHi, 0, s), idesc, s > 0 ? 1u : 0u);
+#pragma unroll
+                for (int s = 0; s < KS; ++s)
+                    tc_mma_u8(d + TS, S::LA::desc(wHi, 0, s), S::LB::desc(xLo, 0, s), idesc, s > 0 ? 1u : 0u);
+#pragma unroll
+                for (int s = 0; s < KS; ++s)
+                    tc_mma_u8(d + TS, S::LA::desc(wLo, 0, s), S::LB::desc(xHi, 0, s), idesc, 1u);
+#pragma unroll
+                for (int s = 0; s < KS; ++s)
+                    tc_mma_u8(d + 2 * TS, S::LA::desc(wLo, 0, s), S::LB::desc(xLo, 0, s), idesc, s > 0 ? 1u : 0u);
+                tc_commit(&bars[S::S_FREE + b]);
+                tc_commit(&bars[S::D_FULL + a]);
+            }
+            tc_commit(&bars[S::DRAIN]);
+            mbar_wait_bounded(&bars[S::DRAIN], 0);
+        }
+        __syncwarp();
+    } else {
+        // ================= epilogue =================
+        // thread = output value l of the super-rows of one half of the tile
+        const int et = threadIdx.x - 32 * S::LW;  // 0..255
+        const int q = warp & 3, ch = (warp - S::LW) >> 2;
+        const int l = 32 * q + lane;
+        const uint32_t laneBase = (uint32_t)(32 * q) << 16;
+        // sum x w = 2^16 hh + 2^8 mid + ll + cl - 2^15 rowsum, |sum x w| <= 2^37;
+        // shiftAndRound as (v + 2^(s-1)) >> s, which equals the reference's
+        // ((v >> (s-1)) + 1) >> 1; every shift of 39 or more gives 0 for
+        // such v, as 39 itself does
+        const long long cl = (128ll << 30) - 32768ll * (long long)colsum[l];
+        const uint32_t s8 = shift & 0xFFu;
+        const uint32_t sh = s8 > 39u ? 39u : s8;
+        const long long rnd = sh ? (1ll << (sh - 1u)) : 0ll;
+        uint32_t i = 0;
+        for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
+            const int a = (int)(i % NA);
+            const uint32_t ua = i / NA, slot = i % RS;
+            bool bad = false;
+            if (et == 0) bad = !tc_wait(&bars[S::D_FULL + a], ua & 1u, abortFlag, err);
+            if (group_sync_or(3, 32 * S::EW, bad)) break;
+            tc_fence_after();
+            const uint64_t base = (uint64_t)tile * TS * 128u + (uint64_t)l;
+            const bool full = (uint64_t)(tile + 1) * TS * 128u <= comps;
+            const uint32_t dbase = tmem + laneBase + (uint32_t)a * S::ACC;
+#pragma unroll
+            for (int cc = 0; cc < TS / 2; cc += 16) {
+                const int c0 = ch * (TS / 2) + cc;
+                int32_t hh[16], mid[16], ll[16];
+                tmem_ld16_s32(dbase + (uint32_t)c0, hh);
+                tmem_ld16_s32(dbase + (uint32_t)(TS + c0), mid);
+                tmem_ld16_s32(dbase + (uint32_t)(2 * TS + c0), ll);
+                int16_t out[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const long long v = ((long long)hh[e] << 16) + ((long long)mid[e] << 8) + (long long)ll[e] + cl -
+                                        ((long long)rowsum[slot * TS + c0 + e] << 15);
+                    const long long q = (v + rnd) >> sh;
+                    out[e] = q > 32767ll ? (int16_t)32767 : (q < -32768ll ? (int16_t)-32768 : (int16_t)q);
+                }
+                int16_t* yb = y + base + (uint64_t)c0 * 128u;
+                if (full) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) yb[e * 128] = out[e];
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)
+                        if (base + (uint64_t)(c0 + e) * 128u < comps) yb[e * 128] = out[e];
+                }
+            }
+            tc_fence_before();
+            group_sync(3, 32 * S::EW);
+            if (et == 0) mbar_arrive(&bars[S::D_FREE + a]);
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == S::MMA_WARP) {
+        tc_fence_after();
+        tmem_dealloc(tmem, S::TMEM_COLS);
+    }
+}
+
+} // namespace
+
+bool int16_tc_supported(uint32_t n2, const void* x, const void* y)
+{
+    return n2 >= 2 && n2 <= 128 && 128u % n2 == 0 && ((uintptr_t)x & 7u) == 0 && ((uintptr_t)y & 1u) == 0;
+}
+
+cudaError_t launch_int16_tc(const int16_t* x, int16_t* y, const int16_t* w, uint32_t n2, uint32_t ld, uint32_t rows,
+                            uint32_t shift, cudaStream_t s)
+{
+    using S = IntTc;
+    const uint64_t comps = (uint64_t)rows * n2;
+    if (comps == 0) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static bool configured[64] = {};
+    static int sms[64] = {};
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev >= 64) return cudaErrorInvalidDevice;
+        if (!configured[dev]) {
+            e = cudaFuncSetAttribute(k_int16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+            if (e != cudaSuccess) return e;
+            e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess) return e;
+            configured[dev] = true;
+        }
+    }
+    const uint64_t tiles = ((comps + 127u) / 128u + S::TS - 1) / S::TS;
+    const uint32_t grid = (uint32_t)(tiles < (uint64_t)sms[dev] ? tiles : (uint64_t)sms[dev]);
+    k_int16_tc<<<grid, S::THREADS, S::SMEM, s>>>(x, y, w, n2, ld, comps, shift, error_word().dev);
+    return cudaGetLastError();
+}
+
+} // namespace fftb200

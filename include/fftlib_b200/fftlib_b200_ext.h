@@ -108,6 +108,12 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_destroy(FFTLIB_b200_mixedHandle handle);
 void FFTLIB_b200_tw_gen_c2c(FFTLIB_F32 *pW, uint32_t numPoints);
 void FFTLIB_b200_tw_gen_i16(int16_t *pW, uint32_t numPoints);
 
+/* The INT16 dftSmall / dftLarge products of the DFT coordinator and its
+ * variants run on the tensor cores (exact u8 x u8 limb products) where the
+ * row length divides 128 values; 0 selects the CUDA-core kernel instead,
+ * which gives the same bits (for comparisons), 1 restores the default. */
+void FFTLIB_b200_FFT_setIntTensorCores(int32_t enable);
+
 /* The same generators on the GPU, for callers that keep no host copy of the
  * tables: the reference's formulas with pi truncated to 3.141592654 and the
  * same order of double operations, so the tables are bit-identical to the

@@ -97,3 +97,35 @@ def test_high_radix_needs_distinct_buffers(torch_cuda):
     st = F.lib().FFTLIB_FFT_fft_ixX_cxX_oxX_exec(d.handle, F.ptr(X), F.ptr(d.w), F.ptr(X))
     assert st == F.FFTLIB_ERR_INVALID_VALUE
     assert d.path == 3
+
+
+@pytest.mark.parametrize("bits,n,batch,il", [(16, 16, 1 << 16, 1), (16, 32, 40000, 0), (16, 64, 20001, 1),
+                                             (16, 8, 3333, 1), (16, 1, 999, 1), (16, 2, 70, 0), (16, 4, 513, 1)])
+def test_tensor_core_and_cuda_core_products_agree(torch_cuda, bits, n, batch, il):
+    """The INT16 dftSmall / dftLarge product on the tensor cores (byte limbs
+    of offset-binary values, exact) against the CUDA-core kernel on the same
+    full-range inputs, ragged batches included, and against the oracle."""
+    L = F.lib()
+    x = _rand(bits, 2 * n * batch, 3 * n + batch, True)
+    for sh in ([0] * 5, [bits - 1] * 5, [7] * 5):
+        try:
+            L.FFTLIB_b200_FFT_setIntTensorCores(0)
+            y_cc = run(torch_cuda, bits, n, batch, il, sh, x)
+        finally:
+            L.FFTLIB_b200_FFT_setIntTensorCores(1)
+        y_tc = run(torch_cuda, bits, n, batch, il, sh, x)
+        assert np.array_equal(y_tc, y_cc), sh
+        k = min(batch, 257)
+        assert np.array_equal(y_tc[: 2 * n * k], O.mma_exec(bits, n, k, il, sh, x[: 2 * n * k])), sh
+
+
+def test_tensor_core_product_in_place(torch_cuda):
+    import torch
+
+    bits, n, batch = 16, 32, 5000
+    x = _rand(bits, 2 * n * batch, 77, True)
+    sh = [3] * 5
+    d = F.DftMma(n, batch, dtype=F.FFTLIB_INT16, interleave=1, shifts=sh)
+    X = torch.from_numpy(np.ascontiguousarray(x, np.int16)).cuda()
+    d.exec(X, X)
+    assert np.array_equal(X.cpu().numpy(), O.mma_exec(bits, n, batch, 1, sh, x))
