@@ -147,6 +147,16 @@ cudaError_t matmul_typed(uint32_t M, uint32_t K, uint32_t N, const void* a, size
                          void* c, size_t ldc, uint32_t shift, cudaStream_t s)
 {
     if (M == 0 || N == 0) return cudaSuccess;
+    if constexpr (IntT<T>::kBits <= 16) {
+        // square products of dense rows of at most 128 values (the DFT
+        // shape): the super-row kernel keeps the whole B in shared memory
+        if (IntT<T>::kBits == 16 && int_tensor_cores() && K == N && lda == K && ldc == N &&
+            int16_tc_supported(K, a, c) && a != c)
+            return launch_int16_tc(static_cast<const int16_t*>(a), static_cast<int16_t*>(c),
+                                   static_cast<const int16_t*>(b), K, (uint32_t)ldb, M, shift, s);
+        if (int_mm_tc_supported(IntT<T>::kBits, M, K, N, a, lda, b, ldb))
+            return launch_int_mm_tc(IntT<T>::kBits, M, K, N, a, lda, b, ldb, c, ldc, shift, s);
+    }
     const uint64_t gx = ((uint64_t)M + kMmTile - 1) / kMmTile, gy = ((uint64_t)N + kMmTile - 1) / kMmTile;
     if (gx > 0x7FFFFFFFull || gy > 65535ull) return cudaErrorInvalidValue;
     k_int_mm<T><<<dim3((unsigned)gx, (unsigned)gy), 256, 0, s>>>(static_cast<const T*>(a), lda,

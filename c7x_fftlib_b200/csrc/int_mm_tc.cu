@@ -1,0 +1,516 @@
+// int_mm_tc.cu -- the LINALG integer matrix multiply C = round_shift(A B) on
+// the tensor cores (tcgen05.mma kind::i8), bit-exact with the reference's
+// natural C (src/linalg_c7xmma/FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX/
+// FFTLIB_LINALG_matrixMatrixMultiply_ixX_ixX_oxX_cn.cpp:27-62).
+//
+// INT8: signed 8-bit A and B, products summed in the 32-bit accumulators
+// (the reference's int32 sum; both wrap only where that sum overflows).
+// INT16: every value in offset binary v' = v + 32768 = 256 h + l, four u8 x u8
+// products per product of values summed in three accumulators, then
+//   sum a b = 2^16 hh + 2^8 mid + ll - 2^15 (sum a' + sum b') + Kp 2^30
+// in 64 bits (Kp = K rounded up to the 128-value chunks; the zero padding is
+// offset like the data). K is limited to 16384 so that the accumulators
+// cannot overflow; larger K runs the CUDA-core kernel.
+//
+// A CTA computes 128 x BN tiles of C (BN = 128 for INT8, 64 for INT16) and
+// walks K in chunks of 128 values through a ring of shared-memory stages.
+// Roles (one persistent CTA per SM): 8 loader warps (HBM -> registers ->
+// K-major swizzled operands; B is transposed with byte permutes; INT16 also
+// forms the offset limbs and the row and column sums), one warp that
+// allocates tensor memory and issues the MMAs, and 4 epilogue warps (tensor
+// memory lane = row of C -> shift, round, saturate -> HBM). Two accumulator
+// buffers let the epilogue of one tile overlap the MMAs of the next. Every
+// wait is bounded; a wait that gives up sets kErrTcTimeout in the launch's
+// error word.
+#include <mutex>
+#include <type_traits>
+
+#include "dft_int.h"
+#include "int_arith.cuh"
+#include "plan.h"
+#include "tc_dft.cuh"
+
+namespace fftb200 {
+
+namespace {
+
+template <bool I16>
+struct MmTc {
+    static constexpr int BN = I16 ? 64 : 128;
+    static constexpr int NS = I16 ? 3 : 4;  // K-chunk stages
+    static constexpr int NA = 2;            // accumulator buffers
+    static constexpr int RS = 8;            // row / column sum slots (INT16)
+    static constexpr int LW = 8, EW = 4;
+    static constexpr int MMA_WARP = LW + EW;
+    static constexpr int THREADS = 32 * (MMA_WARP + 1);
+    static constexpr int KC = 128;  // K values per chunk
+    static constexpr int LIMBS = I16 ? 2 : 1;
+    using LA = KMajor<128, 64>;  // 128 rows of 128 bytes
+    using LB = KMajor<BN, 64>;   // BN rows of 128 bytes
+    static constexpr uint32_t A_LIMB = LA::BYTES;
+    static constexpr uint32_t B_LIMB = LB::BYTES;
+    static constexpr uint32_t LIMB_PAIR = A_LIMB + B_LIMB;  // A limb then B limb
+    static constexpr uint32_t STAGE = LIMBS * LIMB_PAIR;
+    static constexpr uint32_t OFF_RS = NS * STAGE;
+    static constexpr uint32_t OFF_CP = OFF_RS + (I16 ? 4u * RS * 128u : 0u);  // column-sum partials [LW][BN]
+    static constexpr uint32_t OFF_CS = OFF_CP + (I16 ? 4u * LW * BN : 0u);    // column sums [RS][BN]
+    static constexpr uint32_t OFF_BAR = (OFF_CS + (I16 ? 4u * RS * BN : 0u) + 7u) & ~7u;
+    static constexpr int NBARS = 2 * NS + 2 * NA + 1;
+    static constexpr uint32_t OFF_MISC = OFF_BAR + 8u * NBARS;
+    static constexpr uint32_t SMEM = OFF_MISC + 16u + 1024u;
+    static constexpr uint32_t ACC = (I16 ? 3u : 1u) * BN;
+    static constexpr uint32_t TMEM_COLS = I16 ? 512u : 256u;
+    static constexpr int FULL = 0, EMPTY = NS, AFULL = 2 * NS, AEMPTY = 2 * NS + NA, DRAIN = 2 * NS + 2 * NA;
+    static_assert(NA * ACC <= TMEM_COLS, "tensor memory");
+    static_assert(NS + NA <= RS, "sum slots");
+    static_assert(SMEM <= 227u * 1024u, "shared memory per CTA");
+    static_assert(A_LIMB % 1024u == 0 && B_LIMB % 1024u == 0, "1024-byte aligned operands");
+};
+
+// Instruction descriptor: S32 accumulator, 8-bit A and B (signed or
+// unsigned, the same for both), K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t umma_idesc_i8(int n, bool is_signed)
+{
+    const uint32_t f = is_signed ? 1u : 0u;
+    return (2u << 4) | (f << 7) | (f << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+FFT_DEV void tc_mma_i8(uint32_t d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n"
+        "  .reg .pred p;\n"
+        "  setp.ne.b32 p, %4, 0;\n"
+        "  tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n"
+        "}\n" ::"r"(d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+FFT_DEV void tmem_ld16_i32(uint32_t taddr, int32_t (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])::"memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = (int32_t)r[i];
+}
+
+struct MmArgs {
+    const void* a;
+    const void* b;
+    void* c;
+    size_t lda, ldb, ldc;  // elements
+    uint32_t M, K, N;
+    uint32_t shift;
+    uint32_t tilesN, numTiles, chunks;  // chunks of 128 K values per tile
+    uint32_t* err;
+};
+
+template <bool I16>
+__global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
+{
+    using S = MmTc<I16>;
+    using T = typename std::conditional<I16, int16_t, int8_t>::type;
+    constexpr int BN = S::BN, NS = S::NS, NA = S::NA, RS = S::RS;
+    extern __shared__ unsigned char mm_tc_smem_raw[];
+    unsigned char* sm = mm_tc_smem_raw + ((1024u - (smem_addr(mm_tc_smem_raw) & 1023u)) & 1023u);
+    const uint32_t sbase = smem_addr(sm);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + S::OFF_BAR);
+    uint32_t* misc = reinterpret_cast<uint32_t*>(sm + S::OFF_MISC);
+    volatile uint32_t* abortFlag = misc + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const T* A = static_cast<const T*>(p.a);
+    const T* B = static_cast<const T*>(p.b);
+    T* Cm = static_cast<T*>(p.c);
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S::NBARS; ++i) mbar_init(&bars[i], 1);
+        misc[1] = 0;
+        fence_mbarrier_init();
+    }
+    if (warp == S::MMA_WARP) {
+        tmem_alloc(&misc[0], S::TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = misc[0];
+
+    if (warp < S::LW) {
+        // ================= loaders =================
+        const int tid = threadIdx.x;  // 0..255
+        int32_t* rowsum = reinterpret_cast<int32_t*>(sm + S::OFF_RS);
+        int32_t* cpart = reinterpret_cast<int32_t*>(sm + S::OFF_CP);
+        int32_t* colsum = reinterpret_cast<int32_t*>(sm + S::OFF_CS);
+        uint32_t g = 0, ti = 0;  // chunk counter, tile counter of this CTA
+        bool stop = false;
+        for (uint32_t tile = blockIdx.x; tile < p.numTiles && !stop; tile += gridDim.x, ++ti) {
+            const uint32_t m0 = (tile / p.tilesN) * 128u, n0 = (tile % p.tilesN) * (uint32_t)BN;
+            int32_t rs = 0, cs0 = 0, cs1 = 0;
+            for (uint32_t ch = 0; ch < p.chunks; ++ch, ++g) {
+                const int st = (int)(g % NS);
+                const uint32_t u = g / NS;
+                const uint32_t k0 = ch * 128u;
+                bool bad = false;
+                if (u >= 1 && tid == 0) bad = !tc_wait(&bars[S::EMPTY + st], (u - 1) & 1u, abortFlag, p.err);
+                if (group_sync_or(1, 32 * S::LW, bad)) {
+                    stop = true;
+                    break;
+                }
+                unsigned char* aHi = sm + st * S::STAGE;
+                unsigned char* bHi = aHi + S::A_LIMB;
+                if constexpr (!I16) {
+                    // A: 128 rows x 8 chunks of 16 bytes
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int it = tid + 256 * q;
+                        const int row = it >> 3, j = it & 7;
+                        const uint32_t m = m0 + row, k = k0 + 16u * j;
+                        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                        if (m < p.M) {
+                            const T* src = A + (size_t)m * p.lda + k;
+                            if (k + 16u <= p.K) {
+                                v = *reinterpret_cast<const uint4*>(src);
+                            } else {
+                                uint32_t wv[4] = {0u, 0u, 0u, 0u};
+                                for (int e = 0; e < 16; ++e)
+                                    if (k + e < p.K) wv[e >> 2] |= (uint32_t)(uint8_t)src[e] << (8 * (e & 3));
+                                v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                            }
+                        }
+                        *reinterpret_cast<uint4*>(aHi + S::LA::chunk(row, j)) = v;
+                    }
+                    // B: 32 x 32 blocks of 4 K rows x 4 columns, transposed
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int it = tid + 256 * q;
+                        const int kb = it >> 5, nb = it & 31;
+                        const uint32_t n = n0 + 4u * nb;
+                        uint32_t r[4];
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) {
+                            const uint32_t k = k0 + 4u * kb + t;
+                            r[t] = 0u;
+                            if (k < p.K) {
+                                const T* src = B + (size_t)k * p.ldb + n;
+                                if (n + 4u <= p.N) {
+                                    r[t] = *reinterpret_cast<const uint32_t*>(src);
+                                } else {
+                                    for (int e = 0; e < 4; ++e)
+                                        if (n + e < p.N) r[t] |= (uint32_t)(uint8_t)src[e] << (8 * e);
+                                }
+                            }
+                        }
+                        const uint32_t t01l = __byte_perm(r[0], r[1], 0x5140u), t23l = __byte_perm(r[2], r[3], 0x5140u);
+                        const uint32_t t01h = __byte_perm(r[0], r[1], 0x7362u), t23h = __byte_perm(r[2], r[3], 0x7362u);
+                        const uint32_t col[4] = {__byte_perm(t01l, t23l, 0x5410u), __byte_perm(t01l, t23l, 0x7632u),
+                                                 __byte_perm(t01h, t23h, 0x5410u), __byte_perm(t01h, t23h, 0x7632u)};
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            *reinterpret_cast<uint32_t*>(bHi + S::LB::chunk(4 * nb + c, kb >> 2) + (kb & 3) * 4) =
+                                col[c];
+                    }
+                } else {
+                    unsigned char* aLo = aHi + S::LIMB_PAIR;
+                    unsigned char* bLo = bHi + S::LIMB_PAIR;
+                    // A: row tid/2, half tid&1 of the chunk's 128 values, 8 units of 8 values
+                    {
+                        const int row = tid >> 1, h = tid & 1;
+                        const uint32_t m = m0 + row;
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int unit = 8 * h + j;  // values 8 unit .. 8 unit + 7
+                            const uint32_t k = k0 + 8u * unit;
+                            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                            if (m < p.M) {
+                                const T* src = A + (size_t)m * p.lda + k;
+                                if (k + 8u <= p.K) {
+                                    v = *reinterpret_cast<const uint4*>(src);
+                                } else {
+                                    uint32_t wv[4] = {0u, 0u, 0u, 0u};
+                                    for (int e = 0; e < 8; ++e)
+                                        if (k + e < p.K) wv[e >> 1] |= (uint32_t)(uint16_t)src[e] << (16 * (e & 1));
+                                    v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                                }
+                            }
+                            const uint32_t a0 = v.x ^ 0x80008000u, a1 = v.y ^ 0x80008000u;
+                            const uint32_t a2 = v.z ^ 0x80008000u, a3 = v.w ^ 0x80008000u;
+                            const uint32_t h0 = __byte_perm(a0, a1, 0x7531u), h1 = __byte_perm(a2, a3, 0x7531u);
+                            const uint32_t l0 = __byte_perm(a0, a1, 0x6420u), l1 = __byte_perm(a2, a3, 0x6420u);
+                            rs += (int32_t)(256u * (__dp4a(h0, 0x01010101u, 0u) + __dp4a(h1, 0x01010101u, 0u)) +
+                                            __dp4a(l0, 0x01010101u, 0u) + __dp4a(l1, 0x01010101u, 0u));
+                            const uint32_t off = S::LA::chunk(row, unit >> 1) + (uint32_t)(unit & 1) * 8u;
+                            *reinterpret_cast<uint2*>(aHi + off) = make_uint2(h0, h1);
+                            *reinterpret_cast<uint2*>(aLo + off) = make_uint2(l0, l1);
+                        }
+                    }
+                    // B: 32 x 32 blocks of 4 K rows x 2 columns; column pair nb = tid & 31
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int it = tid + 256 * q;
+                        const int kb = it >> 5, nb = it & 31;
+                        const uint32_t n = n0 + 2u * nb;
+                        uint32_t r[4];
+#pragma unroll
+                        for (int t = 0; t < 4; ++t) {
+                            const uint32_t k = k0 + 4u * kb + t;
+                            uint32_t wv = 0u;
+                            if (k < p.K) {
+                                const T* src = B + (size_t)k * p.ldb + n;
+                                if (n + 2u <= p.N) {
+                                    wv = *reinterpret_cast<const uint32_t*>(src);
+                                } else if (n < p.N) {
+                                    wv = (uint32_t)(uint16_t)src[0];
+                                }
+                            }
+                            r[t] = wv ^ 0x80008000u;
+                        }
+                        const uint32_t t01 = __byte_perm(r[0], r[1], 0x7351u), t23 = __byte_perm(r[2], r[3], 0x7351u);
+                        const uint32_t u01 = __byte_perm(r[0], r[1], 0x6240u), u23 = __byte_perm(r[2], r[3], 0x6240u);
+                        const uint32_t hiN0 = __byte_perm(t01, t23, 0x5410u), hiN1 = __byte_perm(t01, t23, 0x7632u);
+                        const uint32_t loN0 = __byte_perm(u01, u23, 0x5410u), loN1 = __byte_perm(u01, u23, 0x7632u);
+                        cs0 += (int32_t)(256u * __dp4a(hiN0, 0x01010101u, 0u) + __dp4a(loN0, 0x01010101u, 0u));
+                        cs1 += (int32_t)(256u * __dp4a(hiN1, 0x01010101u, 0u) + __dp4a(loN1, 0x01010101u, 0u));
+                        const uint32_t o0 = S::LB::chunk(2 * nb, kb >> 2) + (kb & 3) * 4;
+                        const uint32_t o1 = S::LB::chunk(2 * nb + 1, kb >> 2) + (kb & 3) * 4;
+                        *reinterpret_cast<uint32_t*>(bHi + o0) = hiN0;
+                        *reinterpret_cast<uint32_t*>(bHi + o1) = hiN1;
+                        *reinterpret_cast<uint32_t*>(bLo + o0) = loN0;
+                        *reinterpret_cast<uint32_t*>(bLo + o1) = loN1;
+                    }
+                    if (ch + 1 == p.chunks) {
+                        // the tile's sums: rows from the two threads of a row,
+                        // columns from the 8 warps' partials
+                        const int slot = (int)(ti % RS);
+                        const int32_t rsum = rs + __shfl_xor_sync(0xffffffffu, rs, 1);
+                        if ((tid & 1) == 0) rowsum[slot * 128 + (tid >> 1)] = rsum;
+                        cpart[warp * BN + 2 * lane] = cs0;
+                        cpart[warp * BN + 2 * lane + 1] = cs1;
+                        group_sync(1, 32 * S::LW);
+                        if (tid < BN) {
+                            int32_t sum = 0;
+#pragma unroll
+                            for (int w8 = 0; w8 < S::LW; ++w8) sum += cpart[w8 * BN + tid];
+                            colsum[slot * BN + tid] = sum;
+                        }
+                    }
+                }
+                fence_proxy_async_smem();
+                group_sync(1, 32 * S::LW);
+                if (tid == 0) mbar_arrive(&bars[S::FULL + st]);
+            }
+        }
+    } else if (warp == S::MMA_WARP) {
+        // ================= MMA issue =================
+        if (lane == 0) {
+            constexpr uint32_t idesc = umma_idesc_i8(BN, !I16);
+            constexpr int KS = 128 / 32;
+            uint32_t g = 0, ti = 0;
+            bool stop = false;
+            for (uint32_t tile = blockIdx.x; tile < p.numTiles && !stop; tile += gridDim.x, ++ti) {
+                const int a = (int)(ti % NA);
+                const uint32_t ua = ti / NA;
+                if (ua >= 1 && !tc_wait(&bars[S::AEMPTY + a], (ua - 1) & 1u, abortFlag, p.err)) break;
+                const uint32_t d = tmem + (uint32_t)a * S::ACC;
+                for (uint32_t ch = 0; ch < p.chunks; ++ch, ++g) {
+                    const int st = (int)(g % NS);
+                    const uint32_t u = g / NS;
+                    if (!tc_wait(&bars[S::FULL + st], u & 1u, abortFlag, p.err)) {
+                        stop = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t aHi = sbase + st * S::STAGE, bHi = aHi + S::A_LIMB;
+                    if constexpr (!I16) {
+#pragma unroll
+                        for (int s = 0; s < KS; ++s)
+                            tc_mma_i8(d, S::LA::desc(aHi, 0, s), S::LB::desc(bHi, 0, s), idesc,
+                                      (ch > 0 || s > 0) ? 1u : 0u);
+                    } else {
+                        const uint32_t aLo = aHi + S::LIMB_PAIR, bLo = bHi + S::LIMB_PAIR;
+#pragma unroll
+                        for (int s = 0; s < KS; ++s)
+                            tc_mma_i8(d, S::LA::desc(aHi, 0, s), S::LB::desc(bHi, 0, s), idesc,
+                                      (ch > 0 || s > 0) ? 1u : 0u);
+#pragma unroll
+                        for (int s = 0; s < KS; ++s)
+                            tc_mma_i8(d + BN, S::LA::desc(aHi, 0, s), S::LB::desc(bLo, 0, s), idesc,
+                                      (ch > 0 || s > 0) ? 1u : 0u);
+#pragma unroll
+                        for (int s = 0; s < KS; ++s)
+                            tc_mma_i8(d + BN, S::LA::desc(aLo, 0, s), S::LB::desc(bHi, 0, s), idesc, 1u);
+#pragma unroll
+                        for (int s = 0; s < KS; ++s)
+                            tc_mma_i8(d + 2 * BN, S::LA::desc(aLo, 0, s), S::LB::desc(bLo, 0, s), idesc,
+                                      (ch > 0 || s > 0) ? 1u : 0u);
+                    }
+                    tc_commit(&bars[S::EMPTY + st]);
+                }
+                if (stop) break;
+                tc_commit(&bars[S::AFULL + a]);
+            }
+            tc_commit(&bars[S::DRAIN]);
+            mbar_wait_bounded(&bars[S::DRAIN], 0);
+        }
+        __syncwarp();
+    } else {
+        // ================= epilogue =================
+        const int et = threadIdx.x - 32 * S::LW;  // 0..127
+        const int q = warp & 3;
+        const uint32_t laneBase = (uint32_t)(32 * q) << 16;
+        const int32_t* rowsum = reinterpret_cast<const int32_t*>(sm + S::OFF_RS);
+        const int32_t* colsum = reinterpret_cast<const int32_t*>(sm + S::OFF_CS);
+        // INT16: |sum a b| <= K 2^30 <= 2^44, so every shift of 46 or more
+        // gives 0, as 46 itself does; (v + 2^(s-1)) >> s equals the
+        // reference's ((v >> (s-1)) + 1) >> 1
+        const uint32_t s8 = p.shift & 0xFFu;
+        const uint32_t sh = s8 > 46u ? 46u : s8;
+        const long long rnd = sh ? (1ll << (sh - 1u)) : 0ll;
+        const long long kp = (long long)p.chunks * 128ll << 30;
+        uint32_t ti = 0;
+        for (uint32_t tile = blockIdx.x; tile < p.numTiles; tile += gridDim.x, ++ti) {
+            const int a = (int)(ti % NA);
+            const uint32_t ua = ti / NA;
+            bool bad = false;
+            if (et == 0) bad = !tc_wait(&bars[S::AFULL + a], ua & 1u, abortFlag, p.err);
+            if (group_sync_or(3, 32 * S::EW, bad)) break;
+            tc_fence_after();
+            const uint32_t m0 = (tile / p.tilesN) * 128u, n0 = (tile % p.tilesN) * (uint32_t)BN;
+            const uint32_t m = m0 + (uint32_t)(32 * q + lane);
+            const uint32_t dbase = tmem + laneBase + (uint32_t)a * S::ACC;
+            const int slot = (int)(ti % RS);
+            long long rowc = 0;
+            if constexpr (I16) rowc = kp - ((long long)rowsum[slot * 128 + 32 * q + lane] << 15);
+            T* crow = Cm + (size_t)m * p.ldc + n0;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                T out[16];
+                if constexpr (!I16) {
+                    int32_t acc[16];
+                    tmem_ld16_i32(dbase + (uint32_t)c0, acc);
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) out[e] = shift_round<int8_t>(acc[e], p.shift);
+                } else {
+                    int32_t hh[16], mid[16], ll[16];
+                    tmem_ld16_i32(dbase + (uint32_t)c0, hh);
+                    tmem_ld16_i32(dbase + (uint32_t)(BN + c0), mid);
+                    tmem_ld16_i32(dbase + (uint32_t)(2 * BN + c0), ll);
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const long long v = ((long long)hh[e] << 16) + ((long long)mid[e] << 8) + (long long)ll[e] +
+                                            rowc - ((long long)colsum[slot * BN + c0 + e] << 15);
+                        const long long qv = (v + rnd) >> sh;
+                        out[e] = qv > 32767ll ? (int16_t)32767 : (qv < -32768ll ? (int16_t)-32768 : (int16_t)qv);
+                    }
+                }
+                if (m < p.M) {
+                    T* dst = crow + c0;
+                    const bool vec = n0 + (uint32_t)c0 + 16u <= p.N && ((uintptr_t)dst & 15u) == 0;
+                    if (vec) {
+                        if constexpr (!I16) {
+                            uint32_t wv[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                            for (int e = 0; e < 16; ++e) wv[e >> 2] |= (uint32_t)(uint8_t)out[e] << (8 * (e & 3));
+                            *reinterpret_cast<uint4*>(dst) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                        } else {
+                            uint32_t wv[8];
+#pragma unroll
+                            for (int e = 0; e < 8; ++e)
+                                wv[e] = (uint32_t)(uint16_t)out[2 * e] | ((uint32_t)(uint16_t)out[2 * e + 1] << 16);
+                            *reinterpret_cast<uint4*>(dst) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                            *reinterpret_cast<uint4*>(dst + 8) = make_uint4(wv[4], wv[5], wv[6], wv[7]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 16; ++e)
+                            if (n0 + (uint32_t)(c0 + e) < p.N) dst[e] = out[e];
+                    }
+                }
+            }
+            tc_fence_before();
+            group_sync(3, 32 * S::EW);
+            if (et == 0) mbar_arrive(&bars[S::AEMPTY + a]);
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == S::MMA_WARP) {
+        tc_fence_after();
+        tmem_dealloc(tmem, S::TMEM_COLS);
+    }
+}
+
+template <bool I16>
+cudaError_t launch_mm_tc(MmArgs p, cudaStream_t s)
+{
+    using S = MmTc<I16>;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static bool configured[64] = {};
+    static int sms[64] = {};
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev >= 64) return cudaErrorInvalidDevice;
+        if (!configured[dev]) {
+            e = cudaFuncSetAttribute(k_int_mm_tc<I16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+            if (e != cudaSuccess) return e;
+            e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess) return e;
+            configured[dev] = true;
+        }
+    }
+    p.tilesN = (p.N + S::BN - 1) / S::BN;
+    const uint64_t tiles = (uint64_t)((p.M + 127u) / 128u) * p.tilesN;
+    if (tiles > 0xFFFFFFFFull) return cudaErrorInvalidValue;
+    p.numTiles = (uint32_t)tiles;
+    p.chunks = (p.K + 127u) / 128u;
+    p.err = error_word().dev;
+    const uint32_t grid = (uint32_t)(tiles < (uint64_t)sms[dev] ? tiles : (uint64_t)sms[dev]);
+    k_int_mm_tc<I16><<<grid, S::THREADS, S::SMEM, s>>>(p);
+    return cudaGetLastError();
+}
+
+} // namespace
+
+bool int_mm_tc_supported(int bits, uint32_t M, uint32_t K, uint32_t N, const void* a, size_t lda, const void* b,
+                         size_t ldb)
+{
+    if (!int_tensor_cores() || M == 0 || N == 0 || K == 0) return false;
+    if (bits == 8)
+        return ((uintptr_t)a & 15u) == 0 && lda % 16u == 0 && ((uintptr_t)b & 3u) == 0 && ldb % 4u == 0;
+    if (bits == 16)
+        return K <= 16384u && ((uintptr_t)a & 15u) == 0 && lda % 8u == 0 && ((uintptr_t)b & 3u) == 0 &&
+               ldb % 2u == 0;
+    return false;
+}
+
+cudaError_t launch_int_mm_tc(int bits, uint32_t M, uint32_t K, uint32_t N, const void* a, size_t lda, const void* b,
+                             size_t ldb, void* c, size_t ldc, uint32_t shift, cudaStream_t s)
+{
+    MmArgs p{};
+    p.a = a;
+    p.b = b;
+    p.c = c;
+    p.lda = lda;
+    p.ldb = ldb;
+    p.ldc = ldc;
+    p.M = M;
+    p.K = K;
+    p.N = N;
+    p.shift = shift;
+    return bits == 16 ? launch_mm_tc<true>(p, s) : launch_mm_tc<false>(p, s);
+}
+
+} // namespace fftb200

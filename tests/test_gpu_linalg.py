@@ -95,3 +95,35 @@ def test_overlapping_source_rows(torch_cuda):
     Cm = np.zeros((m, n), np.int16)
     mm.exec(flat, b, Cm)
     assert np.array_equal(Cm, O.linalg_mm(bits, a, b, 2))
+
+
+@pytest.mark.parametrize("bits", [8, 16])
+@pytest.mark.parametrize("m,k,n,lda,ldb,ldc", [(128, 128, 128, 128, 128, 128), (300, 100, 70, 112, 72, 70),
+                                               (129, 257, 65, 272, 68, 80), (1000, 64, 64, 64, 64, 64),
+                                               (64, 1000, 200, 1008, 200, 203), (1, 16, 4, 16, 4, 4)])
+def test_tensor_core_and_cuda_core_agree(torch_cuda, bits, m, k, n, lda, ldb, ldc):
+    """The tensor-core multiply (rows of A 16-byte aligned, of B 4-byte
+    aligned) against the CUDA-core kernel on the same full-range data, ragged
+    tiles and K chunks included, and against the oracle."""
+    torch = torch_cuda
+    L = F.lib()
+    rng = np.random.default_rng(m * 7 + k + n + bits)
+    mx = (1 << (bits - 1)) - 1
+    A = rng.integers(-mx - 1, mx + 1, (m, lda)).astype(NP[bits])
+    B = rng.integers(-mx - 1, mx + 1, (k, ldb)).astype(NP[bits])
+    Ad, Bd = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    for sh in (0, 3, bits + 5, 2 * bits - 1, 4 * bits):
+        mm = F.MatMul(m, k, n, DT[bits], shift=sh, lda=lda, ldb=ldb, ldc=ldc)
+        outs = []
+        for tc in (0, 1):
+            L.FFTLIB_b200_FFT_setIntTensorCores(tc)
+            try:
+                Cd = torch.full((m, ldc), 5, dtype=Ad.dtype, device="cuda")
+                mm.exec(Ad, Bd, Cd)
+                outs.append(Cd.cpu().numpy())
+            finally:
+                L.FFTLIB_b200_FFT_setIntTensorCores(1)
+        assert np.array_equal(outs[0], outs[1]), sh
+        want = O.linalg_mm(bits, A[:, :k], B[:, :n], sh)
+        assert np.array_equal(outs[1][:, :n], want), sh
+        assert (outs[1][:, n:] == 5).all()
