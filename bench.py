@@ -679,8 +679,10 @@ def run_case(args):
     JSON line with the per-launch time. For profiler captures and sweeps.
     Cases: tc:N:rows (tensor-core DFT), fft:N:rows (CUDA-core FFT through the
     coordinator), c2c:N:channels, r2c:N:channels, c2r:N:channels,
-    i16:N:channels (fft1dBatched kernels), mixed:COUNT:SEED (uneven lengths,
-    one graph launch)."""
+    i16:N:channels (fft1dBatched kernels), int16:N:rows / int32:N:rows (the
+    coordinator's integer paths), mm8:N:M / mm16:N:M (LINALG multiply of an
+    M x N by an N x N matrix), mixed:COUNT:SEED (uneven lengths, one graph
+    launch)."""
     import numpy as np
     import torch
 
@@ -754,6 +756,18 @@ def run_case(args):
 
         def launch():
             d.exec_async(x, y, sp)
+    elif kind in ("mm8", "mm16"):  # mmB:N:M -- LINALG multiply of M x N by N x N
+        bits = int(kind[2:])
+        dt = F.FFTLIB_INT8 if bits == 8 else F.FFTLIB_INT16
+        tdt = torch.int8 if bits == 8 else torch.int16
+        nbytes = float(2 * n * batch + n * n) * (bits // 8)
+        a = torch.randint(-100, 100, (batch, n), dtype=torch.int64, device="cuda").to(tdt)
+        bm = torch.randint(-100, 100, (n, n), dtype=torch.int64, device="cuda").to(tdt)
+        c = torch.empty((batch, n), dtype=tdt, device="cuda")
+        mm = F.MatMul(batch, n, n, dt, shift=bits)
+
+        def launch():
+            mm.exec_async(a, bm, c, sp)
     elif kind == "mixed":  # mixed:COUNT:SEED -- the uneven-length batch, one graph launch
         lengths = np.sort(mixed_lengths(n, seed=batch))[::-1].copy()
         total = int(lengths.sum())
