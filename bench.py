@@ -161,6 +161,21 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of every rank's x (the job's time is its slowest rank's)."""
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: float, world: int, seconds_max: float) -> float:
+    """Whole-job throughput of weak-scaled replicas: the units all ranks
+    processed over the slowest rank's time."""
+    return units_per_rank * world / seconds_max
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -246,12 +261,10 @@ def our_arm(args, world, rank, local):
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, "cuda")
     ms_step = ms / args.steps
     per_gpu_gbs = algo_bytes(n, ch) / (ms_step * 1e-3) / 1e9
-    value = per_gpu_gbs * world
+    value = job_rate(algo_bytes(n, ch), world, ms_step * 1e-3) / 1e9
 
     if args.quick:  # profiling runs: the timed launches only
         if dist:
@@ -283,10 +296,8 @@ def our_arm(args, world, rank, local):
         F.check(kern(F.ptr(Xh), b, F.ptr(W), bw, F.ptr(Yh), b, n, ch, pb), "kernel (host)")
     e2e_s = time.perf_counter() - t0
     if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_gbs = algo_bytes(n, ch) * e2e_steps * world / e2e_s / 1e9
+        e2e_s = max_over_ranks(e2e_s, dist, "cuda")
+    e2e_gbs = job_rate(algo_bytes(n, ch) * e2e_steps, world, e2e_s) / 1e9
 
     if dist:
         dist.barrier()
