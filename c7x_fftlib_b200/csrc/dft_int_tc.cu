@@ -46,7 +46,9 @@ struct IntTc {
     static constexpr int LW = 8, EW = 8;
     static constexpr int MMA_WARP = LW + EW;
     static constexpr int THREADS = 32 * (MMA_WARP + 1);
-    static constexpr int RPW = TS / LW;  // super-rows per loader warp per tile
+    static constexpr int RPW = TS / LW;        // super-rows per loader warp per tile
+    static constexpr int CPG = TS / (EW / 4);  // columns (super-rows) per epilogue warp
+    static_assert(EW % 4 == 0 && CPG % 16 == 0, "epilogue partition");
     // 128-byte K-major rows (KMajor counts 16-bit units: 64 of them)
     using LA = KMajor<128, 64>;  // matrix limb: 128 output values x 128 input values
     using LB = KMajor<TS, 64>;   // data limb: TS super-rows x 128 input values
@@ -269,8 +271,8 @@ __global__ void __launch_bounds__(IntTc::THREADS, 1)
     } else {
         // ================= epilogue =================
         // thread = output value l of the super-rows of one half of the tile
-        const int et = threadIdx.x - 32 * S::LW;  // 0..255
-        const int q = warp & 3, ch = (warp - S::LW) >> 2;
+        const int et = threadIdx.x - 32 * S::LW;  // 0 .. 32 EW - 1
+        const int q = warp & 3, ch = (warp - S::LW) >> 2;  // lane quarter, column group
         const int l = 32 * q + lane;
         const uint32_t laneBase = (uint32_t)(32 * q) << 16;
         // sum x w = 2^16 hh + 2^8 mid + ll + cl - 2^15 rowsum, |sum x w| <= 2^37;
@@ -293,8 +295,8 @@ __global__ void __launch_bounds__(IntTc::THREADS, 1)
             const bool full = (uint64_t)(tile + 1) * TS * 128u <= comps;
             const uint32_t dbase = tmem + laneBase + (uint32_t)a * S::ACC;
 #pragma unroll
-            for (int cc = 0; cc < TS / 2; cc += 16) {
-                const int c0 = ch * (TS / 2) + cc;
+            for (int cc = 0; cc < S::CPG; cc += 16) {
+                const int c0 = ch * S::CPG + cc;
                 int32_t hh[16], mid[16], ll[16];
                 tmem_ld16_s32(dbase + (uint32_t)c0, hh);
                 tmem_ld16_s32(dbase + (uint32_t)(TS + c0), mid);
