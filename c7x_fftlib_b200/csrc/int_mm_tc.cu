@@ -15,7 +15,8 @@
 // A CTA computes 128 x BN tiles of C (BN = 128 for INT8, 64 for INT16) and
 // walks K in chunks of 128 values through a ring of shared-memory stages.
 // Roles (one persistent CTA per SM): 8 loader warps (HBM -> registers ->
-// K-major swizzled operands; B is transposed with byte permutes; INT16 also
+// swizzled operands, the next chunk's loads in flight while one is stored;
+// INT8 keeps B MN-major, INT16 transposes it with byte permutes and also
 // forms the offset limbs and the row and column sums), one warp that
 // allocates tensor memory and issues the MMAs, and 4 epilogue warps (tensor
 // memory lane = row of C -> shift, round, saturate -> HBM). Two accumulator
@@ -114,6 +115,21 @@ struct MmArgs {
     uint32_t* err;
 };
 
+// One chunk's global data of a loader thread, held in registers between its
+// loads and its conversion into the shared-memory operands.
+template <bool I16>
+struct RawChunk;
+template <>
+struct RawChunk<false> {
+    uint4 a[4];
+    uint4 bv[4];
+};
+template <>
+struct RawChunk<true> {
+    uint4 a[8];
+    uint32_t b[4][4];
+};
+
 template <bool I16>
 __global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
 {
@@ -147,172 +163,207 @@ __global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
 
     if (warp < S::LW) {
         // ================= loaders =================
+        // The CTA's chunks are walked as one sequence (tile-major); the global
+        // loads of chunk g + 1 are issued into registers before chunk g is
+        // converted and stored, so two chunks of loads are in flight.
         const int tid = threadIdx.x;  // 0..255
         int32_t* rowsum = reinterpret_cast<int32_t*>(sm + S::OFF_RS);
         int32_t* cpart = reinterpret_cast<int32_t*>(sm + S::OFF_CP);
         int32_t* colsum = reinterpret_cast<int32_t*>(sm + S::OFF_CS);
-        uint32_t g = 0, ti = 0;  // chunk counter, tile counter of this CTA
-        bool stop = false;
-        for (uint32_t tile = blockIdx.x; tile < p.numTiles && !stop; tile += gridDim.x, ++ti) {
-            const uint32_t m0 = (tile / p.tilesN) * 128u, n0 = (tile % p.tilesN) * (uint32_t)BN;
-            int32_t rs = 0, cs0 = 0, cs1 = 0;
-            for (uint32_t ch = 0; ch < p.chunks; ++ch, ++g) {
-                const int st = (int)(g % NS);
-                const uint32_t u = g / NS;
-                const uint32_t k0 = ch * 128u;
-                bool bad = false;
-                if (u >= 1 && tid == 0) bad = !tc_wait(&bars[S::EMPTY + st], (u - 1) & 1u, abortFlag, p.err);
-                if (group_sync_or(1, 32 * S::LW, bad)) {
-                    stop = true;
-                    break;
+        const uint32_t myTiles = blockIdx.x < p.numTiles ? (p.numTiles - 1u - blockIdx.x) / gridDim.x + 1u : 0u;
+        const uint32_t total = myTiles * p.chunks;
+        auto coords = [&](uint32_t gg, uint32_t& m0, uint32_t& n0, uint32_t& k0) {
+            const uint32_t ti = gg / p.chunks, ch = gg - ti * p.chunks;
+            const uint32_t tile = blockIdx.x + ti * gridDim.x;
+            m0 = (tile / p.tilesN) * 128u;
+            n0 = (tile % p.tilesN) * (uint32_t)BN;
+            k0 = ch * 128u;
+        };
+        RawChunk<I16> cur, nxt;
+        auto load = [&](uint32_t gg, RawChunk<I16>& R) {
+            uint32_t m0, n0, k0;
+            coords(gg, m0, n0, k0);
+            if constexpr (!I16) {
+                // A: 128 rows x 8 pieces of 16 bytes
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int it = tid + 256 * q;
+                    const int row = it >> 3, j = it & 7;
+                    const uint32_t m = m0 + row, k = k0 + 16u * j;
+                    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                    if (m < p.M) {
+                        const T* src = A + (size_t)m * p.lda + k;
+                        if (k + 16u <= p.K) {
+                            v = *reinterpret_cast<const uint4*>(src);
+                        } else {
+                            uint32_t wv[4] = {0u, 0u, 0u, 0u};
+                            for (int e = 0; e < 16; ++e)
+                                if (k + e < p.K) wv[e >> 2] |= (uint32_t)(uint8_t)src[e] << (8 * (e & 3));
+                            v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                        }
+                    }
+                    R.a[q] = v;
                 }
-                unsigned char* aHi = sm + st * S::STAGE;
-                unsigned char* bHi = aHi + S::A_LIMB;
-                if constexpr (!I16) {
-                    // A: 128 rows x 8 chunks of 16 bytes
+                // B: 128 K rows x 8 pieces of 16 bytes, kept MN-major (rows of n)
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int it = tid + 256 * q;
-                        const int row = it >> 3, j = it & 7;
-                        const uint32_t m = m0 + row, k = k0 + 16u * j;
-                        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-                        if (m < p.M) {
-                            const T* src = A + (size_t)m * p.lda + k;
-                            if (k + 16u <= p.K) {
-                                v = *reinterpret_cast<const uint4*>(src);
-                            } else {
-                                uint32_t wv[4] = {0u, 0u, 0u, 0u};
-                                for (int e = 0; e < 16; ++e)
-                                    if (k + e < p.K) wv[e >> 2] |= (uint32_t)(uint8_t)src[e] << (8 * (e & 3));
-                                v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
-                            }
-                        }
-                        *reinterpret_cast<uint4*>(aHi + S::LA::chunk(row, j)) = v;
-                    }
-                    // B: 32 x 32 blocks of 4 K rows x 4 columns, transposed
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int it = tid + 256 * q;
-                        const int kb = it >> 5, nb = it & 31;
-                        const uint32_t n = n0 + 4u * nb;
-                        uint32_t r[4];
-#pragma unroll
-                        for (int t = 0; t < 4; ++t) {
-                            const uint32_t k = k0 + 4u * kb + t;
-                            r[t] = 0u;
-                            if (k < p.K) {
-                                const T* src = B + (size_t)k * p.ldb + n;
-                                if (n + 4u <= p.N) {
-                                    r[t] = *reinterpret_cast<const uint32_t*>(src);
-                                } else {
-                                    for (int e = 0; e < 4; ++e)
-                                        if (n + e < p.N) r[t] |= (uint32_t)(uint8_t)src[e] << (8 * e);
-                                }
-                            }
-                        }
-                        const uint32_t t01l = __byte_perm(r[0], r[1], 0x5140u), t23l = __byte_perm(r[2], r[3], 0x5140u);
-                        const uint32_t t01h = __byte_perm(r[0], r[1], 0x7362u), t23h = __byte_perm(r[2], r[3], 0x7362u);
-                        const uint32_t col[4] = {__byte_perm(t01l, t23l, 0x5410u), __byte_perm(t01l, t23l, 0x7632u),
-                                                 __byte_perm(t01h, t23h, 0x5410u), __byte_perm(t01h, t23h, 0x7632u)};
-#pragma unroll
-                        for (int c = 0; c < 4; ++c)
-                            *reinterpret_cast<uint32_t*>(bHi + S::LB::chunk(4 * nb + c, kb >> 2) + (kb & 3) * 4) =
-                                col[c];
-                    }
-                } else {
-                    unsigned char* aLo = aHi + S::LIMB_PAIR;
-                    unsigned char* bLo = bHi + S::LIMB_PAIR;
-                    // A: row tid/2, half tid&1 of the chunk's 128 values, 8 units of 8 values
-                    {
-                        const int row = tid >> 1, h = tid & 1;
-                        const uint32_t m = m0 + row;
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int unit = 8 * h + j;  // values 8 unit .. 8 unit + 7
-                            const uint32_t k = k0 + 8u * unit;
-                            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-                            if (m < p.M) {
-                                const T* src = A + (size_t)m * p.lda + k;
-                                if (k + 8u <= p.K) {
-                                    v = *reinterpret_cast<const uint4*>(src);
-                                } else {
-                                    uint32_t wv[4] = {0u, 0u, 0u, 0u};
-                                    for (int e = 0; e < 8; ++e)
-                                        if (k + e < p.K) wv[e >> 1] |= (uint32_t)(uint16_t)src[e] << (16 * (e & 1));
-                                    v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
-                                }
-                            }
-                            const uint32_t a0 = v.x ^ 0x80008000u, a1 = v.y ^ 0x80008000u;
-                            const uint32_t a2 = v.z ^ 0x80008000u, a3 = v.w ^ 0x80008000u;
-                            const uint32_t h0 = __byte_perm(a0, a1, 0x7531u), h1 = __byte_perm(a2, a3, 0x7531u);
-                            const uint32_t l0 = __byte_perm(a0, a1, 0x6420u), l1 = __byte_perm(a2, a3, 0x6420u);
-                            rs += (int32_t)(256u * (__dp4a(h0, 0x01010101u, 0u) + __dp4a(h1, 0x01010101u, 0u)) +
-                                            __dp4a(l0, 0x01010101u, 0u) + __dp4a(l1, 0x01010101u, 0u));
-                            const uint32_t off = S::LA::chunk(row, unit >> 1) + (uint32_t)(unit & 1) * 8u;
-                            *reinterpret_cast<uint2*>(aHi + off) = make_uint2(h0, h1);
-                            *reinterpret_cast<uint2*>(aLo + off) = make_uint2(l0, l1);
+                for (int q = 0; q < 4; ++q) {
+                    const int it = tid + 256 * q;
+                    const int row = it >> 3, j = it & 7;
+                    const uint32_t k = k0 + row, n = n0 + 16u * j;
+                    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                    if (k < p.K) {
+                        const T* src = B + (size_t)k * p.ldb + n;
+                        if (n + 16u <= p.N) {
+                            v = *reinterpret_cast<const uint4*>(src);
+                        } else {
+                            uint32_t wv[4] = {0u, 0u, 0u, 0u};
+                            for (int e = 0; e < 16; ++e)
+                                if (n + e < p.N) wv[e >> 2] |= (uint32_t)(uint8_t)src[e] << (8 * (e & 3));
+                            v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
                         }
                     }
-                    // B: 32 x 32 blocks of 4 K rows x 2 columns; column pair nb = tid & 31
+                    R.bv[q] = v;
+                }
+            } else {
+                // A: row tid/2, half tid&1 of the chunk's 128 values, 8 pieces of 8 values
+                const int row = tid >> 1, h = tid & 1;
+                const uint32_t m = m0 + row;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int it = tid + 256 * q;
-                        const int kb = it >> 5, nb = it & 31;
-                        const uint32_t n = n0 + 2u * nb;
-                        uint32_t r[4];
-#pragma unroll
-                        for (int t = 0; t < 4; ++t) {
-                            const uint32_t k = k0 + 4u * kb + t;
-                            uint32_t wv = 0u;
-                            if (k < p.K) {
-                                const T* src = B + (size_t)k * p.ldb + n;
-                                if (n + 2u <= p.N) {
-                                    wv = *reinterpret_cast<const uint32_t*>(src);
-                                } else if (n < p.N) {
-                                    wv = (uint32_t)(uint16_t)src[0];
-                                }
-                            }
-                            r[t] = wv ^ 0x80008000u;
+                for (int j = 0; j < 8; ++j) {
+                    const uint32_t k = k0 + 8u * (uint32_t)(8 * h + j);
+                    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                    if (m < p.M) {
+                        const T* src = A + (size_t)m * p.lda + k;
+                        if (k + 8u <= p.K) {
+                            v = *reinterpret_cast<const uint4*>(src);
+                        } else {
+                            uint32_t wv[4] = {0u, 0u, 0u, 0u};
+                            for (int e = 0; e < 8; ++e)
+                                if (k + e < p.K) wv[e >> 1] |= (uint32_t)(uint16_t)src[e] << (16 * (e & 1));
+                            v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
                         }
-                        const uint32_t t01 = __byte_perm(r[0], r[1], 0x7351u), t23 = __byte_perm(r[2], r[3], 0x7351u);
-                        const uint32_t u01 = __byte_perm(r[0], r[1], 0x6240u), u23 = __byte_perm(r[2], r[3], 0x6240u);
-                        const uint32_t hiN0 = __byte_perm(t01, t23, 0x5410u), hiN1 = __byte_perm(t01, t23, 0x7632u);
-                        const uint32_t loN0 = __byte_perm(u01, u23, 0x5410u), loN1 = __byte_perm(u01, u23, 0x7632u);
-                        cs0 += (int32_t)(256u * __dp4a(hiN0, 0x01010101u, 0u) + __dp4a(loN0, 0x01010101u, 0u));
-                        cs1 += (int32_t)(256u * __dp4a(hiN1, 0x01010101u, 0u) + __dp4a(loN1, 0x01010101u, 0u));
-                        const uint32_t o0 = S::LB::chunk(2 * nb, kb >> 2) + (kb & 3) * 4;
-                        const uint32_t o1 = S::LB::chunk(2 * nb + 1, kb >> 2) + (kb & 3) * 4;
-                        *reinterpret_cast<uint32_t*>(bHi + o0) = hiN0;
-                        *reinterpret_cast<uint32_t*>(bHi + o1) = hiN1;
-                        *reinterpret_cast<uint32_t*>(bLo + o0) = loN0;
-                        *reinterpret_cast<uint32_t*>(bLo + o1) = loN1;
                     }
-                    if (ch + 1 == p.chunks) {
-                        // the tile's sums: rows from the two threads of a row,
-                        // columns from the 8 warps' partials
-                        const int slot = (int)(ti % RS);
-                        const int32_t rsum = rs + __shfl_xor_sync(0xffffffffu, rs, 1);
-                        if ((tid & 1) == 0) rowsum[slot * 128 + (tid >> 1)] = rsum;
-                        cpart[warp * BN + 2 * lane] = cs0;
-                        cpart[warp * BN + 2 * lane + 1] = cs1;
-                        group_sync(1, 32 * S::LW);
-                        if (tid < BN) {
-                            int32_t sum = 0;
+                    R.a[j] = v;
+                }
+                // B: 32 x 32 blocks of 4 K rows x 2 columns; column pair tid & 31
 #pragma unroll
-                            for (int w8 = 0; w8 < S::LW; ++w8) sum += cpart[w8 * BN + tid];
-                            colsum[slot * BN + tid] = sum;
+                for (int q = 0; q < 4; ++q) {
+                    const int it = tid + 256 * q;
+                    const int kb = it >> 5, nb = it & 31;
+                    const uint32_t n = n0 + 2u * nb;
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) {
+                        const uint32_t k = k0 + 4u * kb + t;
+                        uint32_t wv = 0u;
+                        if (k < p.K) {
+                            const T* src = B + (size_t)k * p.ldb + n;
+                            if (n + 2u <= p.N) {
+                                wv = *reinterpret_cast<const uint32_t*>(src);
+                            } else if (n < p.N) {
+                                wv = (uint32_t)(uint16_t)src[0];
+                            }
                         }
+                        R.b[q][t] = wv;
                     }
                 }
-                fence_proxy_async_smem();
-                group_sync(1, 32 * S::LW);
-                if (tid == 0) mbar_arrive(&bars[S::FULL + st]);
             }
+        };
+        int32_t rs = 0, cs0 = 0, cs1 = 0;  // INT16: this thread's row and column sums of the tile
+        auto store = [&](const RawChunk<I16>& R, int st) {
+            unsigned char* aHi = sm + st * S::STAGE;
+            unsigned char* bHi = aHi + S::A_LIMB;
+            if constexpr (!I16) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int it = tid + 256 * q;
+                    *reinterpret_cast<uint4*>(aHi + S::LA::chunk(it >> 3, it & 7)) = R.a[q];
+                }
+                // B MN-major: row k holds 128 bytes of n, in 16-byte pieces swizzled
+                // like the K-major rows (the canonical 128-byte-swizzle MN layout)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int it = tid + 256 * q;
+                    *reinterpret_cast<uint4*>(bHi + S::LB::chunk(it >> 3, it & 7)) = R.bv[q];
+                }
+            } else {
+                unsigned char* aLo = aHi + S::LIMB_PAIR;
+                unsigned char* bLo = bHi + S::LIMB_PAIR;
+                const int row = tid >> 1, h = tid & 1;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int unit = 8 * h + j;  // values 8 unit .. 8 unit + 7
+                    const uint4 v = R.a[j];
+                    const uint32_t a0 = v.x ^ 0x80008000u, a1 = v.y ^ 0x80008000u;
+                    const uint32_t a2 = v.z ^ 0x80008000u, a3 = v.w ^ 0x80008000u;
+                    const uint32_t h0 = __byte_perm(a0, a1, 0x7531u), h1 = __byte_perm(a2, a3, 0x7531u);
+                    const uint32_t l0 = __byte_perm(a0, a1, 0x6420u), l1 = __byte_perm(a2, a3, 0x6420u);
+                    rs += (int32_t)(256u * (__dp4a(h0, 0x01010101u, 0u) + __dp4a(h1, 0x01010101u, 0u)) +
+                                    __dp4a(l0, 0x01010101u, 0u) + __dp4a(l1, 0x01010101u, 0u));
+                    const uint32_t off = S::LA::chunk(row, unit >> 1) + (uint32_t)(unit & 1) * 8u;
+                    *reinterpret_cast<uint2*>(aHi + off) = make_uint2(h0, h1);
+                    *reinterpret_cast<uint2*>(aLo + off) = make_uint2(l0, l1);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int it = tid + 256 * q;
+                    const int kb = it >> 5, nb = it & 31;
+                    uint32_t r[4];
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) r[t] = R.b[q][t] ^ 0x80008000u;
+                    const uint32_t t01 = __byte_perm(r[0], r[1], 0x7351u), t23 = __byte_perm(r[2], r[3], 0x7351u);
+                    const uint32_t u01 = __byte_perm(r[0], r[1], 0x6240u), u23 = __byte_perm(r[2], r[3], 0x6240u);
+                    const uint32_t hiN0 = __byte_perm(t01, t23, 0x5410u), hiN1 = __byte_perm(t01, t23, 0x7632u);
+                    const uint32_t loN0 = __byte_perm(u01, u23, 0x5410u), loN1 = __byte_perm(u01, u23, 0x7632u);
+                    cs0 += (int32_t)(256u * __dp4a(hiN0, 0x01010101u, 0u) + __dp4a(loN0, 0x01010101u, 0u));
+                    cs1 += (int32_t)(256u * __dp4a(hiN1, 0x01010101u, 0u) + __dp4a(loN1, 0x01010101u, 0u));
+                    const uint32_t o0 = S::LB::chunk(2 * nb, kb >> 2) + (kb & 3) * 4;
+                    const uint32_t o1 = S::LB::chunk(2 * nb + 1, kb >> 2) + (kb & 3) * 4;
+                    *reinterpret_cast<uint32_t*>(bHi + o0) = hiN0;
+                    *reinterpret_cast<uint32_t*>(bHi + o1) = hiN1;
+                    *reinterpret_cast<uint32_t*>(bLo + o0) = loN0;
+                    *reinterpret_cast<uint32_t*>(bLo + o1) = loN1;
+                }
+            }
+        };
+        if (total > 0u) load(0u, cur);
+        for (uint32_t g = 0; g < total; ++g) {
+            const int st = (int)(g % NS);
+            const uint32_t u = g / NS;
+            const uint32_t ti = g / p.chunks, ch = g - ti * p.chunks;
+            if (g + 1u < total) load(g + 1u, nxt);
+            bool bad = false;
+            if (u >= 1 && tid == 0) bad = !tc_wait(&bars[S::EMPTY + st], (u - 1) & 1u, abortFlag, p.err);
+            if (group_sync_or(1, 32 * S::LW, bad)) break;
+            if (ch == 0u) rs = cs0 = cs1 = 0;
+            store(cur, st);
+            if constexpr (I16) {
+                if (ch + 1u == p.chunks) {
+                    // the tile's sums: rows from the two threads of a row,
+                    // columns from the 8 warps' partials
+                    const int slot = (int)(ti % RS);
+                    const int32_t rsum = rs + __shfl_xor_sync(0xffffffffu, rs, 1);
+                    if ((tid & 1) == 0) rowsum[slot * 128 + (tid >> 1)] = rsum;
+                    cpart[warp * BN + 2 * lane] = cs0;
+                    cpart[warp * BN + 2 * lane + 1] = cs1;
+                    group_sync(1, 32 * S::LW);
+                    if (tid < BN) {
+                        int32_t sum = 0;
+#pragma unroll
+                        for (int w8 = 0; w8 < S::LW; ++w8) sum += cpart[w8 * BN + tid];
+                        colsum[slot * BN + tid] = sum;
+                    }
+                }
+            }
+            fence_proxy_async_smem();
+            group_sync(1, 32 * S::LW);
+            if (tid == 0) mbar_arrive(&bars[S::FULL + st]);
+            cur = nxt;
         }
     } else if (warp == S::MMA_WARP) {
         // ================= MMA issue =================
         if (lane == 0) {
-            constexpr uint32_t idesc = umma_idesc_i8(BN, !I16);
+            // INT8: B is MN-major (bit 16 of the instruction descriptor)
+            constexpr uint32_t idesc = umma_idesc_i8(BN, !I16) | (I16 ? 0u : (1u << 16));
             constexpr int KS = 128 / 32;
             uint32_t g = 0, ti = 0;
             bool stop = false;
@@ -331,10 +382,11 @@ __global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
                     tc_fence_after();
                     const uint32_t aHi = sbase + st * S::STAGE, bHi = aHi + S::A_LIMB;
                     if constexpr (!I16) {
+                        // B MN-major: a K step of 32 rows is 4 atoms of 8 rows x 128 bytes
 #pragma unroll
                         for (int s = 0; s < KS; ++s)
-                            tc_mma_i8(d, S::LA::desc(aHi, 0, s), S::LB::desc(bHi, 0, s), idesc,
-                                      (ch > 0 || s > 0) ? 1u : 0u);
+                            tc_mma_i8(d, S::LA::desc(aHi, 0, s), umma_desc(bHi + 4096u * (uint32_t)s, 1024u, 2u),
+                                      idesc, (ch > 0 || s > 0) ? 1u : 0u);
                     } else {
                         const uint32_t aLo = aHi + S::LIMB_PAIR, bLo = bHi + S::LIMB_PAIR;
 #pragma unroll
@@ -489,7 +541,7 @@ bool int_mm_tc_supported(int bits, uint32_t M, uint32_t K, uint32_t N, const voi
 {
     if (!int_tensor_cores() || M == 0 || N == 0 || K == 0) return false;
     if (bits == 8)
-        return ((uintptr_t)a & 15u) == 0 && lda % 16u == 0 && ((uintptr_t)b & 3u) == 0 && ldb % 4u == 0;
+        return ((uintptr_t)a & 15u) == 0 && lda % 16u == 0 && ((uintptr_t)b & 15u) == 0 && ldb % 16u == 0;
     if (bits == 16)
         return K <= 16384u && ((uintptr_t)a & 15u) == 0 && lda % 8u == 0 && ((uintptr_t)b & 3u) == 0 &&
                ldb % 2u == 0;
