@@ -59,9 +59,9 @@ void int_dft_w1_host(int bits, uint32_t n, void* out);
 bool int16_tc_supported(uint32_t n2, const void* x, const void* y);
 cudaError_t launch_int16_tc(const int16_t* x, int16_t* y, const int16_t* w, uint32_t n2, uint32_t ld, uint32_t rows,
                             uint32_t shift, cudaStream_t s);
-// The LINALG multiply on the tensor cores (int_mm_tc.cu): INT8 with A and B
-// rows 16-byte aligned; INT16 with A rows 16-byte and B rows 4-byte aligned
-// and K <= 16384. The same bits as the CUDA-core kernel.
+// The LINALG multiply on the tensor cores (int_mm_tc.cu): A and B rows
+// 16-byte aligned; INT16 also K <= 16384. The same bits as the CUDA-core
+// kernel.
 bool int_mm_tc_supported(int bits, uint32_t M, uint32_t K, uint32_t N, const void* a, size_t lda, const void* b,
                          size_t ldb);
 cudaError_t launch_int_mm_tc(int bits, uint32_t M, uint32_t K, uint32_t N, const void* a, size_t lda, const void* b,

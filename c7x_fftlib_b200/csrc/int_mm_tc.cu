@@ -16,8 +16,8 @@
 // walks K in chunks of 128 values through a ring of shared-memory stages.
 // Roles (one persistent CTA per SM): 8 loader warps (HBM -> registers ->
 // swizzled operands, the next chunk's loads in flight while one is stored;
-// INT8 keeps B MN-major, INT16 transposes it with byte permutes and also
-// forms the offset limbs and the row and column sums), one warp that
+// A K-major, B MN-major as it lies in memory; INT16 also forms the offset
+// limbs and the row and column sums), one warp that
 // allocates tensor memory and issues the MMAs, and 4 epilogue warps (tensor
 // memory lane = row of C -> shift, round, saturate -> HBM). Two accumulator
 // buffers let the epilogue of one tile overlap the MMAs of the next. Every
@@ -47,7 +47,8 @@ struct MmTc {
     static constexpr int KC = 128;  // K values per chunk
     static constexpr int LIMBS = I16 ? 2 : 1;
     using LA = KMajor<128, 64>;  // 128 rows of 128 bytes
-    using LB = KMajor<BN, 64>;   // BN rows of 128 bytes
+    using LB = KMajor<BN, 64>;   // INT8 B, MN-major: 128 K rows of 128 bytes (BN = 128)
+    using LBM = KMajor<128, 32>;  // INT16 B limb, MN-major: 128 K rows of 64 bytes (BN = 64)
     static constexpr uint32_t A_LIMB = LA::BYTES;
     static constexpr uint32_t B_LIMB = LB::BYTES;
     static constexpr uint32_t LIMB_PAIR = A_LIMB + B_LIMB;  // A limb then B limb
@@ -127,7 +128,7 @@ struct RawChunk<false> {
 template <>
 struct RawChunk<true> {
     uint4 a[8];
-    uint32_t b[4][4];
+    uint4 bv[4];
 };
 
 template <bool I16>
@@ -245,30 +246,30 @@ __global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
                     }
                     R.a[j] = v;
                 }
-                // B: 32 x 32 blocks of 4 K rows x 2 columns; column pair tid & 31
+                // B: 128 K rows x 8 pieces of 8 values, kept MN-major (rows of n);
+                // a thread's pieces are always columns 8 (tid & 7) .. + 7
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int it = tid + 256 * q;
-                    const int kb = it >> 5, nb = it & 31;
-                    const uint32_t n = n0 + 2u * nb;
-#pragma unroll
-                    for (int t = 0; t < 4; ++t) {
-                        const uint32_t k = k0 + 4u * kb + t;
-                        uint32_t wv = 0u;
-                        if (k < p.K) {
-                            const T* src = B + (size_t)k * p.ldb + n;
-                            if (n + 2u <= p.N) {
-                                wv = *reinterpret_cast<const uint32_t*>(src);
-                            } else if (n < p.N) {
-                                wv = (uint32_t)(uint16_t)src[0];
-                            }
+                    const int row = it >> 3, j = it & 7;
+                    const uint32_t k = k0 + row, n = n0 + 8u * j;
+                    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                    if (k < p.K) {
+                        const T* src = B + (size_t)k * p.ldb + n;
+                        if (n + 8u <= p.N) {
+                            v = *reinterpret_cast<const uint4*>(src);
+                        } else {
+                            uint32_t wv[4] = {0u, 0u, 0u, 0u};
+                            for (int e = 0; e < 8; ++e)
+                                if (n + e < p.N) wv[e >> 1] |= (uint32_t)(uint16_t)src[e] << (16 * (e & 1));
+                            v = make_uint4(wv[0], wv[1], wv[2], wv[3]);
                         }
-                        R.b[q][t] = wv;
                     }
+                    R.bv[q] = v;
                 }
             }
         };
-        int32_t rs = 0, cs0 = 0, cs1 = 0;  // INT16: this thread's row and column sums of the tile
+        int32_t rs = 0, cs[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // INT16: this thread's row and column sums of the tile
         auto store = [&](const RawChunk<I16>& R, int st) {
             unsigned char* aHi = sm + st * S::STAGE;
             unsigned char* bHi = aHi + S::A_LIMB;
@@ -303,25 +304,24 @@ __global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
                     *reinterpret_cast<uint2*>(aHi + off) = make_uint2(h0, h1);
                     *reinterpret_cast<uint2*>(aLo + off) = make_uint2(l0, l1);
                 }
+                // B MN-major: limb row k holds 64 bytes of n (64-byte swizzle)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int it = tid + 256 * q;
-                    const int kb = it >> 5, nb = it & 31;
-                    uint32_t r[4];
+                    const int row = it >> 3, j = it & 7;
+                    const uint4 v = R.bv[q];
+                    const uint32_t w[4] = {v.x ^ 0x80008000u, v.y ^ 0x80008000u, v.z ^ 0x80008000u,
+                                           v.w ^ 0x80008000u};
 #pragma unroll
-                    for (int t = 0; t < 4; ++t) r[t] = R.b[q][t] ^ 0x80008000u;
-                    const uint32_t t01 = __byte_perm(r[0], r[1], 0x7351u), t23 = __byte_perm(r[2], r[3], 0x7351u);
-                    const uint32_t u01 = __byte_perm(r[0], r[1], 0x6240u), u23 = __byte_perm(r[2], r[3], 0x6240u);
-                    const uint32_t hiN0 = __byte_perm(t01, t23, 0x5410u), hiN1 = __byte_perm(t01, t23, 0x7632u);
-                    const uint32_t loN0 = __byte_perm(u01, u23, 0x5410u), loN1 = __byte_perm(u01, u23, 0x7632u);
-                    cs0 += (int32_t)(256u * __dp4a(hiN0, 0x01010101u, 0u) + __dp4a(loN0, 0x01010101u, 0u));
-                    cs1 += (int32_t)(256u * __dp4a(hiN1, 0x01010101u, 0u) + __dp4a(loN1, 0x01010101u, 0u));
-                    const uint32_t o0 = S::LB::chunk(2 * nb, kb >> 2) + (kb & 3) * 4;
-                    const uint32_t o1 = S::LB::chunk(2 * nb + 1, kb >> 2) + (kb & 3) * 4;
-                    *reinterpret_cast<uint32_t*>(bHi + o0) = hiN0;
-                    *reinterpret_cast<uint32_t*>(bHi + o1) = hiN1;
-                    *reinterpret_cast<uint32_t*>(bLo + o0) = loN0;
-                    *reinterpret_cast<uint32_t*>(bLo + o1) = loN1;
+                    for (int e = 0; e < 4; ++e) {
+                        cs[2 * e] += (int32_t)(w[e] & 0xFFFFu);
+                        cs[2 * e + 1] += (int32_t)(w[e] >> 16);
+                    }
+                    const uint32_t h0 = __byte_perm(w[0], w[1], 0x7531u), h1 = __byte_perm(w[2], w[3], 0x7531u);
+                    const uint32_t l0 = __byte_perm(w[0], w[1], 0x6420u), l1 = __byte_perm(w[2], w[3], 0x6420u);
+                    const uint32_t off = S::LBM::chunk(row, j >> 1) + (uint32_t)(j & 1) * 8u;
+                    *reinterpret_cast<uint2*>(bHi + off) = make_uint2(h0, h1);
+                    *reinterpret_cast<uint2*>(bLo + off) = make_uint2(l0, l1);
                 }
             }
         };
@@ -334,7 +334,11 @@ __global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
             bool bad = false;
             if (u >= 1 && tid == 0) bad = !tc_wait(&bars[S::EMPTY + st], (u - 1) & 1u, abortFlag, p.err);
             if (group_sync_or(1, 32 * S::LW, bad)) break;
-            if (ch == 0u) rs = cs0 = cs1 = 0;
+            if (ch == 0u) {
+                rs = 0;
+#pragma unroll
+                for (int e = 0; e < 8; ++e) cs[e] = 0;
+            }
             store(cur, st);
             if constexpr (I16) {
                 if (ch + 1u == p.chunks) {
@@ -343,8 +347,16 @@ __global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
                     const int slot = (int)(ti % RS);
                     const int32_t rsum = rs + __shfl_xor_sync(0xffffffffu, rs, 1);
                     if ((tid & 1) == 0) rowsum[slot * 128 + (tid >> 1)] = rsum;
-                    cpart[warp * BN + 2 * lane] = cs0;
-                    cpart[warp * BN + 2 * lane + 1] = cs1;
+                    // lanes l, l ^ 8, l ^ 16, l ^ 24 hold the same 8 columns
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        cs[e] += __shfl_xor_sync(0xffffffffu, cs[e], 8);
+                        cs[e] += __shfl_xor_sync(0xffffffffu, cs[e], 16);
+                    }
+                    if (lane < 8) {
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) cpart[warp * BN + 8 * lane + e] = cs[e];
+                    }
                     group_sync(1, 32 * S::LW);
                     if (tid < BN) {
                         int32_t sum = 0;
@@ -362,8 +374,14 @@ __global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
     } else if (warp == S::MMA_WARP) {
         // ================= MMA issue =================
         if (lane == 0) {
-            // INT8: B is MN-major (bit 16 of the instruction descriptor)
-            constexpr uint32_t idesc = umma_idesc_i8(BN, !I16) | (I16 ? 0u : (1u << 16));
+            // B is MN-major (bit 16 of the instruction descriptor)
+            constexpr uint32_t idesc = umma_idesc_i8(BN, !I16) | (1u << 16);
+            // MN-major B, K step of 32 rows: INT8 4 atoms of 8 rows x 128 bytes
+            // (128-byte swizzle), INT16 limbs 4 atoms of 8 rows x 64 bytes (64-byte swizzle)
+            auto bdesc = [](uint32_t base, int s) {
+                return I16 ? umma_desc(base + 2048u * (uint32_t)s, 512u, 4u)
+                           : umma_desc(base + 4096u * (uint32_t)s, 1024u, 2u);
+            };
             constexpr int KS = 128 / 32;
             uint32_t g = 0, ti = 0;
             bool stop = false;
@@ -382,27 +400,25 @@ __global__ void __launch_bounds__(MmTc<I16>::THREADS, 1) k_int_mm_tc(MmArgs p)
                     tc_fence_after();
                     const uint32_t aHi = sbase + st * S::STAGE, bHi = aHi + S::A_LIMB;
                     if constexpr (!I16) {
-                        // B MN-major: a K step of 32 rows is 4 atoms of 8 rows x 128 bytes
 #pragma unroll
                         for (int s = 0; s < KS; ++s)
-                            tc_mma_i8(d, S::LA::desc(aHi, 0, s), umma_desc(bHi + 4096u * (uint32_t)s, 1024u, 2u),
-                                      idesc, (ch > 0 || s > 0) ? 1u : 0u);
+                            tc_mma_i8(d, S::LA::desc(aHi, 0, s), bdesc(bHi, s), idesc, (ch > 0 || s > 0) ? 1u : 0u);
                     } else {
                         const uint32_t aLo = aHi + S::LIMB_PAIR, bLo = bHi + S::LIMB_PAIR;
 #pragma unroll
                         for (int s = 0; s < KS; ++s)
-                            tc_mma_i8(d, S::LA::desc(aHi, 0, s), S::LB::desc(bHi, 0, s), idesc,
+                            tc_mma_i8(d, S::LA::desc(aHi, 0, s), bdesc(bHi, s), idesc,
                                       (ch > 0 || s > 0) ? 1u : 0u);
 #pragma unroll
                         for (int s = 0; s < KS; ++s)
-                            tc_mma_i8(d + BN, S::LA::desc(aHi, 0, s), S::LB::desc(bLo, 0, s), idesc,
+                            tc_mma_i8(d + BN, S::LA::desc(aHi, 0, s), bdesc(bLo, s), idesc,
                                       (ch > 0 || s > 0) ? 1u : 0u);
 #pragma unroll
                         for (int s = 0; s < KS; ++s)
-                            tc_mma_i8(d + BN, S::LA::desc(aLo, 0, s), S::LB::desc(bHi, 0, s), idesc, 1u);
+                            tc_mma_i8(d + BN, S::LA::desc(aLo, 0, s), bdesc(bHi, s), idesc, 1u);
 #pragma unroll
                         for (int s = 0; s < KS; ++s)
-                            tc_mma_i8(d + 2 * BN, S::LA::desc(aLo, 0, s), S::LB::desc(bLo, 0, s), idesc,
+                            tc_mma_i8(d + 2 * BN, S::LA::desc(aLo, 0, s), bdesc(bLo, s), idesc,
                                       (ch > 0 || s > 0) ? 1u : 0u);
                     }
                     tc_commit(&bars[S::EMPTY + st]);
@@ -543,8 +559,8 @@ bool int_mm_tc_supported(int bits, uint32_t M, uint32_t K, uint32_t N, const voi
     if (bits == 8)
         return ((uintptr_t)a & 15u) == 0 && lda % 16u == 0 && ((uintptr_t)b & 15u) == 0 && ldb % 16u == 0;
     if (bits == 16)
-        return K <= 16384u && ((uintptr_t)a & 15u) == 0 && lda % 8u == 0 && ((uintptr_t)b & 3u) == 0 &&
-               ldb % 2u == 0;
+        return K <= 16384u && ((uintptr_t)a & 15u) == 0 && lda % 8u == 0 && ((uintptr_t)b & 15u) == 0 &&
+               ldb % 8u == 0;
     return false;
 }
 

@@ -104,8 +104,8 @@ def test_overlapping_source_rows(torch_cuda):
                                                (64, 1000, 200, 1008, 200, 203), (64, 1000, 200, 1008, 208, 203),
                                                (1, 16, 4, 16, 4, 4), (1, 16, 4, 16, 16, 4)])
 def test_tensor_core_and_cuda_core_agree(torch_cuda, bits, m, k, n, lda, ldb, ldc):
-    """The tensor-core multiply (rows of A 16-byte aligned; of B 16-byte
-    aligned for INT8, 4-byte for INT16) against the CUDA-core kernel on the same full-range data, ragged
+    """The tensor-core multiply (rows of A and B 16-byte aligned) against the
+    CUDA-core kernel on the same full-range data, ragged
     tiles and K chunks included, and against the oracle."""
     torch = torch_cuda
     L = F.lib()
