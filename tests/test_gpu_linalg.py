@@ -102,9 +102,12 @@ def test_overlapping_source_rows(torch_cuda):
                                                (300, 100, 70, 112, 80, 70), (129, 257, 65, 272, 68, 80),
                                                (129, 257, 65, 272, 80, 80), (1000, 64, 64, 64, 64, 64),
                                                (64, 1000, 200, 1008, 200, 203), (64, 1000, 200, 1008, 208, 203),
-                                               (1, 16, 4, 16, 4, 4), (1, 16, 4, 16, 16, 4)])
+                                               (1, 16, 4, 16, 4, 4), (1, 16, 4, 16, 16, 4),
+                                               (300, 200, 130, 208, 144, 133), (129, 129, 129, 144, 144, 129),
+                                               (520, 384, 256, 384, 256, 256)])
 def test_tensor_core_and_cuda_core_agree(torch_cuda, bits, m, k, n, lda, ldb, ldc):
-    """The tensor-core multiply (rows of A and B 16-byte aligned) against the
+    """The tensor-core multiplies (rows of A and B 16-byte aligned; INT8 with
+    N and K of a full tile or more through the bulk tensor copies) against the
     CUDA-core kernel on the same full-range data, ragged
     tiles and K chunks included, and against the oracle."""
     torch = torch_cuda
