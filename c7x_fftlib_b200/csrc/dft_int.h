@@ -71,6 +71,10 @@ cudaError_t launch_int_mm_tc(int bits, uint32_t M, uint32_t K, uint32_t N, const
 // (16-byte aligned, non-overlapping rows) do not hold.
 cudaError_t launch_int8_mm_tma(uint32_t M, uint32_t K, uint32_t N, const void* a, size_t lda, const void* b,
                                size_t ldb, void* c, size_t ldc, uint32_t shift, cudaStream_t s);
+// The INT16 multiply with its raw tiles copied by the Tensor Memory
+// Accelerator and converted to byte limbs in shared memory (K <= 16384).
+cudaError_t launch_int16_mm_tma(uint32_t M, uint32_t K, uint32_t N, const void* a, size_t lda, const void* b,
+                                size_t ldb, void* c, size_t ldc, uint32_t shift, cudaStream_t s);
 // Whether the integer products use the tensor cores when they can (default
 // on; the CUDA-core kernels give the same bits).
 void int_set_tensor_cores(bool on);

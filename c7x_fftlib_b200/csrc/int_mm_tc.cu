@@ -578,11 +578,15 @@ cudaError_t launch_int_mm_tc(int bits, uint32_t M, uint32_t K, uint32_t N, const
     p.K = K;
     p.N = N;
     p.shift = shift;
-    // whole 128 x 128-byte tiles: the bulk tensor copies; narrow products
-    // (N or K below one tile, e.g. 2^20 x 64 x 64) are faster with the loader
-    // warps, which keep more rows in flight per tile
+    // whole tiles: the bulk tensor copies; narrow products (N or K below one
+    // tile, e.g. 2^20 x 64 x 64 INT8) are faster with the loader warps, which
+    // keep more rows in flight per tile
     if (bits == 8 && K >= 128u && N >= 128u) {
         const cudaError_t e = launch_int8_mm_tma(M, K, N, a, lda, b, ldb, c, ldc, shift, s);
+        if (e != cudaErrorNotSupported) return e;
+    }
+    if (bits == 16 && K >= 128u && N >= 64u) {
+        const cudaError_t e = launch_int16_mm_tma(M, K, N, a, lda, b, ldb, c, ldc, shift, s);
         if (e != cudaErrorNotSupported) return e;
     }
     return bits == 16 ? launch_mm_tc<true>(p, s) : launch_mm_tc<false>(p, s);
