@@ -19,13 +19,14 @@
 // a super-row with one store. The zero entries of the block-diagonal matrix
 // are offset like the others, which the correction term accounts for.
 //
-// Roles per CTA (one persistent CTA per SM): 8 loader warps (HBM -> offset
-// bytes -> swizzled K-major shared memory, and the super-row sums), 8
-// epilogue warps (three accumulators -> 64-bit combination -> shift, round,
-// saturate -> HBM) and one warp that allocates tensor memory and issues the
-// 16 MMAs of a tile. Four operand buffers in shared memory and two
-// accumulator buffers in tensor memory (3 x 64 columns each); the next tile
-// of the CTA is prefetched into L2. Every wait is bounded and a wait that
+// Roles per CTA (one persistent CTA per SM): one thread bulk-copies each
+// tile's raw values (64 contiguous super-rows) into a ring of three raw
+// stages; 8 loader warps (raw stage -> offset bytes -> swizzled K-major
+// shared memory, and the super-row sums); 8 epilogue warps (three
+// accumulators -> 64-bit combination -> shift, round, saturate -> HBM); one
+// warp that allocates tensor memory and issues the 16 MMAs of a tile. Four
+// operand buffers in shared memory and two accumulator buffers in tensor
+// memory (3 x 64 columns each). Every wait is bounded and a wait that
 // gives up sets kErrTcTimeout in the launch's error word.
 #include <mutex>
 
@@ -43,9 +44,10 @@ struct IntTc {
     static constexpr int NB = 4;   // operand tile buffers (shared memory)
     static constexpr int NA = 2;   // accumulator buffers (tensor memory)
     static constexpr int RS = 8;   // super-row sum slots: a slot is rewritten NB + NA tiles after its epilogue
+    static constexpr int NR = 3;   // raw tile stages (bulk copies of 64 super-rows)
     static constexpr int LW = 8, EW = 8;
-    static constexpr int MMA_WARP = LW + EW;
-    static constexpr int THREADS = 32 * (MMA_WARP + 1);
+    static constexpr int MMA_WARP = LW + EW, COPY_WARP = MMA_WARP + 1;
+    static constexpr int THREADS = 32 * (COPY_WARP + 1);
     static constexpr int RPW = TS / LW;        // super-rows per loader warp per tile
     static constexpr int CPG = TS / (EW / 4);  // columns (super-rows) per epilogue warp
     static_assert(EW % 4 == 0 && CPG % 16 == 0, "epilogue partition");
@@ -56,16 +58,19 @@ struct IntTc {
     static constexpr uint32_t X_LIMB = LB::BYTES;  // 8 KB
     static constexpr uint32_t TILE = 2 * X_LIMB;
     static constexpr uint32_t OFF_W = NB * TILE;
-    static constexpr uint32_t OFF_CS = OFF_W + 2 * W_LIMB;  // 128 column sums of the offset matrix
+    static constexpr uint32_t RAWB = (uint32_t)TS * 128u * 2u;  // 16 KB of raw INT16 values
+    static constexpr uint32_t OFF_RAW = OFF_W + 2 * W_LIMB;
+    static constexpr uint32_t OFF_CS = OFF_RAW + NR * RAWB;  // 128 column sums of the offset matrix
     static constexpr uint32_t OFF_RS = OFF_CS + 4u * 128u;  // RS x TS super-row sums
     static constexpr uint32_t OFF_BAR = (OFF_RS + 4u * RS * TS + 7u) & ~7u;
-    static constexpr int NBARS = 2 * NB + 2 * NA + 1;
+    static constexpr int NBARS = 2 * NB + 2 * NA + 1 + 2 * NR;
     static constexpr uint32_t OFF_MISC = OFF_BAR + 8u * NBARS;
     static constexpr uint32_t SMEM = OFF_MISC + 16u + 1024u;
     static constexpr uint32_t ACC = 3 * TS;  // hh, mid, ll columns of one buffer
     static constexpr uint32_t TMEM_COLS = 512;
     // A_FULL/S_FREE per operand buffer, D_FULL/D_FREE per accumulator buffer
-    static constexpr int A_FULL = 0, S_FREE = NB, D_FULL = 2 * NB, D_FREE = 2 * NB + NA, DRAIN = 2 * NB + 2 * NA;
+    static constexpr int A_FULL = 0, S_FREE = NB, D_FULL = 2 * NB, D_FREE = 2 * NB + NA, DRAIN = 2 * NB + 2 * NA,
+                         R_FULL = DRAIN + 1, R_EMPTY = R_FULL + NR;
     static_assert(NA * ACC <= TMEM_COLS, "tensor memory");
     static_assert(RS >= NB + NA, "super-row sum slots");
     static_assert(SMEM <= 227u * 1024u, "shared memory per CTA");
@@ -109,13 +114,24 @@ FFT_DEV void tmem_ld16_s32(uint32_t taddr, int32_t (&v)[16])
 }
 
 // w entry (k, l) of the block-diagonal 128 x 128 matrix built from the 2N x 2N
-// table (row stride ld), plus the 32768 offset.
-__device__ __forceinline__ uint32_t offset_entry(const int16_t* __restrict__ w, uint32_t n2, uint32_t ld, int k,
+// table (row stride ld), plus the 32768 offset; n2 = 2^lg divides 128.
+__device__ __forceinline__ uint32_t offset_entry(const int16_t* __restrict__ w, uint32_t lg, uint32_t ld, int k,
                                                  int l)
 {
+    const uint32_t mask = (1u << lg) - 1u;
     int32_t v = 0;
-    if ((uint32_t)k / n2 == (uint32_t)l / n2) v = w[(size_t)((uint32_t)k % n2) * ld + (uint32_t)l % n2];
+    if (((uint32_t)k >> lg) == ((uint32_t)l >> lg)) v = w[(size_t)((uint32_t)k & mask) * ld + ((uint32_t)l & mask)];
     return (uint32_t)(v + 32768);
+}
+
+// Bytes of a tile's raw values that the bulk copy brings in: a multiple of
+// 16 from a 16-byte aligned start (the copy's rules); the loaders read any
+// rest straight from global memory.
+__device__ __forceinline__ uint32_t raw_bytes(const int16_t* x, uint64_t base, uint64_t comps)
+{
+    if ((((uintptr_t)(x + base)) & 15u) != 0u) return 0u;
+    const uint64_t cnt = min((uint64_t)IntTc::TS * 128u, comps - base);
+    return (uint32_t)(cnt * 2u) & ~15u;
 }
 
 __global__ void __launch_bounds__(IntTc::THREADS, 1)
@@ -133,6 +149,7 @@ __global__ void __launch_bounds__(IntTc::THREADS, 1)
     int32_t* colsum = reinterpret_cast<int32_t*>(sm + S::OFF_CS);
     int32_t* rowsum = reinterpret_cast<int32_t*>(sm + S::OFF_RS);
 
+    const uint32_t lg = (uint32_t)(__ffs((int)n2) - 1);  // n2 is a power of two
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t superRows = (comps + 127u) / 128u;
     const uint32_t numTiles = (uint32_t)((superRows + TS - 1) / TS);
@@ -156,7 +173,7 @@ __global__ void __launch_bounds__(IntTc::THREADS, 1)
             uint32_t h[4] = {0u, 0u, 0u, 0u}, q[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
             for (int e = 0; e < 16; ++e) {
-                const uint32_t u = offset_entry(w, n2, ld, 16 * j + e, l);
+                const uint32_t u = offset_entry(w, lg, ld, 16 * j + e, l);
                 h[e >> 2] |= (u >> 8) << (8 * (e & 3));
                 q[e >> 2] |= (u & 255u) << (8 * (e & 3));
             }
@@ -164,9 +181,11 @@ __global__ void __launch_bounds__(IntTc::THREADS, 1)
             *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
             *reinterpret_cast<uint4*>(lo + off) = make_uint4(q[0], q[1], q[2], q[3]);
         }
+        // column l of the offset matrix: its block's n2 table entries plus
+        // 32768 for each of the 128 rows
         for (int l = threadIdx.x; l < 128; l += blockDim.x) {
-            int32_t s = 0;
-            for (int k = 0; k < 128; ++k) s += (int32_t)offset_entry(w, n2, ld, k, l);
+            int32_t s = 128 * 32768;
+            for (uint32_t k = 0; k < n2; ++k) s += (int32_t)w[(size_t)k * ld + ((uint32_t)l & (n2 - 1u))];
             colsum[l] = s;
         }
     }
@@ -181,26 +200,24 @@ __global__ void __launch_bounds__(IntTc::THREADS, 1)
         // lane l holds values 4l .. 4l+3 of a super-row (8 bytes); the next
         // tile of this CTA is pulled into L2 while this one is converted
         const int j = threadIdx.x;
-        auto prefetch = [&](uint32_t tl) {
-            if (j != 0 || tl >= numTiles) return;
-            const uint64_t first = (uint64_t)tl * TS * 128u;
-            const uint64_t cnt = min((uint64_t)TS * 128u, comps - first);
-            if ((((uintptr_t)(x + first)) & 15u) != 0 || (cnt * 2u) % 16u != 0) return;
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(x + first), "r"((uint32_t)(cnt * 2u))
-                         : "memory");
-        };
-        prefetch(blockIdx.x);
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
-            prefetch(tile + gridDim.x);
-            const int b = (int)(i % NB);
-            const uint32_t u = i / NB, slot = i % RS;
+            const int b = (int)(i % NB), rr = (int)(i % S::NR);
+            const uint32_t u = i / NB, ur = i / S::NR, slot = i % RS;
             const uint64_t base = (uint64_t)tile * TS * 128u;
+            const uint32_t have = raw_bytes(x, base, comps) / 2u;  // values in the raw stage
+            const unsigned char* raw = sm + S::OFF_RAW + rr * S::RAWB;
+            bool badr = false;
+            if (j == 0) badr = !tc_wait(&bars[S::R_FULL + rr], ur & 1u, abortFlag, err);
+            if (group_sync_or(1, 32 * S::LW, badr)) break;
             uint2 v[S::RPW];
 #pragma unroll
             for (int k = 0; k < S::RPW; ++k) {
-                const uint64_t e0 = base + (uint64_t)(warp * S::RPW + k) * 128u + 4u * lane;
-                if (e0 + 4u <= comps) {
+                const uint32_t o = (uint32_t)(warp * S::RPW + k) * 128u + 4u * lane;  // value offset in the tile
+                const uint64_t e0 = base + o;
+                if (o + 4u <= have) {
+                    v[k] = *reinterpret_cast<const uint2*>(raw + 2u * o);
+                } else if (e0 + 4u <= comps) {
                     v[k] = *reinterpret_cast<const uint2*>(x + e0);
                 } else {
                     uint16_t t[4];
@@ -232,8 +249,31 @@ __global__ void __launch_bounds__(IntTc::THREADS, 1)
             }
             fence_proxy_async_smem();
             group_sync(1, 32 * S::LW);
-            if (j == 0) mbar_arrive(&bars[S::A_FULL + b]);
+            if (j == 0) {
+                mbar_arrive(&bars[S::A_FULL + b]);
+                mbar_arrive(&bars[S::R_EMPTY + rr]);
+            }
         }
+    } else if (warp == S::COPY_WARP) {
+        // ================= raw tile copies =================
+        if (lane == 0) {
+            uint32_t i = 0;
+            for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
+                const int rr = (int)(i % S::NR);
+                const uint32_t ur = i / S::NR;
+                if (ur >= 1 && !tc_wait(&bars[S::R_EMPTY + rr], (ur - 1) & 1u, abortFlag, err)) break;
+                const uint64_t base = (uint64_t)tile * TS * 128u;
+                const uint32_t bytes = raw_bytes(x, base, comps);
+                mbar_expect_tx(&bars[S::R_FULL + rr], bytes);
+                if (bytes) bulk_copy_g2s(sm + S::OFF_RAW + rr * S::RAWB, x + base, bytes, &bars[S::R_FULL + rr]);
+            }
+            // the copies still in flight land before the CTA ends
+            for (int rr = 0; rr < S::NR; ++rr) {
+                const uint32_t armed = i > (uint32_t)rr ? (i - 1u - (uint32_t)rr) / S::NR + 1u : 0u;
+                if (armed) mbar_wait_bounded(&bars[S::R_FULL + rr], (armed - 1u) & 1u);
+            }
+        }
+        __syncwarp();
     } else if (warp == S::MMA_WARP) {
         // ================= MMA issue =================
         if (lane == 0) {
