@@ -679,10 +679,13 @@ def cpu_baseline():
         return None
     sample = 512
     threads = O.host_threads()
-    t, used = O.time_reference_c2c(N_POINTS, sample, threads, reps=3)
+    t, used = O.time_reference_c2c(N_POINTS, sample, threads, reps=5)
+    t1, _ = O.time_reference_c2c(N_POINTS, 64, 1, reps=5)
     return {"value": round(algo_bytes(N_POINTS, sample) / t / 1e9, 4), "unit": "GB/s", "cores": used,
             "kind": "reference",
-            "sample": f"{sample} channels of N={N_POINTS}, median of 3, reference _cn (gcc -O3), one thread per core"}
+            "single_thread_value": round(algo_bytes(N_POINTS, 64) / t1 / 1e9, 4),
+            "sample": f"{sample} channels of N={N_POINTS}, median of 5, reference _cn (gcc -O3), one thread per "
+                      f"core; single_thread_value: 64 channels on one thread, median of 5"}
 
 
 def run_case(args):
