@@ -407,12 +407,25 @@ cudaError_t launch_typed(int v, uint32_t n, uint32_t batch, uint32_t interleave,
     const int planar = interleave ? 0 : 1;
     const T* tw = w;
     uint32_t len = n, rad = d0;
+    // INT16 radix-16 stages and the final stage of interleaved rows run on the
+    // tensor cores (dft_int_hr_tc.cu), the rest on the CUDA cores
+    bool tcHr = false;
+    if constexpr (IntT<T>::kBits == 16) tcHr = int_tensor_cores() && !planar && int16_hr_tc_supported(n, x, y, w);
     for (int st = 0; len > R; ++st) {
-        const uint64_t threads = (uint64_t)batch * (n / rad);
-        k_int_stage<T><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(x, n, len, rad, shifts[st],
-                                                                       st == 0 ? w1 : w1 + MMA * MMA / 2, tw,
-                                                                       batch, planar);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        const T* F = st == 0 ? w1 : w1 + MMA * MMA / 2;
+        bool done = false;
+        if constexpr (IntT<T>::kBits == 16) {
+            if (tcHr && rad == R) {
+                if ((e = launch_int16_hr_stage(x, F, tw, n, len, batch, shifts[st], s)) != cudaSuccess) return e;
+                done = true;
+            }
+        }
+        if (!done) {
+            const uint64_t threads = (uint64_t)batch * (n / rad);
+            k_int_stage<T><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(x, n, len, rad, shifts[st], F, tw,
+                                                                           batch, planar);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
         tw += 2u * len;
         len /= rad;
         rad = R;
@@ -421,6 +434,9 @@ cudaError_t launch_typed(int v, uint32_t n, uint32_t batch, uint32_t interleave,
     const uint32_t mC = g1 > R ? R : g1;
     const uint32_t iC = g1 > R ? (g1 / R > R ? R : g1 / R) : 1u;
     const uint32_t hC = g1 / R > R ? g1 / (R * R) : 1u;
+    if constexpr (IntT<T>::kBits == 16) {
+        if (tcHr) return launch_int16_hr_final(x, y, tw, n, d0, mC, iC, hC, batch, shifts[4], s);
+    }
     const uint64_t threads = (uint64_t)batch * (n / R);
     k_int_final<T><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(x, y, n, d0, mC, iC, hC, shifts[4], tw, batch,
                                                                    planar);

@@ -59,6 +59,18 @@ void int_dft_w1_host(int bits, uint32_t n, void* out);
 bool int16_tc_supported(uint32_t n2, const void* x, const void* y);
 cudaError_t launch_int16_tc(const int16_t* x, int16_t* y, const int16_t* w, uint32_t n2, uint32_t ld, uint32_t rows,
                             uint32_t shift, cudaStream_t s);
+// The INT16 highRadix stages on the tensor cores (dft_int_hr_tc.cu):
+// interleaved rows of n = 2^k >= 64 points, x 16-byte aligned, y and the
+// twiddles 4-byte aligned. A decimation stage over blocks of s = 16^j points
+// (j >= 2), in place, with its 16-point DFT F (the internal table's rows) and
+// twiddles tw; the final stage of 16-point groups with the caller's last table
+// block D into the digit-reversed positions of y (digits d0, mC, iC, hC).
+bool int16_hr_tc_supported(uint32_t n, const void* x, const void* y, const void* tw);
+cudaError_t launch_int16_hr_stage(int16_t* x, const int16_t* F, const int16_t* tw, uint32_t n, uint32_t s,
+                                  uint32_t rows, uint32_t shift, cudaStream_t st);
+cudaError_t launch_int16_hr_final(const int16_t* x, int16_t* y, const int16_t* D, uint32_t n, uint32_t d0,
+                                  uint32_t mC, uint32_t iC, uint32_t hC, uint32_t rows, uint32_t shift,
+                                  cudaStream_t st);
 // The LINALG multiply on the tensor cores (int_mm_tc.cu): A and B rows
 // 16-byte aligned; INT16 also K <= 16384. The same bits as the CUDA-core
 // kernel.

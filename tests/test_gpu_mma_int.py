@@ -129,3 +129,46 @@ def test_tensor_core_product_in_place(torch_cuda):
     X = torch.from_numpy(np.ascontiguousarray(x, np.int16)).cuda()
     d.exec(X, X)
     assert np.array_equal(X.cpu().numpy(), O.mma_exec(bits, n, batch, 1, sh, x))
+
+
+@pytest.mark.parametrize("n,batch,il", [(256, 301, 1), (1024, 77, 1), (4096, 9, 1), (65536, 3, 1), (128, 100, 1),
+                                        (64, 513, 1), (512, 33, 1), (2048, 5, 1), (256, 7, 0), (1024, 1, 1),
+                                        (16384, 2, 1)])
+def test_high_radix_tensor_core_stages_agree(torch_cuda, n, batch, il):
+    """The INT16 highRadix radix-16 stages and final stage on the tensor cores
+    against the CUDA-core kernels and the oracle: full-range inputs with
+    imaginary parts of -32768 planted (the reference's saturating negation),
+    ragged batches, shifts that saturate and shifts that do not."""
+    L = F.lib()
+    x = _rand(16, 2 * n * batch, 5 * n + batch, True)
+    x[1::37] = -32768
+    x[0::53] = -32768
+    x[3::41] = 32767
+    for sh in ([0] * 5, [15] * 5, [2, 2, 2, 2, 4], [1, 3, 0, 2, 5]):
+        try:
+            L.FFTLIB_b200_FFT_setIntTensorCores(0)
+            y_cc = run(torch_cuda, 16, n, batch, il, sh, x)
+        finally:
+            L.FFTLIB_b200_FFT_setIntTensorCores(1)
+        y_tc = run(torch_cuda, 16, n, batch, il, sh, x)
+        assert np.array_equal(y_tc, y_cc), sh
+        k = max(1, min(batch, 16384 // n))
+        assert np.array_equal(y_tc[: 2 * n * k], O.mma_exec(16, n, k, il, sh, x[: 2 * n * k])), sh
+
+
+def test_high_radix_tensor_core_unaligned_rows_fall_back(torch_cuda):
+    """Rows that start off a 16-byte boundary take the CUDA-core kernels with
+    the same bits."""
+    import torch
+
+    n, batch, sh = 256, 9, [2, 2, 2, 2, 4]
+    x = _rand(16, 2 * n * batch, 99, True)
+    d = F.DftMma(n, batch, dtype=F.FFTLIB_INT16, interleave=1, shifts=sh)
+    X = torch.zeros(2 * n * batch + 8, dtype=torch.int16, device="cuda")
+    X[2:2 + 2 * n * batch] = torch.from_numpy(np.ascontiguousarray(x, np.int16)).cuda()
+    Y = torch.zeros(2 * n * batch + 8, dtype=torch.int16, device="cuda")
+    st = F.lib().FFTLIB_FFT_fft_ixX_cxX_oxX_exec(d.handle, F.ptr(X.data_ptr() + 4), F.ptr(d.w),
+                                                 F.ptr(Y.data_ptr() + 4))
+    F.check(st, "exec")
+    torch.cuda.synchronize()
+    assert np.array_equal(Y[2:2 + 2 * n * batch].cpu().numpy(), O.mma_exec(16, n, batch, 1, sh, x))
