@@ -17,10 +17,14 @@
 //
 // Exactness as in dft_int_tc.cu: values in offset binary v' = v + 32768 =
 // 256 h + l, three u8 x u8 products summed exactly in S32 accumulators,
-//   sum x W = 2^16 hh + 2^8 mid + ll - 2^15 (sum x' + sum W') + 32 2^30,
-// where the ones column gives sum x' = 256 mid + ll of that column. The
-// internal table's entries lie in [-32767, 32767], so the negated ones of a
-// stage's matrix are INT16 values too.
+//   sum x W = 2^16 hh + 2^8 mid + ll - 2^15 (sum x' + sum W') + 32 2^30
+//           = 256 T + ll,  T = 256 hh + mid + 128 (2^20 - sum x' - sum W'),
+// where the ones column gives sum x' = 256 mid + ll of that column. With
+// K = 32, hh < 2^21, mid < 2^22 and |128 (2^20 - ...)| < 2^29, so T is a
+// 32-bit value and the epilogue rounds and saturates 256 T + ll without
+// 64-bit arithmetic (hr_round). The internal table's entries lie in
+// [-32767, 32767], so the negated ones of a stage's matrix are INT16 values
+// too.
 //
 // The reference forms a stage's real part with the saturating negation of the
 // imaginary inputs, c1 neg(ai); neg(-32768) = 32767 = -(-32768) - 1, so the
@@ -34,7 +38,7 @@
 //
 // Roles per CTA (one persistent CTA per SM): 4 converter warps (raw values ->
 // offset bytes -> swizzled K-major shared memory, one data row per thread),
-// 8 epilogue warps (three accumulators -> 64-bit sums -> shift, round,
+// 8 epilogue warps (three accumulators -> 32-bit T -> shift, round,
 // saturate, twiddle -> HBM), one warp that owns tensor memory and issues the
 // 4 MMAs of a tile, one copy thread. Every wait is bounded; a wait that gives
 // up sets kErrTcTimeout in the launch's error word.
@@ -67,8 +71,8 @@ struct HrTc {
     static constexpr uint32_t RAWB = (uint32_t)TM * 16u * 4u;  // 8 KB: 16 complex INT16 points per row
     static constexpr uint32_t OFF_B = NB * TILE;
     static constexpr uint32_t OFF_RAW = OFF_B + 2 * B_LIMB;
-    static constexpr uint32_t OFF_CW = OFF_RAW + NR * RAWB;  // 32 long long column terms
-    static constexpr uint32_t OFF_MK = OFF_CW + 8u * 32u;    // RS x TM masks (uint16)
+    static constexpr uint32_t OFF_CW = OFF_RAW + NR * RAWB;  // 32 column terms 128 (2^20 - sum W')
+    static constexpr uint32_t OFF_MK = OFF_CW + 4u * 32u;    // RS x TM masks (uint16)
     static constexpr uint32_t OFF_BAR = (OFF_MK + 2u * RS * TM + 7u) & ~7u;
     static constexpr int NBARS = 2 * NB + 2 * NA + 1 + 2 * NR;
     static constexpr uint32_t OFF_MISC = OFF_BAR + 8u * NBARS;
@@ -157,6 +161,41 @@ __device__ __forceinline__ uint32_t hr_limb_entry(const HrArgs& a, int k, int n)
     return n == 32 ? 1u : 0u;
 }
 
+// floor((256 T + L + 2^(s-1)) / 2^s) saturated to INT16 (the reference's
+// shiftAndRound of the exact sum 256 T + L, |256 T + L| < 2^36), in 32-bit
+// integers. s = the shift's low byte, capped at 37: every larger shift gives 0
+// for such sums, as 37 does. For s >= 8 the low byte L folds into T, for
+// s < 8 T is first clamped to +-2^22, beyond which the result saturates either
+// way.
+struct HrRound {
+    bool big;
+    int sE, sh, r1, r2;
+};
+
+__device__ __forceinline__ HrRound hr_round_of(uint32_t shift)
+{
+    HrRound R;
+    const uint32_t s8 = shift & 0xFFu;
+    R.sE = s8 > 37u ? 37 : (int)s8;
+    R.big = R.sE >= 8;
+    R.sh = R.big ? R.sE - 8 : 8 - R.sE;
+    R.r1 = R.sE == 8 ? 128 : (R.sE > 0 && R.sE < 8 ? (1 << (R.sE - 1)) : 0);
+    R.r2 = R.sE > 8 ? (1 << (R.sE - 9)) : 0;
+    return R;
+}
+
+__device__ __forceinline__ int32_t hr_round(const HrRound& R, int32_t T, int32_t L)
+{
+    int32_t q;
+    if (R.big) {
+        q = (T + ((L + R.r1) >> 8) + R.r2) >> R.sh;
+    } else {
+        const int32_t A = min(max(T, -(1 << 22)), 1 << 22);
+        q = A * (1 << R.sh) + ((L + R.r1) >> R.sE);
+    }
+    return min(max(q, -32768), 32767);
+}
+
 // First point of data row r (global index) of a decimation stage; q is its
 // butterfly index inside the block.
 __device__ __forceinline__ uint64_t hr_stage_point(const HrArgs& a, uint64_t r, uint32_t* q)
@@ -179,7 +218,7 @@ __global__ void __launch_bounds__(HrTc::THREADS, 1) k_int16_hr_tc(const HrArgs a
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + S::OFF_BAR);
     uint32_t* misc = reinterpret_cast<uint32_t*>(sm + S::OFF_MISC);
     volatile uint32_t* abortFlag = misc + 1;
-    long long* colterm = reinterpret_cast<long long*>(sm + S::OFF_CW);
+    int32_t* colE = reinterpret_cast<int32_t*>(sm + S::OFF_CW);
     uint16_t* masks = reinterpret_cast<uint16_t*>(sm + S::OFF_MK);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -213,11 +252,11 @@ __global__ void __launch_bounds__(HrTc::THREADS, 1) k_int16_hr_tc(const HrArgs a
             *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
             *reinterpret_cast<uint4*>(lo + off) = make_uint4(q[0], q[1], q[2], q[3]);
         }
-        // per output column: 32 2^30 - 2^15 sum W'
+        // per output column: 128 (2^20 - sum W')
         for (int n = threadIdx.x; n < 32; n += blockDim.x) {
-            long long s = 0;
+            int32_t s = 0;
             for (int k = 0; k < 32; ++k) s += hr_entry<FINAL>(a, k, n) + 32768;
-            colterm[n] = (32ll << 30) - (s << 15);
+            colE[n] = 128 * ((1 << 20) - s);
         }
     }
     fence_proxy_async_smem();
@@ -361,6 +400,7 @@ __global__ void __launch_bounds__(HrTc::THREADS, 1) k_int16_hr_tc(const HrArgs a
         const int qd = warp & 3, hf = (warp - S::CW) >> 2;
         const int r = 32 * qd + lane;
         const uint32_t laneBase = (uint32_t)(32 * qd) << 16;
+        const HrRound R = hr_round_of(a.shift);
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
             const int ac = (int)(i % NA);
@@ -373,9 +413,9 @@ __global__ void __launch_bounds__(HrTc::THREADS, 1) k_int16_hr_tc(const HrArgs a
             int32_t hh[16], mid[16], ll[16];
             // the ones column first: sum x' of the row
             hr_ld16(dbase + (uint32_t)(NO + 32), mid);
-            long long sx = (long long)mid[0] << 8;
+            int32_t sx = mid[0] * 256;
             hr_ld16(dbase + (uint32_t)(2 * NO + 32), ll);
-            sx += (long long)ll[0];
+            sx += ll[0];
             hr_ld16(dbase + (uint32_t)(16 * hf), hh);
             hr_ld16(dbase + (uint32_t)(NO + 16 * hf), mid);
             hr_ld16(dbase + (uint32_t)(2 * NO + 16 * hf), ll);
@@ -387,11 +427,11 @@ __global__ void __launch_bounds__(HrTc::THREADS, 1) k_int16_hr_tc(const HrArgs a
 
             const uint64_t row = (uint64_t)tile * TM + (uint64_t)r;
             if (row >= a.total) continue;
-            long long v[16];
+            // T of each output: sum x W = 256 T + ll
+            const int32_t sx128 = 128 * sx;
+            int32_t T[16];
 #pragma unroll
-            for (int c = 0; c < 16; ++c)
-                v[c] = ((long long)hh[c] << 16) + ((long long)mid[c] << 8) + (long long)ll[c] + colterm[16 * hf + c] -
-                       (sx << 15);
+            for (int c = 0; c < 16; ++c) T[c] = hh[c] * 256 + mid[c] + (colE[16 * hf + c] - sx128);
             if (!FINAL) {
                 uint32_t q;
                 const uint64_t p0 = hr_stage_point(a, row, &q);
@@ -400,17 +440,21 @@ __global__ void __launch_bounds__(HrTc::THREADS, 1) k_int16_hr_tc(const HrArgs a
 #pragma unroll
                 for (int c2 = 0; c2 < 8; ++c2) {
                     const int l = 8 * hf + c2;
-                    long long yr = v[2 * c2];
+                    int32_t lr = ll[2 * c2];
                     if (mask) {
-                        for (uint32_t mm = mask; mm; mm &= mm - 1u) yr -= a.F[l * 32 + 2 * (__ffs((int)mm) - 1) + 1];
+                        for (uint32_t mm = mask; mm; mm &= mm - 1u) lr -= a.F[l * 32 + 2 * (__ffs((int)mm) - 1) + 1];
                     }
-                    const int16_t tr = shift_round<int16_t>(yr, a.shift);
-                    const int16_t ti = shift_round<int16_t>(v[2 * c2 + 1], a.shift);
+                    const int32_t tr = hr_round(R, T[2 * c2], lr);
+                    const int32_t ti = hr_round(R, T[2 * c2 + 1], ll[2 * c2 + 1]);
                     const uint32_t e = *reinterpret_cast<const uint32_t*>(twq + l * 32);
-                    const int16_t e0 = (int16_t)(e & 0xFFFFu), e1 = (int16_t)(e >> 16);
-                    const int16_t re =
-                        shift_round<int16_t>(mul<int16_t>(e1, tr) + mul<int16_t>(neg_sat<int16_t>(e0), ti), 15u);
-                    const int16_t im = shift_round<int16_t>(mul<int16_t>(e0, tr) + mul<int16_t>(e1, ti), 15u);
+                    const int32_t e0 = (int16_t)(e & 0xFFFFu), e1 = (int16_t)(e >> 16);
+                    const int32_t ne0 = e0 == -32768 ? 32767 : -e0;  // the reference's saturating negation
+                    // |e1 tr + ne0 ti| < 2^31; e0 tr + e1 ti reaches 2^31 (and wraps
+                    // to INT32_MIN) only for four values of -32768, a result of 32767
+                    const int32_t sr = e1 * tr + ne0 * ti;
+                    const int32_t si = (int32_t)((uint32_t)(e0 * tr) + (uint32_t)(e1 * ti));
+                    const int32_t re = min(max((sr + 16384) >> 15, -32768), 32767);
+                    const int32_t im = si == INT32_MIN ? 32767 : min(max((si + 16384) >> 15, -32768), 32767);
                     out[(uint64_t)l << a.lgStride] = (uint32_t)(uint16_t)re | ((uint32_t)(uint16_t)im << 16);
                 }
             } else {
@@ -427,8 +471,8 @@ __global__ void __launch_bounds__(HrTc::THREADS, 1) k_int16_hr_tc(const HrArgs a
 #pragma unroll
                 for (int c2 = 0; c2 < 8; ++c2) {
                     const int l = 8 * hf + c2;
-                    const int16_t vr = shift_round<int16_t>(v[2 * c2], a.shift);
-                    const int16_t vi = shift_round<int16_t>(v[2 * c2 + 1], a.shift);
+                    const int32_t vr = hr_round(R, T[2 * c2], ll[2 * c2]);
+                    const int32_t vi = hr_round(R, T[2 * c2 + 1], ll[2 * c2 + 1]);
                     out[(uint64_t)l << a.lgPer] = (uint32_t)(uint16_t)vr | ((uint32_t)(uint16_t)vi << 16);
                 }
             }
