@@ -98,7 +98,7 @@ struct HrArgs {
     uint32_t n;         // points per row
     uint32_t lgPer;     // log2 of the data rows per row (n / 16)
     uint32_t lgStride;  // stage: log2 of s / 16, the distance of a butterfly's points
-    uint32_t d0, mC, iC, hC;  // final: the digits of a group index
+    uint32_t lgD0, lgM, lgI, lgH;  // final: log2 of the digits d0, mC, iC, hC of a group index
     uint32_t shift;
     uint64_t total;  // data rows of the launch
     uint32_t* err;
@@ -184,16 +184,26 @@ __device__ __forceinline__ HrRound hr_round_of(uint32_t shift)
     return R;
 }
 
+// The rounded value before saturation (|q| < 2^31).
+__device__ __forceinline__ int32_t hr_round_q(const HrRound& R, int32_t T, int32_t L)
+{
+    if (R.big) return (T + ((L + R.r1) >> 8) + R.r2) >> R.sh;
+    const int32_t A = min(max(T, -(1 << 22)), 1 << 22);
+    return A * (1 << R.sh) + ((L + R.r1) >> R.sE);
+}
+
 __device__ __forceinline__ int32_t hr_round(const HrRound& R, int32_t T, int32_t L)
 {
-    int32_t q;
-    if (R.big) {
-        q = (T + ((L + R.r1) >> 8) + R.r2) >> R.sh;
-    } else {
-        const int32_t A = min(max(T, -(1 << 22)), 1 << 22);
-        q = A * (1 << R.sh) + ((L + R.r1) >> R.sE);
-    }
-    return min(max(q, -32768), 32767);
+    return min(max(hr_round_q(R, T, L), -32768), 32767);
+}
+
+// One complex INT16 point from two 32-bit values, each saturated: the real
+// part in the low half, the imaginary part in the high half.
+__device__ __forceinline__ uint32_t hr_pack_sat(int32_t re, int32_t im)
+{
+    uint32_t d;
+    asm("cvt.pack.sat.s16.s32 %0, %1, %2;" : "=r"(d) : "r"(im), "r"(re));
+    return d;
 }
 
 // First point of data row r (global index) of a decimation stage; q is its
@@ -283,21 +293,14 @@ __global__ void __launch_bounds__(HrTc::THREADS, 1) k_int16_hr_tc(const HrArgs a
             const unsigned char* raw = sm + S::OFF_RAW + rr * S::RAWB;
             uint32_t w[16];
             if (FINAL) {
-                // 64 contiguous bytes; start at a chunk that depends on the row
-                // so that a quarter warp's 16-byte loads hit distinct banks
+                // 64 contiguous bytes
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    const int cc = (c + (r >> 1)) & 3;
-                    const uint4 v = *reinterpret_cast<const uint4*>(raw + 4u * rowPos + 16u * (uint32_t)cc);
-                    // registers are indexed statically: select by cc
-#pragma unroll
-                    for (int z = 0; z < 4; ++z)
-                        if (z == cc) {
-                            w[4 * z] = v.x;
-                            w[4 * z + 1] = v.y;
-                            w[4 * z + 2] = v.z;
-                            w[4 * z + 3] = v.w;
-                        }
+                for (int z = 0; z < 4; ++z) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(raw + 4u * rowPos + 16u * (uint32_t)z);
+                    w[4 * z] = v.x;
+                    w[4 * z + 1] = v.y;
+                    w[4 * z + 2] = v.z;
+                    w[4 * z + 3] = v.w;
                 }
             } else {
 #pragma unroll
@@ -453,27 +456,27 @@ __global__ void __launch_bounds__(HrTc::THREADS, 1) k_int16_hr_tc(const HrArgs a
                     // to INT32_MIN) only for four values of -32768, a result of 32767
                     const int32_t sr = e1 * tr + ne0 * ti;
                     const int32_t si = (int32_t)((uint32_t)(e0 * tr) + (uint32_t)(e1 * ti));
-                    const int32_t re = min(max((sr + 16384) >> 15, -32768), 32767);
-                    const int32_t im = si == INT32_MIN ? 32767 : min(max((si + 16384) >> 15, -32768), 32767);
-                    out[(uint64_t)l << a.lgStride] = (uint32_t)(uint16_t)re | ((uint32_t)(uint16_t)im << 16);
+                    const int32_t im = si == INT32_MIN ? 32767 : (si + 16384) >> 15;
+                    out[(uint64_t)l << a.lgStride] = hr_pack_sat((sr + 16384) >> 15, im);
                 }
             } else {
                 const uint64_t rw = row >> a.lgPer;
                 uint32_t g = (uint32_t)(row & ((1ull << a.lgPer) - 1u));
-                const uint32_t h = g % a.hC;
-                g /= a.hC;
-                const uint32_t ii = g % a.iC;
-                g /= a.iC;
-                const uint32_t mm = g % a.mC;
-                const uint32_t k = g / a.mC;
-                const uint32_t dst0 = h * a.d0 * a.mC * a.iC + ii * a.d0 * a.mC + mm * a.d0 + k;
+                // digits of the group index (powers of two): h fastest, then i, m, k
+                const uint32_t h = g & ((1u << a.lgH) - 1u);
+                g >>= a.lgH;
+                const uint32_t ii = g & ((1u << a.lgI) - 1u);
+                g >>= a.lgI;
+                const uint32_t mm = g & ((1u << a.lgM) - 1u);
+                const uint32_t k = g >> a.lgM;
+                const uint32_t dst0 =
+                    (h << (a.lgD0 + a.lgM + a.lgI)) + (ii << (a.lgD0 + a.lgM)) + (mm << a.lgD0) + k;
                 uint32_t* out = reinterpret_cast<uint32_t*>(a.y) + rw * a.n + dst0;
 #pragma unroll
                 for (int c2 = 0; c2 < 8; ++c2) {
                     const int l = 8 * hf + c2;
-                    const int32_t vr = hr_round(R, T[2 * c2], ll[2 * c2]);
-                    const int32_t vi = hr_round(R, T[2 * c2 + 1], ll[2 * c2 + 1]);
-                    out[(uint64_t)l << a.lgPer] = (uint32_t)(uint16_t)vr | ((uint32_t)(uint16_t)vi << 16);
+                    out[(uint64_t)l << a.lgPer] =
+                        hr_pack_sat(hr_round_q(R, T[2 * c2], ll[2 * c2]), hr_round_q(R, T[2 * c2 + 1], ll[2 * c2 + 1]));
                 }
             }
         }
@@ -548,17 +551,20 @@ cudaError_t launch_int16_hr_final(const int16_t* x, int16_t* y, const int16_t* D
                                   uint32_t mC, uint32_t iC, uint32_t hC, uint32_t rows, uint32_t shift,
                                   cudaStream_t st)
 {
-    if (n < 64 || (n & (n - 1u)) || (uint64_t)d0 * mC * iC * hC * 16u != n) return cudaErrorInvalidValue;
+    const auto pow2 = [](uint32_t v) { return v != 0 && (v & (v - 1u)) == 0; };
+    if (n < 64 || !pow2(n) || !pow2(d0) || !pow2(mC) || !pow2(iC) || !pow2(hC) ||
+        (uint64_t)d0 * mC * iC * hC * 16u != n)
+        return cudaErrorInvalidValue;
     HrArgs a{};
     a.x = x;
     a.y = y;
     a.D = D;
     a.n = n;
     a.lgPer = hr_lg2(n) - 4u;
-    a.d0 = d0;
-    a.mC = mC;
-    a.iC = iC;
-    a.hC = hC;
+    a.lgD0 = hr_lg2(d0);
+    a.lgM = hr_lg2(mC);
+    a.lgI = hr_lg2(iC);
+    a.lgH = hr_lg2(hC);
     a.shift = shift;
     a.total = (uint64_t)rows << a.lgPer;
     a.err = error_word().dev;
