@@ -315,14 +315,22 @@ __global__ void __launch_bounds__(IntTc::THREADS, 1)
         const int q = warp & 3, ch = (warp - S::LW) >> 2;  // lane quarter, column group
         const int l = 32 * q + lane;
         const uint32_t laneBase = (uint32_t)(32 * q) << 16;
-        // sum x w = 2^16 hh + 2^8 mid + ll + cl - 2^15 rowsum, |sum x w| <= 2^37;
-        // shiftAndRound as (v + 2^(s-1)) >> s, which equals the reference's
-        // ((v >> (s-1)) + 1) >> 1; every shift of 39 or more gives 0 for
-        // such v, as 39 itself does
-        const long long cl = (128ll << 30) - 32768ll * (long long)colsum[l];
+        // sum x w = 2^16 hh + 2^8 mid + ll - 2^15 (rowsum + colsum) + 128 2^30
+        //         = 2^15 V + W,  V = U + (R >> 15),  W = R & 0x7FFF,  with
+        // U = 2 hh + 2^22 - colsum - rowsum (|U| < 2^25) and R = 256 mid + ll,
+        // which fits in 32 unsigned bits (mid <= 2 128 255^2), so no 64-bit
+        // arithmetic is needed. shiftAndRound (v + 2^(s-1)) >> s, which equals
+        // the reference's ((v >> (s-1)) + 1) >> 1, then saturation: for s >= 15
+        // W folds into V; below 15, V is clamped to +-2^15 first, beyond which
+        // the result saturates either way. |sum x w| <= 2^37, so every shift of
+        // 39 or more gives 0, as 39 itself does.
+        const int32_t cu = (1 << 22) - colsum[l];
         const uint32_t s8 = shift & 0xFFu;
-        const uint32_t sh = s8 > 39u ? 39u : s8;
-        const long long rnd = sh ? (1ll << (sh - 1u)) : 0ll;
+        const int sE = s8 > 39u ? 39 : (int)s8;
+        const bool big = sE >= 15;
+        const int sh = big ? sE - 15 : 15 - sE;
+        const int32_t r1 = sE == 15 ? (1 << 14) : (sE > 0 && sE < 15 ? (1 << (sE - 1)) : 0);
+        const int32_t r2 = sE > 15 ? (1 << (sE - 16)) : 0;
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < numTiles; tile += gridDim.x, ++i) {
             const int a = (int)(i % NA);
@@ -344,10 +352,16 @@ __global__ void __launch_bounds__(IntTc::THREADS, 1)
                 int16_t out[16];
 #pragma unroll
                 for (int e = 0; e < 16; ++e) {
-                    const long long v = ((long long)hh[e] << 16) + ((long long)mid[e] << 8) + (long long)ll[e] + cl -
-                                        ((long long)rowsum[slot * TS + c0 + e] << 15);
-                    const long long q = (v + rnd) >> sh;
-                    out[e] = q > 32767ll ? (int16_t)32767 : (q < -32768ll ? (int16_t)-32768 : (int16_t)q);
+                    const uint32_t R = (uint32_t)mid[e] * 256u + (uint32_t)ll[e];
+                    const int32_t V = 2 * hh[e] + cu - rowsum[slot * TS + c0 + e] + (int32_t)(R >> 15);
+                    const int32_t W = (int32_t)(R & 0x7FFFu);
+                    int32_t q;
+                    if (big) {
+                        q = (V + ((W + r1) >> 15) + r2) >> sh;
+                    } else {
+                        q = min(max(V, -(1 << 15)), 1 << 15) * (1 << sh) + ((W + r1) >> sE);
+                    }
+                    out[e] = (int16_t)min(max(q, -32768), 32767);
                 }
                 int16_t* yb = y + base + (uint64_t)c0 * 128u;
                 if (full) {
