@@ -173,12 +173,14 @@ cudaError_t matmul_typed(uint32_t M, uint32_t K, uint32_t N, const void* a, size
 // the imaginary part negated with saturation as the reference does), rounds
 // by `shift`, multiplies by its twiddle (the caller's (-sin, cos) pair of
 // (q, l)) and rounds by bits - 1, and writes the result to q + l s/rad.
-template <class T>
-__global__ void __launch_bounds__(256) k_int_stage(T* buf, uint32_t n, uint32_t s, uint32_t rad, uint32_t shift,
+template <class T, uint32_t RAD>
+__global__ void __launch_bounds__(256) k_int_stage(T* buf, uint32_t n, uint32_t s, uint32_t radRt, uint32_t shift,
                                                    const T* __restrict__ F, const T* __restrict__ tw, uint32_t rows,
                                                    int planar)
 {
     constexpr uint32_t MMA = IntT<T>::kMma, R = MMA / 2;
+    // a radix fixed at compile time (2, 4, 8, MMA/2) drops the unused terms; 0: radRt
+    const uint32_t rad = RAD ? RAD : radRt;
     const uint32_t per = n / rad;
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (uint64_t)rows * per) return;
@@ -422,8 +424,12 @@ cudaError_t launch_typed(int v, uint32_t n, uint32_t batch, uint32_t interleave,
         }
         if (!done) {
             const uint64_t threads = (uint64_t)batch * (n / rad);
-            k_int_stage<T><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(x, n, len, rad, shifts[st], F, tw,
-                                                                           batch, planar);
+            const unsigned grid = (unsigned)((threads + 255) / 256);
+            if (rad == 2) k_int_stage<T, 2><<<grid, 256, 0, s>>>(x, n, len, rad, shifts[st], F, tw, batch, planar);
+            else if (rad == 4) k_int_stage<T, 4><<<grid, 256, 0, s>>>(x, n, len, rad, shifts[st], F, tw, batch, planar);
+            else if (rad == 8) k_int_stage<T, 8><<<grid, 256, 0, s>>>(x, n, len, rad, shifts[st], F, tw, batch, planar);
+            else if (rad == R) k_int_stage<T, R><<<grid, 256, 0, s>>>(x, n, len, rad, shifts[st], F, tw, batch, planar);
+            else k_int_stage<T, 0><<<grid, 256, 0, s>>>(x, n, len, rad, shifts[st], F, tw, batch, planar);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         tw += 2u * len;
