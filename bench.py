@@ -44,6 +44,20 @@ METRIC = "batched FFT HBM GB/s (% peak); TC-DFT vs FP32-FFT speedup at ≤2e-6 r
 WORKLOAD = "fft1dBatched_i32fc_c32fc_o32fc c2c FP32 forward, N=4096 x 8192 channels"
 
 
+REL_L2_BOUND = 2e-6  # FP32 paths against FP64 (relative L2)
+
+# Parity checks of the timed outputs: every bench line carries them, and a
+# line whose checks fail is printed with parity.ok false and the process
+# exits non-zero.
+PARITY_FAILURES = []
+
+
+def parity_check(name, ok, value=None):
+    if not ok:
+        PARITY_FAILURES.append(f"{name}: {value}")
+    return ok
+
+
 def algo_bytes(n, ch):
     return 16.0 * n * ch
 
@@ -205,7 +219,9 @@ def reference_arm(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_full, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_channels_per_step": sample, "parallelism": "host threads"},
+        "config": {"workload": WORKLOAD, "sample_channels_per_step": sample, "parallelism": "host threads",
+                   "ms_per_step_basis": f"extrapolated: the time of the {sample}-channel sample per step scaled "
+                                        f"to {CHANNELS} channels (channels are independent)"},
         "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": threads, "kind": "reference",
                          "sample": f"{sample} channels of N={N_POINTS} per step, reference "
                                    f"FFTLIB_fft1dBatched_i32fc_c32fc_o32fc_cn built with gcc -O3"},
@@ -282,6 +298,7 @@ def our_arm(args, world, rank, local):
     want = np.fft.fft(xs[:, 0::2] + 1j * xs[:, 1::2], axis=1)
     got = ys[:, 0::2] + 1j * ys[:, 1::2]
     rel = float(np.linalg.norm(got - want) / np.linalg.norm(want))
+    parity_check("c2c_4096 sampled rel-L2", rel <= REL_L2_BOUND, rel)
 
     # end to end through the synchronous FFTLIB call with pinned host buffers
     e2e_steps = max(2, min(args.steps, 5))
@@ -320,13 +337,18 @@ def our_arm(args, world, rank, local):
         "e2e": {"value": round(e2e_gbs, 2), "unit": "GB/s", "h2d_bytes_per_step": int(8 * n * ch),
                 "d2h_bytes_per_step": int(8 * n * ch), "path": "FFTLIB _kernel, pinned host buffers"},
         "gpu_launches": args.steps,
-        "parity": {"rel_l2_vs_fp64_sampled": rel, "bound": 2e-6},
+        "parity": {"rel_l2_vs_fp64_sampled": rel, "bound": REL_L2_BOUND},
         "clocks": clk.summary(),
     }
     if world == 1:
         out["cpu_baseline"] = cpu_baseline()
         out["configs"] = secondary_configs(args)
+    out["parity"]["ok"] = not PARITY_FAILURES
+    if PARITY_FAILURES:
+        out["parity"]["failures"] = PARITY_FAILURES
     print(json.dumps(out))
+    if PARITY_FAILURES:
+        sys.exit(1)
 
 
 def _time_launches(torch, stream, fn, steps, warmup=3):
@@ -381,8 +403,15 @@ def secondary_configs(args):
     F.check(F.fn(F.KERNELS["i16"] + "_init")(F.ptr(x), bx, F.ptr(wd), bw, F.ptr(y), bx, F.ptr(sh), bs, n, ch, pb))
     k = F.fn("FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync")
     ms = _time_launches(torch, stream, lambda: k(F.ptr(x), F.ptr(wd), F.ptr(y), F.ptr(sh), 5, n, ch, pb, sp), steps)
+    torch.cuda.synchronize()
+    import oracle as O
+
+    k16 = 16  # bit-exact sample: the first 16 channels against the oracle's restated _cn
+    xs = x[: 2 * n * k16].cpu().numpy()
+    exact16 = bool(np.array_equal(y[: 2 * n * k16].cpu().numpy(), O.fft_c2c_i16(xs, n, k16, [2] * 5)))
+    parity_check("int16_c2c_1024 bit-exact sample", exact16)
     res["int16_c2c_n1024_x4096"] = {"ms": round(ms, 4), "GBps": round(8.0 * n * ch / ms / 1e6, 1),
-                                     "transforms_per_s": round(ch / ms * 1e3, 1)}
+                                     "transforms_per_s": round(ch / ms * 1e3, 1), "bit_exact_sample": exact16}
 
     # r2c then c2r, N=4096 x 8192 reals (128 MiB), outmode / inMode 0
     n, ch = 4096, 8192
@@ -400,10 +429,18 @@ def secondary_configs(args):
     ms_r = _time_launches(torch, stream, lambda: kr(F.ptr(xr), None, F.ptr(yc), n, ch, 0, pr, sp), steps)
     ms_c = _time_launches(torch, stream, lambda: kc(F.ptr(yc), None, F.ptr(xb), n, ch, 0, pc, sp), steps)
     bytes_rc = (4.0 * n + 8.0 * (n // 2 + 1)) * ch
+    torch.cuda.synchronize()
     rt = float(torch.linalg.norm(xb - xr) / torch.linalg.norm(xr))
+    idx = [0, ch // 2, ch - 1]
+    xs = xr.view(ch, n)[idx].cpu().numpy().astype(np.float64)
+    want = np.fft.rfft(xs, axis=1)
+    got = yc.view(ch, n // 2 + 1, 2)[idx].cpu().numpy().astype(np.float64)
+    fwd = float(np.linalg.norm(got[..., 0] + 1j * got[..., 1] - want) / np.linalg.norm(want))
+    parity_check("r2c_4096 sampled rel-L2", fwd <= REL_L2_BOUND, fwd)
+    parity_check("r2c->c2r round trip rel-L2", rt <= REL_L2_BOUND, rt)
     res["r2c_c2r_n4096_x8192"] = {"r2c_ms": round(ms_r, 4), "r2c_GBps": round(bytes_rc / ms_r / 1e6, 1),
                                   "c2r_ms": round(ms_c, 4), "c2r_GBps": round(bytes_rc / ms_c / 1e6, 1),
-                                  "roundtrip_rel_l2": rt}
+                                  "r2c_rel_l2_vs_fp64_sampled": fwd, "roundtrip_rel_l2": rt}
 
     # uneven lengths: 20,000 c2c transforms, 12 * 2^a 3^b 5^c <= 4096, log-uniform,
     # laid out grouped by length so per-length batched calls can run on the same memory
@@ -433,6 +470,24 @@ def secondary_configs(args):
             ka(F.ptr(xs), F.ptr(ys), nn, cc, pbk, sp)
 
     ms_api = _time_launches(torch, stream, per_length_api, steps)
+    # sampled check of the graph launch's output: the first and last
+    # transform of every length against numpy's FP64 FFT
+    mb.exec(xm, ym, sp)
+    torch.cuda.synchronize()
+    starts = np.concatenate([[0], np.cumsum(lengths.astype(np.int64))[:-1]])
+    pick = sorted({int(np.argmax(lengths == u)) for u in uniq} |
+                  {len(lengths) - 1 - int(np.argmax(lengths[::-1] == u)) for u in uniq})
+    xh, yh = xm.cpu().numpy().astype(np.float64), ym.cpu().numpy().astype(np.float64)
+    e2 = r2 = 0.0
+    for i in pick:
+        o, nn = int(starts[i]), int(lengths[i])
+        xc = xh[2 * o: 2 * (o + nn)]
+        want = np.fft.fft(xc[0::2] + 1j * xc[1::2])
+        yc_ = yh[2 * o: 2 * (o + nn)]
+        e2 += float(np.sum(np.abs(yc_[0::2] + 1j * yc_[1::2] - want) ** 2))
+        r2 += float(np.sum(np.abs(want) ** 2))
+    mixed_rel = (e2 / r2) ** 0.5
+    parity_check("mixed_20000 sampled rel-L2", mixed_rel <= REL_L2_BOUND, mixed_rel)
     mbytes = 16.0 * total
     res["mixed_20000"] = {"lengths": len(uniq), "total_points": total,
                           "persistent_graph_ms": round(ms_graph, 4),
@@ -440,6 +495,7 @@ def secondary_configs(args):
                           "per_length_same_kernel_ms": round(ms_per, 4),
                           "per_length_batched_api_ms": round(ms_api, 4),
                           "speedup_vs_per_length_api": round(ms_api / ms_graph, 3),
+                          "rel_l2_vs_fp64_sampled": mixed_rel, "sampled_transforms": len(pick),
                           "transforms_per_s": round(20000 / ms_graph * 1e3, 1)}
     mb.close()
     res["tc_dft"] = tc_dft_configs(args, steps)
@@ -487,6 +543,7 @@ def int_dft_configs(steps):
         xs = x0[: 2 * n * k].cpu().numpy()
         want = O.mma_exec(bits, n, k, 1, sh, xs)
         exact = bool(np.array_equal(y[: 2 * n * k].cpu().numpy(), want))
+        parity_check(f"int{bits}_dft_{n} bit-exact sample", exact)
         entry = {"variant": O.mma_variant(bits, n, rows, 1), "rows": rows, "ms": round(ms, 4),
                  "GBps": round(2.0 * 2 * n * rows * (bits // 8) / ms / 1e6, 1),
                  "rows_per_s": round(rows / ms * 1e3, 1), "bit_exact_sample": exact}
@@ -537,6 +594,7 @@ def linalg_configs(steps):
             rs = 16
             a_s, b_h = a[:rs].cpu().numpy(), b.cpu().numpy()
             exact = bool(np.array_equal(c[:rs].cpu().numpy(), O.linalg_mm(bits, a_s, b_h, shift)))
+            parity_check(f"linalg_int{bits}_{m}x{k}x{n} bit-exact sample", exact)
             entry = {"m": m, "k": k, "n": n, "ms": round(ms, 4),
                      "TMACps": round(m * k * n / ms / 1e9, 3),
                      "GBps": round((m * k + k * n + m * n) * (bits // 8) / ms / 1e6, 1),
@@ -596,6 +654,7 @@ def fft1d_single_configs(steps):
         got = yh.numpy().astype(np.float64)
         want = np.fft.fft(x0.numpy().astype(np.float64).view(np.complex128))
         rel = float(np.linalg.norm(got.view(np.complex128) - want) / np.linalg.norm(want))
+        parity_check(f"fft1d_{n} rel-L2", rel <= REL_L2_BOUND, rel)
         entry = {"plan": F.describe_plan(n), "device_ms": round(ms, 5),
                  "device_GBps": round(16.0 * n / ms / 1e6, 1), "e2e_ms": round(e2e_ms, 4),
                  "h2d_d2h_bytes": 16 * n, "rel_l2_vs_fp64": rel}
@@ -660,6 +719,7 @@ def tc_dft_configs(args, steps):
         ys = y.view(batch, 2 * n)[torch.from_numpy(rows).cuda()].cpu().numpy().astype(np.float64)
         want = np.fft.fft(xs[:, 0::2] + 1j * xs[:, 1::2], axis=1)
         rel = float(np.linalg.norm(ys[:, 0::2] + 1j * ys[:, 1::2] - want) / np.linalg.norm(want))
+        parity_check(f"tc_dft_{n} sampled rel-L2", rel <= REL_L2_BOUND, rel)
         gbs = 16.0 * n * batch / ms_tc / 1e6
         tfs = tc_flops(n) * batch / ms_tc / 1e9
         out[str(n)] = {"rows": batch, "tc_ms": round(ms_tc, 4), "tc_GBps": round(gbs, 1),

@@ -11,8 +11,6 @@
 // until the process exits.
 #include <string.h>
 
-#include <mutex>
-
 #include "capi_common.h"
 #include "fft_engine.h"
 #include "fftlib_b200_ext.h"
@@ -24,31 +22,26 @@ namespace {
 
 // Scratch: 256 bytes of control words (word 0: error word of the pipelined
 // kernel's bounded waits), then the per-pass twiddle table of the transform.
-constexpr uint32_t kNoAllocControl = 32;                        // float2 slots (256 bytes)
-constexpr uint32_t kNoAllocScratch = kNoAllocControl + 32768;   // float2 slots (256 KiB + 256 B)
+// A single-kernel schedule R[0] x R[1] x ... of N points has per-pass blocks
+// of (R[i] - 1) * (R[0] ... R[i-1]) entries for i >= 1, N - R[0] in total, so
+// kMaxSingleN slots hold the table of every length the planner accepts.
+constexpr uint32_t kNoAllocControl = 32;                              // float2 slots (256 bytes)
+constexpr uint32_t kNoAllocTable = kMaxSingleN;                       // float2 slots (128 KiB)
+constexpr uint32_t kNoAllocScratch = kNoAllocControl + kNoAllocTable; // 128 KiB + 256 B
+static_assert(kNoAllocTable >= kMaxSingleN - 2u, "the table must hold N - R[0] entries for N <= kMaxSingleN");
 
 static __device__ __align__(256) float2 g_noalloc_scratch[kNoAllocScratch];
 
-// Device address of g_noalloc_scratch per device. In host code the symbol
-// name is only a host-side stand-in: the address must come from
-// cudaGetSymbolAddress with the device current.
-float2* scratch_address(int dev, cudaError_t* err)
+// Device address of g_noalloc_scratch on the current device. In host code the
+// symbol name is only a host-side stand-in: the address comes from
+// cudaGetSymbolAddress with the device current. It is looked up on every call
+// (no allocation once the module is loaded), so a cudaDeviceReset, which
+// reloads the module, never leaves a stale address behind.
+float2* scratch_address(cudaError_t* err)
 {
-    static std::mutex mu;
-    static float2* addr[64] = {};
-    *err = cudaSuccess;
-    if (dev < 0 || dev >= 64) {
-        *err = cudaErrorInvalidDevice;
-        return nullptr;
-    }
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        *err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (*err != cudaSuccess) return nullptr;
-        addr[dev] = (float2*)p;
-    }
-    return addr[dev];
+    void* p = nullptr;
+    *err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    return *err == cudaSuccess ? (float2*)p : nullptr;
 }
 
 // Per-pass twiddle block layout of a schedule (the same as the planned path).
@@ -87,20 +80,13 @@ extern "C" FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAllo
                   kMaxSingleN);
         return FFTLIB_ERR_INVALID_DIMENSION;
     }
-    const TwiddlePasses tp = pass_layout(e);
-    if (tp.total > kNoAllocScratch - kNoAllocControl) {
-        set_error("numPoints %u needs %u twiddles, more than the %u the scratch array holds", numPoints, tp.total,
-                  kNoAllocScratch - kNoAllocControl);
-        return FFTLIB_ERR_INVALID_DIMENSION;
-    }
+    const TwiddlePasses tp = pass_layout(e);  // tp.total = N - R[0] < kNoAllocTable (static_assert above)
     if (!is_device_ptr(pX) || !is_device_ptr(pY)) {
         set_error("pX and pY must be device buffers (host buffers would need staging memory)");
         return FFTLIB_ERR_INVALID_VALUE;
     }
-    int dev = 0;
-    cudaError_t err = cudaGetDevice(&dev);
-    if (err != cudaSuccess) return cuda_fail(err, "cudaGetDevice");
-    float2* scratch = scratch_address(dev, &err);
+    cudaError_t err = cudaSuccess;
+    float2* scratch = scratch_address(&err);
     if (!scratch) return cuda_fail(err, "cudaGetSymbolAddress");
     cudaStream_t s = (cudaStream_t)stream;
     uint32_t* errWord = (uint32_t*)scratch;

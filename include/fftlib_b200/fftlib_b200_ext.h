@@ -61,17 +61,25 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync(int16_t *pX
  * real-time loops that must not enter an allocator, or hosts whose allocator
  * belongs to another runtime. The regular _init/_kernel path allocates device
  * memory for plan tables and staging; this call uses only one scratch array
- * that is part of the library image (a static device array of 256 KiB + 256 B,
+ * that is part of the library image (a static device array of 128 KiB + 256 B,
  * held on every GPU that loads the library until the process exits), so it
  * calls no cudaMalloc, cudaFree or other allocator.
  * - pX, pY: device buffers, numChannels rows of numPoints interleaved complex
  *   floats (the layout of FFTLIB_fft1dBatched_i32fc_c32fc_o32fc); pX is not
  *   modified.
- * - numPoints: 2^a 3^b 5^c, at most 16384 (longer or other lengths return
- *   FFTLIB_ERR_INVALID_DIMENSION); stream: a cudaStream_t (NULL = legacy
- *   default stream). The call returns once the result is in pY.
- * - The first call on a device looks up the scratch array's device address
- *   (cudaGetSymbolAddress); make that first call before any stream capture.
+ * - numPoints: 2^a 3^b 5^c, at most 16384, the longest length the
+ *   single-kernel planner accepts (the array holds the twiddle table of any
+ *   such length; longer or other lengths return FFTLIB_ERR_INVALID_DIMENSION);
+ *   stream: a cudaStream_t (NULL = legacy default stream). The call
+ *   synchronizes `stream` and reads the device error word back before it
+ *   returns, so the result is in pY on return.
+ * - Every call looks up the scratch array's device address
+ *   (cudaGetSymbolAddress). The first call in a process builds the host-side
+ *   schedule tables and loads the library's device code on the current
+ *   device; CUDA's lazy module loading (the default) loads each kernel's code
+ *   on its first launch, so make one warm-up call per length at start-up,
+ *   before any stream capture (or run with CUDA_MODULE_LOADING=EAGER), and
+ *   later calls touch no allocator at all.
  * - Every call shares the one array and rebuilds its contents; calls that
  *   overlap on the GPU (other threads or streams) race on it. */
 FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc(FFTLIB_F32 *pX, FFTLIB_F32 *pY,

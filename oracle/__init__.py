@@ -32,12 +32,33 @@ _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _u32 = C.c_uint32
 
 
+REF_ENV = "FFTLIB_REFERENCE_ROOT"
+
+
+def reference_root(ref_root: str | None = None) -> str | None:
+    """The reference tree oracle/_ref is compiled from: the argument, else
+    $FFTLIB_REFERENCE_ROOT, else None (no default location)."""
+    return ref_root or os.environ.get(REF_ENV) or None
+
+
 def build(ref_root: str | None = None, with_ref: bool = True) -> None:
-    """Compile liboracle.so and, if the reference tree exists, oracle/_ref."""
+    """Compile this repository's checkers (liboracle.so, liboracle_gpu.so)
+    and, when a reference tree is named (argument or $FFTLIB_REFERENCE_ROOT),
+    oracle/_ref from the reference's own sources."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    ref_root = ref_root or "/root/reference"
-    if with_ref and os.path.isdir(os.path.join(ref_root, "src")):
-        subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_root}", "all"], check=True)
+    root = reference_root(ref_root)
+    if with_ref and root:
+        build_ref(root)
+
+
+def build_ref(ref_root: str | None = None) -> None:
+    """Compile oracle/_ref from the reference tree; a clear error when none is
+    named or the path holds no reference sources."""
+    root = reference_root(ref_root)
+    if not root or not os.path.isdir(os.path.join(root, "src")):
+        raise RuntimeError(f"oracle/_ref is compiled from the reference's own sources: pass the c7x_fftlib tree "
+                           f"or set {REF_ENV} (got {root!r})")
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={root}", "all"], check=True)
 
 
 _lib = None
@@ -638,3 +659,119 @@ def time_reference_c2c(n: int, channels: int, threads: int | None = None, reps: 
             t.join()
         times.append(time.perf_counter() - t0)
     return float(np.median(times)), threads
+
+
+# --------------------------------------------------------------------------
+# FP64 oracle FFT on the GPU (oracle/fft_f64.cu): the checker for
+# benchmark-size batches. Works on torch CUDA tensors (torch is plumbing
+# here: device memory, streams and the norms of the comparison).
+# --------------------------------------------------------------------------
+
+_glib = None
+
+
+def gpu_lib() -> C.CDLL:
+    global _glib
+    if _glib is None:
+        path = os.path.join(HERE, "liboracle_gpu.so")
+        if not os.path.exists(path):
+            subprocess.run(["make", "-s", "-C", HERE, "liboracle_gpu.so"], check=True)
+        L = C.CDLL(path)
+        L.orc_gpu_fft_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_int,
+                                      C.c_void_p]
+        L.orc_gpu_fft_f64.restype = C.c_int
+        _glib = L
+    return _glib
+
+
+def gpu_fft_f64(x, n: int, batch: int, inverse: bool = False):
+    """FP64 DFT (or scaled inverse DFT) of `batch` rows of n interleaved
+    complex values held in a CUDA tensor (any float dtype); returns a float64
+    CUDA tensor of shape (batch, n, 2)."""
+    import torch
+
+    xd = x.reshape(batch, n, 2).to(torch.float64).contiguous()
+    y = torch.empty_like(xd)
+    w = torch.empty_like(xd)
+    st = torch.cuda.current_stream().cuda_stream
+    rc = gpu_lib().orc_gpu_fft_f64(xd.data_ptr(), y.data_ptr(), w.data_ptr(), n, batch, int(inverse), st)
+    if rc:
+        raise RuntimeError(f"orc_gpu_fft_f64 failed (CUDA error {rc})")
+    return y
+
+
+def gpu_rel_l2_rows(got, ref, batch: int):
+    """(overall rel-L2, largest per-row rel-L2) of `got` against `ref`, both
+    holding `batch` rows (CUDA tensors; compared in FP64). Rows whose
+    reference is all zero count by their absolute error."""
+    import torch
+
+    g = got.reshape(batch, -1).to(torch.float64)
+    r = ref.reshape(batch, -1).to(torch.float64)
+    e = torch.linalg.vector_norm(g - r, dim=1)
+    d = torch.linalg.vector_norm(r, dim=1)
+    overall = float(torch.linalg.vector_norm(e) / torch.linalg.vector_norm(d))
+    per = torch.where(d > 0, e / torch.where(d > 0, d, torch.ones_like(d)), e)
+    return overall, float(per.max())
+
+
+def gpu_check_c2c(x, y, n: int, batch: int, inverse: bool = False, chunk_points: int = 1 << 26):
+    """Checks FP32 results y of a batched c2c (inverse) FFT of x against the
+    GPU FP64 oracle, in chunks of whole rows; returns (overall rel-L2,
+    largest per-row rel-L2)."""
+    import torch
+
+    rows = max(1, chunk_points // max(n, 1))
+    xs = x.reshape(batch, 2 * n)
+    ys = y.reshape(batch, 2 * n)
+    err2 = 0.0
+    ref2 = 0.0
+    worst = 0.0
+    for b0 in range(0, batch, rows):
+        b1 = min(batch, b0 + rows)
+        ref = gpu_fft_f64(xs[b0:b1], n, b1 - b0, inverse)
+        g = ys[b0:b1].to(torch.float64).reshape(b1 - b0, -1)
+        r = ref.reshape(b1 - b0, -1)
+        e = torch.linalg.vector_norm(g - r, dim=1)
+        d = torch.linalg.vector_norm(r, dim=1)
+        err2 += float((e * e).sum())
+        ref2 += float((d * d).sum())
+        per = torch.where(d > 0, e / torch.where(d > 0, d, torch.ones_like(d)), e)
+        worst = max(worst, float(per.max()))
+        del ref, g, r
+    return (err2 ** 0.5) / (ref2 ** 0.5 if ref2 > 0 else 1.0), worst
+
+
+def gpu_fp64_r2c(x, n: int, channels: int, outmode: int = 0):
+    """FP64 spectrum of `channels` rows of n reals (CUDA tensor): the n-point
+    DFT of the real row, its first n/2+1 bins (outmode 0) or all n; returns
+    float64 (channels, bins, 2)."""
+    import torch
+
+    z = torch.zeros(channels, n, 2, dtype=torch.float64, device=x.device)
+    z[..., 0] = x.reshape(channels, n).to(torch.float64)
+    y = gpu_fft_f64(z, n, channels)
+    return y if outmode else y[:, : n // 2 + 1].contiguous()
+
+
+def gpu_fp64_c2r(x, n: int, channels: int, inmode: int = 0):
+    """The reference c2r algorithm in FP64 on the GPU (the same definition as
+    fp64_c2r): Z[i] = X[i] A'[i] + b[i] B'[i], then the n/2-point inverse
+    DFT read as n interleaved reals; returns float64 (channels, n)."""
+    import math
+
+    import torch
+
+    h = n // 2
+    nin = h + 1 if inmode == 0 else n
+    z = x.reshape(channels, nin, 2).to(torch.float64)
+    zc = torch.complex(z[..., 0], z[..., 1])
+    i = torch.arange(h, device=x.device, dtype=torch.float64)
+    t = 2 * math.pi * i / n
+    a = torch.complex(0.5 * (1 - torch.sin(t)), 0.5 * torch.cos(t))
+    bb = torch.complex(0.5 * (1 + torch.sin(t)), -0.5 * torch.cos(t))
+    ii = torch.arange(h, device=x.device)
+    b = torch.conj(zc[:, h - ii]) if inmode == 0 else zc[:, ii + h]
+    zz = zc[:, :h] * a + b * bb
+    y = gpu_fft_f64(torch.view_as_real(zz.contiguous()), h, channels, inverse=True)
+    return y.reshape(channels, n)

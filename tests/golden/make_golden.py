@@ -1,9 +1,9 @@
 """Generate the committed golden fixtures in tests/golden/.
 
-Run in a checkout that has the reference FFTLIB tree (default
-/root/reference) and oracle/_ref built (``make -C oracle all``):
+Run with the reference FFTLIB tree named by --ref or $FFTLIB_REFERENCE_ROOT
+(oracle/_ref is built from it when missing):
 
-    python tests/golden/make_golden.py [--ref /path/to/c7x_fftlib]
+    python tests/golden/make_golden.py --ref /path/to/c7x_fftlib
 
 Outputs (small .npz files; nothing here is read at run time except the
 fixtures themselves):
@@ -322,11 +322,15 @@ def mma_int_static(ref, kernel="FFTLIB_FFT_fft_ixX_cxX_oxX", max_points=None):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="the reference c7x_fftlib tree (default: $FFTLIB_REFERENCE_ROOT)")
     ap.add_argument("--only", default="")
     a = ap.parse_args()
+    a.ref = O.reference_root(a.ref)
+    if not a.ref or not os.path.isdir(os.path.join(a.ref, "src")):
+        ap.error(f"the golden fixtures are read from the reference tree: pass --ref or set {O.REF_ENV} "
+                 f"(got {a.ref!r})")
     if not (O.ref_available() and O.ref1d_available()):
-        O.build(a.ref)
+        O.build_ref(a.ref)
     makers = {
         "r2c_extended": lambda: extended(a.ref, "FFTLIB_fft1dBatched_i32f_c32fc_o32fc", "outmode", 1 << 20),
         "c2r_extended": lambda: extended(a.ref, "FFTLIB_ifft1dBatched_i32fc_c32fc_o32f", "inMode", 1 << 20),

@@ -1,0 +1,183 @@
+"""Parity at the benchmark sizes: every workload bench.py times is checked
+here at the size it is timed at, every transform against the GPU FP64 oracle
+(oracle/fft_f64.cu, itself checked against numpy's FP64 FFT below).
+
+Bound: relative L2 error <= 2e-6 against FP64, for the whole batch and for
+every transform on its own.
+
+* c2c N=4096 x 8192 forward and inverse (the headline launch);
+* r2c then c2r N=4096 x 8192 reals, outmode / inMode 0 (forward, inverse and
+  round trip), the reference's split definitions
+  (FFTLIB_fft1dBatched_i32f_c32fc_o32fc_cn.c:40-121,
+  FFTLIB_ifft1dBatched_i32fc_c32fc_o32f_cn.c:35-87);
+* the 20,000-transform uneven-length batch (the bench's lengths, seed 2024)
+  through the graph-captured persistent launch;
+* the split-FP16 tensor-core DFT at 2^20 rows for N = 8 ... 256 and at
+  N = 4096 x 8192.
+"""
+import numpy as np
+import pytest
+
+import c7x_fftlib_b200 as F
+import fftcall
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+REL_L2 = 2e-6
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    return torch
+
+
+@pytest.mark.parametrize("n,batch", [(1, 5), (2, 7), (7, 3), (12, 33), (60, 9), (256, 16), (3000, 4), (4096, 6),
+                                     (31250, 2), (1 << 20, 1)])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_gpu_fp64_oracle_matches_numpy(torch, n, batch, inverse):
+    x = O.uniform_c2c(n, batch, seed=n + batch)
+    got = O.gpu_fft_f64(torch.from_numpy(x).cuda(), n, batch, inverse).cpu().numpy()
+    want = O.fp64_c2c(x, n, batch, inverse)
+    assert O.rel_l2(got[..., 0] + 1j * got[..., 1], want) <= 1e-13
+
+
+@pytest.mark.parametrize("n,mode", [(64, 0), (64, 1), (4096, 0), (250, 0), (250, 1)])
+def test_gpu_fp64_real_oracles_match_numpy(torch, n, mode):
+    ch = 3
+    x = O.real_signal(n, ch, seed=n)
+    y = O.gpu_fp64_r2c(torch.from_numpy(x).cuda(), n, ch, mode).cpu().numpy()
+    assert O.rel_l2(y[..., 0] + 1j * y[..., 1], O.fp64_r2c(x, n, ch, mode)) <= 1e-13
+    bins = O.uniform_c2c(n if mode else n // 2 + 1, ch, seed=n + 1)
+    xr = O.gpu_fp64_c2r(torch.from_numpy(bins).cuda(), n, ch, mode).cpu().numpy()
+    assert O.rel_l2(xr, O.fp64_c2r(bins, n, ch, mode)) <= 1e-13
+
+
+def _c2c(torch, kind, x, n, ch):
+    w = torch.zeros(2 * n, device="cuda")
+    bX, bW = F.bp(F.FFTLIB_FLOAT32, 2 * n * ch), F.bp(F.FFTLIB_FLOAT32, 2 * n)
+    out = torch.empty_like(x)
+    src = x.clone()  # the kernel may use pX as its work buffer
+    pb = F.pblock(kind)
+    base = F.KERNELS[kind]
+    F.check(F.fn(base + "_init")(F.ptr(src), bX, F.ptr(w), bW, F.ptr(out), bX, n, ch, pb))
+    F.check(F.fn(base + "_kernel")(F.ptr(src), bX, F.ptr(w), bW, F.ptr(out), bX, n, ch, pb))
+    return out
+
+
+@pytest.mark.parametrize("kind", ["c2c", "ifft"])
+def test_headline_c2c_every_channel(torch, kind):
+    n, ch = 4096, 8192
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    x = torch.rand(2 * n * ch, device="cuda", generator=g) * 2 - 1
+    y = _c2c(torch, kind, x, n, ch)
+    overall, worst = O.gpu_check_c2c(x, y, n, ch, inverse=(kind == "ifft"))
+    assert overall <= REL_L2 and worst <= REL_L2, (overall, worst)
+
+
+def _real_workload(torch, n, ch, seed):
+    """N(0,1) noise plus 3 sinusoids per channel (amplitude U[1,10], integer
+    bins U{1..N/2-1}, phase U[0, 2 pi)) generated on the device."""
+    import math
+
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    t = torch.arange(n, device="cuda", dtype=torch.float64)
+    x = torch.randn(ch, n, device="cuda", generator=g, dtype=torch.float64)
+    for _ in range(3):
+        amp = 1 + 9 * torch.rand(ch, 1, device="cuda", generator=g, dtype=torch.float64)
+        k = torch.randint(1, n // 2, (ch, 1), device="cuda", generator=g).to(torch.float64)
+        ph = 2 * math.pi * torch.rand(ch, 1, device="cuda", generator=g, dtype=torch.float64)
+        x += amp * torch.cos(2 * math.pi * k * t / n + ph)
+    return x.to(torch.float32).reshape(-1)
+
+
+def test_r2c_c2r_n4096_x8192_every_channel(torch):
+    n, ch = 4096, 8192
+    h = n // 2
+    x = _real_workload(torch, n, ch, seed=3)
+    yc = torch.empty(2 * (h + 1) * ch, device="cuda")
+    xb = torch.empty(n * ch, device="cuda")
+    b = F.bp(F.FFTLIB_FLOAT32, n * ch)
+    pr, pc = F.pblock("r2c"), F.pblock("c2r")
+    F.check(F.fn(F.KERNELS["r2c"] + "_init")(F.ptr(x), b, F.ptr(x), b, None, b, F.ptr(x), b, F.ptr(yc), b, n, ch, 0,
+                                             pr))
+    F.check(F.fn(F.KERNELS["c2r"] + "_init")(F.ptr(yc), b, F.ptr(yc), b, None, b, F.ptr(yc), b, F.ptr(xb), b, n, ch,
+                                             0, pc))
+    # the asynchronous entries bench.py times (device buffers, no pXFFT)
+    st = torch.cuda.current_stream().cuda_stream
+    F.check(F.fn("FFTLIB_b200_fft1dBatched_i32f_c32fc_o32fc_kernelAsync")(F.ptr(x), None, F.ptr(yc), n, ch, 0, pr,
+                                                                          F.ptr(st)))
+    yc_in = yc.clone()
+    F.check(F.fn("FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32f_kernelAsync")(F.ptr(yc), None, F.ptr(xb), n, ch, 0,
+                                                                           pc, F.ptr(st)))
+    torch.cuda.synchronize()
+    rows = 1024  # FP64 checks in chunks of channels
+    fwd = [0.0, 0.0, 0.0]
+    inv = [0.0, 0.0, 0.0]
+    for c0 in range(0, ch, rows):
+        xs = x.view(ch, n)[c0:c0 + rows]
+        ref = O.gpu_fp64_r2c(xs, n, rows, 0)
+        got = yc.view(ch, h + 1, 2)[c0:c0 + rows]
+        for acc, (g_, r_) in ((fwd, (got, ref)),
+                              (inv, (xb.view(ch, n)[c0:c0 + rows],
+                                     O.gpu_fp64_c2r(yc_in.view(ch, h + 1, 2)[c0:c0 + rows], n, rows, 0)))):
+            e = torch.linalg.vector_norm((g_.to(torch.float64) - r_).reshape(rows, -1), dim=1)
+            d = torch.linalg.vector_norm(r_.reshape(rows, -1), dim=1)
+            acc[0] += float((e * e).sum())
+            acc[1] += float((d * d).sum())
+            acc[2] = max(acc[2], float((e / d).max()))
+    for name, acc in (("r2c", fwd), ("c2r", inv)):
+        overall = (acc[0] / acc[1]) ** 0.5
+        assert overall <= REL_L2 and acc[2] <= REL_L2, (name, overall, acc[2])
+    # round trip, every channel
+    e = torch.linalg.vector_norm((xb - x).view(ch, n).double(), dim=1)
+    d = torch.linalg.vector_norm(x.view(ch, n).double(), dim=1)
+    assert float((e / d).max()) <= REL_L2
+
+
+@pytest.mark.parametrize("inverse", [False, True])
+def test_mixed_20000_bench_set_every_transform(torch, inverse):
+    lengths = np.sort(fftcall.mixed_lengths(20000, seed=2024))[::-1].copy()
+    total = int(lengths.sum())
+    g = torch.Generator(device="cuda").manual_seed(7)
+    x = torch.rand(2 * total, device="cuda", generator=g) * 2 - 1
+    y = torch.empty_like(x)
+    mb = F.MixedBatch(lengths, inverse=inverse)
+    st = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):  # the graph is replayed, as in the bench
+        mb.exec(x, y, F.ptr(st))
+    torch.cuda.synchronize()
+    uniq, counts = np.unique(lengths, return_counts=True)
+    off = 0
+    err2 = ref2 = 0.0
+    for n, c in sorted(zip(uniq.tolist(), counts.tolist()), reverse=True):
+        seg = slice(2 * off, 2 * (off + n * c))
+        ref = O.gpu_fft_f64(x[seg], n, c, inverse)
+        e = torch.linalg.vector_norm((y[seg].view(c, n, 2).double() - ref).reshape(c, -1), dim=1)
+        d = torch.linalg.vector_norm(ref.reshape(c, -1), dim=1)
+        worst = float((e / d).max())
+        assert worst <= REL_L2, (n, worst)
+        err2 += float((e * e).sum())
+        ref2 += float((d * d).sum())
+        off += n * c
+    assert off == total
+    assert (err2 / ref2) ** 0.5 <= REL_L2
+    mb.close()
+
+
+@pytest.mark.parametrize("n,rows", [(8, 1 << 20), (16, 1 << 20), (32, 1 << 20), (64, 1 << 20), (128, 1 << 20),
+                                    (256, 1 << 20), (4096, 8192)])
+def test_tc_dft_bench_rows_every_transform(torch, n, rows):
+    g = torch.Generator(device="cuda").manual_seed(5 + n)
+    x = torch.rand(2 * n * rows, device="cuda", generator=g) * 2 - 1
+    y = torch.empty_like(x)
+    d = F.DftMma(n, rows, F.FFTLIB_FUNCTION_OPTIMIZED)
+    assert d.path == F.MMA_PATH_TC
+    d.exec(x, y)
+    torch.cuda.synchronize()
+    overall, worst = O.gpu_check_c2c(x, y, n, rows)
+    assert overall <= REL_L2 and worst <= REL_L2, (overall, worst)

@@ -21,6 +21,13 @@ CASES = [(4, 3, 1), (8, 2, 0), (16, 4, 1), (16, 1, 0), (32, 8, 1), (32, 4, 0), (
          (16, 1000, 1), (32, 777, 0), (256, 300, 1), (65536, 1, 1)]
 
 
+# Shifts that reach every branch of the tensor-core kernels' 32-bit rounding:
+# exactly 8 (the low byte folds in), 9..37 (a partial shift of the folded
+# value), the cap at 37 and above, and values with bits above the low byte
+# (the reference's shift arithmetic keeps only the low byte).
+WIDE_SHIFTS = ([8] * 5, [16] * 5, [24] * 5, [37] * 5, [40] * 5, [0x108] * 5, [8, 16, 0x108, 24, 9])
+
+
 @pytest.fixture(scope="module")
 def torch_cuda():
     import torch
@@ -61,7 +68,7 @@ def test_bit_exact_with_oracle_and_reference_cn(torch_cuda, bits, n, batch, il):
         pytest.skip("not a d0 x 8^L length within four stages")
     for seed, full in ((1, False), (2, True)):
         x = _rand(bits, 2 * n * batch, 7 * n + seed, full)
-        for sh in ([1, 1, 1, 1, 1], [4, 4, 4, 4, 4], [0, 0, 0, 0, 0], [bits - 1] * 5, [0, 3, 1, 2, 5]):
+        for sh in ([1, 1, 1, 1, 1], [4, 4, 4, 4, 4], [0, 0, 0, 0, 0], [bits - 1] * 5, [0, 3, 1, 2, 5]) + WIDE_SHIFTS:
             y = run(torch_cuda, bits, n, batch, il, sh, x)
             want = O.mma_exec(bits, n, batch, il, sh, x)
             assert np.array_equal(y, want), (bits, n, batch, il, sh, full)
@@ -144,7 +151,7 @@ def test_high_radix_tensor_core_stages_agree(torch_cuda, n, batch, il):
     x[1::37] = -32768
     x[0::53] = -32768
     x[3::41] = 32767
-    for sh in ([0] * 5, [15] * 5, [2, 2, 2, 2, 4], [1, 3, 0, 2, 5]):
+    for sh in ([0] * 5, [15] * 5, [2, 2, 2, 2, 4], [1, 3, 0, 2, 5]) + WIDE_SHIFTS:
         try:
             L.FFTLIB_b200_FFT_setIntTensorCores(0)
             y_cc = run(torch_cuda, 16, n, batch, il, sh, x)

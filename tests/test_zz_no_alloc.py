@@ -51,6 +51,26 @@ def test_no_alloc_matches_kernel_on_consecutive_calls(torch):
         assert O.rel_l2(y, O.fp64_c2c(x, n, ch)) <= REL_L2, (n, ch)
 
 
+def test_no_alloc_allocates_no_device_memory(torch):
+    """After a warm-up call of each length (CUDA loads a kernel's code on its
+    first launch), calls of those lengths leave the device's free memory
+    exactly unchanged."""
+    fn = F.fn("FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc")
+    cases = [(4096, 64), (960, 33), (16384, 4), (12, 500), (3000, 9)]
+    bufs = [(torch.rand(2 * n * ch, device="cuda") * 2 - 1, torch.empty(2 * n * ch, device="cuda"), n, ch)
+            for n, ch in cases]
+    for x, y, n, ch in bufs:
+        F.check(fn(F.ptr(x), F.ptr(y), n, ch, None), "kernelNoAlloc warm-up")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        for x, y, n, ch in bufs:
+            F.check(fn(F.ptr(x), F.ptr(y), n, ch, None), "kernelNoAlloc")
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
 def test_no_alloc_rejects_lengths_beyond_its_scratch(torch):
     X = torch.zeros(2 * 31250, device="cuda")
     fn = F.fn("FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc")
