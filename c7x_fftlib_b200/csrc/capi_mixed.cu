@@ -5,8 +5,9 @@
 // (heuristic, or timed by the autotuner), builds the device tables (group
 // schedules, tiles ordered by cost, per-transform offsets) and the group
 // twiddle tables. exec() replays a CUDA graph holding the counter reset and
-// the single persistent launch; execPerSize() launches the same kernel once
-// per distinct length, for comparison.
+// persistent launches (one per kernel class present, on parallel branches);
+// execPerSize() launches the same kernels once per distinct length, for
+// comparison.
 #include <string.h>
 
 #include <algorithm>
@@ -27,19 +28,23 @@ struct FFTLIB_b200_mixed {
     uint32_t count = 0;
     uint32_t flags = 0;
     std::vector<uint32_t> groupN;
+    std::vector<int> groupCls;
     std::vector<EnginePlan> groupPlan;
     std::vector<uint32_t> groupM;
     std::vector<uint32_t> groupTileBegin, groupTileEnd; // ranges in dTilesByGroup
     std::vector<float2*> groupTw;
     MixedGroup* dGroups = nullptr;
-    MixedTile* dTiles = nullptr;        // ordered by cost (persistent launch)
+    MixedTile* dTiles = nullptr;        // per class, most expensive first (persistent launches)
     MixedTile* dTilesByGroup = nullptr; // grouped (per-size launches)
     uint64_t* dOffsets = nullptr;
-    uint32_t* dCounter = nullptr;
     uint32_t numTiles = 0;
-    size_t smem = 0;
-    uint32_t grid = 0;
-    cudaStream_t capture = nullptr;
+    // per class: its tiles in dTiles, stage length, shared memory, grid
+    uint32_t clsTileBegin[kMixedClasses] = {}, clsTiles[kMixedClasses] = {};
+    uint32_t clsStage[kMixedClasses] = {};
+    uint32_t groupStage = 0;            // largest stage of any group (per-size launches)
+    uint32_t clsGrid[kMixedClasses] = {};
+    cudaStream_t capture = nullptr, side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     const void* gx = nullptr;
@@ -50,16 +55,66 @@ namespace {
 
 constexpr uint32_t kMixedMaxT = 256;
 
+// Transforms per tile: enough to give the CTA its 256 threads, as many as
+// one shared-memory stage holds.
 FftArgs group_args(const EnginePlan& e, const float2* tw, bool inverse)
 {
     FftArgs a = engine_args(e, tw);
     a.inElem = a.outElem = 1; // rows are addressed through the offsets table
     a.conjIn = a.conjOut = inverse ? 1 : 0;
     a.scale = inverse ? 1.0f / (float)e.n : 1.0f;
-    uint32_t M = std::max(1u, (uint32_t)mixed_block() / e.T);
-    M = std::min(M, std::max(1u, (48u * 1024u) / (a.slen * 8u)));
+    a.err = error_word().dev;
+    uint32_t M = std::max(1u, mixed_block() / e.T);
+    M = std::min(M, std::max(1u, mixed_stage_max_bytes() / (a.slen * 8u)));
     a.M = M;
     return a;
+}
+
+// Complex values of the stage a group's tiles need (even: stages start on
+// 16-byte boundaries).
+uint32_t stage_len(const FftArgs& a) { return (a.M * a.slen + 1u) & ~1u; }
+
+// How a tile of `count` transforms whose offsets start at offs reaches
+// shared memory (kTileBulk / kTileRows / plain loads).
+uint32_t tile_flags(const uint64_t* offs, uint32_t count, uint32_t n)
+{
+    bool contiguous = (offs[0] % 2u) == 0 && ((uint64_t)count * n) % 2u == 0;
+    bool rows = (n % 2u) == 0;
+    for (uint32_t m = 0; m < count; ++m) {
+        if (offs[m] != offs[0] + (uint64_t)m * n) contiguous = false;
+        if (offs[m] % 2u) rows = false;
+    }
+    return contiguous ? kTileBulk : rows ? kTileRows : 0u;
+}
+
+int class_of(const EnginePlan& e) { return e.emax > 16 ? kMixedW20 : kMixedW16; }
+
+MixedLaunch class_launch(int cls, const MixedGroup* groups, const MixedTile* tiles, uint32_t numTiles,
+                         const uint64_t* offsets, const float* x, float* y, uint32_t stageLen, uint32_t grid)
+{
+    MixedLaunch L{};
+    L.cls = cls;
+    L.groups = groups;
+    L.tiles = tiles;
+    L.numTiles = numTiles;
+    L.offsets = offsets;
+    L.x = (const float2*)x;
+    L.y = (float2*)y;
+    L.err = error_word().dev;
+    L.stageLen = stageLen;
+    L.smem = mixed_smem(stageLen);
+    L.grid = std::max(1u, std::min(grid, numTiles));
+    return L;
+}
+
+// Resident CTAs of a class's kernel with this stage length, over the device.
+cudaError_t class_grid(int cls, uint32_t stageLen, int device, uint32_t* grid)
+{
+    int resident = 0, sms = 0;
+    cudaError_t err = mixed_configure(cls, mixed_smem(stageLen), &resident);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    *grid = (uint32_t)std::max(1, resident * sms);
+    return err;
 }
 
 // Autotuner timer: one group of `batch` contiguous transforms through the
@@ -71,39 +126,31 @@ float time_mixed_group(const EnginePlan& e, float2* x, float2* y, uint32_t batch
     MixedGroup* dg = nullptr;
     MixedTile* dt = nullptr;
     uint64_t* doff = nullptr;
-    uint32_t* cnt = nullptr;
     float ms = 0.f;
     cudaError_t err = make_pass_table(&tw, e, s);
     const FftArgs a = group_args(e, tw, false);
-    std::vector<MixedTile> tiles;
-    for (uint32_t b = 0; b < batch; b += a.M) tiles.push_back(MixedTile{0, b, std::min(a.M, batch - b), 0});
     std::vector<uint64_t> offs(batch);
     for (uint32_t i = 0; i < batch; ++i) offs[i] = (uint64_t)i * e.n;
+    std::vector<MixedTile> tiles;
+    for (uint32_t b = 0; b < batch; b += a.M) {
+        const uint32_t c = std::min(a.M, batch - b);
+        tiles.push_back(MixedTile{0, b, c, tile_flags(&offs[b], c, e.n)});
+    }
     const MixedGroup g{a};
+    const int cls = class_of(e);
     if (err == cudaSuccess) err = cudaMalloc(&dg, sizeof(g));
     if (err == cudaSuccess) err = cudaMalloc(&dt, tiles.size() * sizeof(MixedTile));
     if (err == cudaSuccess) err = cudaMalloc(&doff, offs.size() * sizeof(uint64_t));
-    if (err == cudaSuccess) err = cudaMalloc(&cnt, sizeof(uint32_t));
     if (err == cudaSuccess) err = cudaMemcpy(dg, &g, sizeof(g), cudaMemcpyHostToDevice);
     if (err == cudaSuccess) err = cudaMemcpy(dt, tiles.data(), tiles.size() * sizeof(MixedTile), cudaMemcpyHostToDevice);
     if (err == cudaSuccess) err = cudaMemcpy(doff, offs.data(), offs.size() * sizeof(uint64_t), cudaMemcpyHostToDevice);
-    int resident = 0, sms = 0;
-    const size_t smem = (size_t)a.M * a.slen * 8u;
     int dev = 0;
+    uint32_t grid = 1;
     if (err == cudaSuccess) err = cudaGetDevice(&dev);
-    if (err == cudaSuccess) err = mixed_configure(smem, &resident);
-    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (err == cudaSuccess) err = class_grid(cls, stage_len(a), dev, &grid);
     if (err == cudaSuccess) {
-        MixedLaunch L{};
-        L.groups = dg;
-        L.tiles = dt;
-        L.numTiles = (uint32_t)tiles.size();
-        L.offsets = doff;
-        L.x = x;
-        L.y = y;
-        L.counter = cnt;
-        L.grid = std::min<uint32_t>(L.numTiles, (uint32_t)std::max(1, resident * sms));
-        L.smem = smem;
+        const MixedLaunch L = class_launch(cls, dg, dt, (uint32_t)tiles.size(), doff, (const float*)x, (float*)y,
+                                           stage_len(a), grid);
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -111,7 +158,7 @@ float time_mixed_group(const EnginePlan& e, float2* x, float2* y, uint32_t batch
         cudaEventRecord(e0, s);
         for (int r = 0; r < 5 && err == cudaSuccess; ++r) err = launch_mixed(L, s);
         cudaEventRecord(e1, s);
-        if (err == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess) {
+        if (err == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess && !take_device_error()) {
             cudaEventElapsedTime(&ms, e0, e1);
             ms /= 5.f;
             *ok = true;
@@ -125,18 +172,24 @@ float time_mixed_group(const EnginePlan& e, float2* x, float2* y, uint32_t batch
     cudaFree(dg);
     cudaFree(dt);
     cudaFree(doff);
-    cudaFree(cnt);
     return ms;
 }
 
+// The group's schedule: the 16-wide class when a schedule of at most 256
+// threads per transform exists there, else the 20-wide class.
 bool mixed_schedule(uint32_t n, uint32_t batch, bool tune, EnginePlan* e)
 {
     if (!is_235(n) || n > kMaxSingleN) return false;
-    if (tune && tune_schedule(n, batch, mixed_emax(), kMixedMaxT, e, &time_mixed_group)) return true;
-    std::vector<EnginePlan> c = engine_candidates(n, mixed_emax(), kMixedMaxT);
-    if (c.empty()) return false;
-    *e = c.front();
-    return true;
+    for (int cls = 0; cls < kMixedClasses; ++cls) {
+        const int emax = mixed_class_emax(cls);
+        if (tune && tune_schedule(n, batch, emax, kMixedMaxT, e, &time_mixed_group)) return true;
+        std::vector<EnginePlan> c = engine_candidates(n, emax, kMixedMaxT);
+        if (!c.empty()) {
+            *e = c.front();
+            return true;
+        }
+    }
+    return false;
 }
 
 void release(FFTLIB_b200_mixed* h)
@@ -146,29 +199,39 @@ void release(FFTLIB_b200_mixed* h)
     if (h->exec) cudaGraphExecDestroy(h->exec);
     if (h->graph) cudaGraphDestroy(h->graph);
     if (h->capture) cudaStreamDestroy(h->capture);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
     for (float2* t : h->groupTw) cudaFree(t);
     cudaFree(h->dGroups);
     cudaFree(h->dTiles);
     cudaFree(h->dTilesByGroup);
     cudaFree(h->dOffsets);
-    cudaFree(h->dCounter);
     delete h;
 }
 
-MixedLaunch launch_desc(const FFTLIB_b200_mixed* h, const MixedTile* tiles, uint32_t numTiles, const float* x,
-                        float* y)
+// The persistent launches of every class that has tiles: the W20 class (few
+// lengths) on a side branch, the W16 class on the main one, joined again.
+cudaError_t enqueue_classes(FFTLIB_b200_mixed* h, const float* x, float* y, cudaStream_t s)
 {
-    MixedLaunch L{};
-    L.groups = h->dGroups;
-    L.tiles = tiles;
-    L.numTiles = numTiles;
-    L.offsets = h->dOffsets;
-    L.x = (const float2*)x;
-    L.y = (float2*)y;
-    L.counter = h->dCounter;
-    L.grid = std::min(h->grid, numTiles);
-    L.smem = h->smem;
-    return L;
+    const bool both = h->clsTiles[kMixedW16] && h->clsTiles[kMixedW20];
+    cudaError_t err = cudaSuccess;
+    if (both) {
+        err = cudaEventRecord(h->fork, s);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(h->side, h->fork, 0);
+    }
+    for (int cls = kMixedClasses - 1; cls >= 0 && err == cudaSuccess; --cls) {
+        if (!h->clsTiles[cls]) continue;
+        const cudaStream_t cs = (both && cls == kMixedW20) ? h->side : s;
+        err = launch_mixed(class_launch(cls, h->dGroups, h->dTiles + h->clsTileBegin[cls], h->clsTiles[cls],
+                                        h->dOffsets, x, y, h->clsStage[cls], h->clsGrid[cls]),
+                           cs);
+    }
+    if (both && err == cudaSuccess) {
+        err = cudaEventRecord(h->join, h->side);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(s, h->join, 0);
+    }
+    return err;
 }
 
 } // namespace
@@ -222,27 +285,39 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
         h->groupTw.push_back(tw);
         const FftArgs a = group_args(e, tw, inverse);
         const uint32_t M = a.M;
-        h->smem = std::max(h->smem, (size_t)M * a.slen * 8u);
+        const int cls = class_of(e);
+        h->clsStage[cls] = std::max(h->clsStage[cls], stage_len(a));
+        h->groupStage = std::max(h->groupStage, stage_len(a));
         const uint32_t g = (uint32_t)groups.size();
         groups.push_back(MixedGroup{a});
         h->groupN.push_back(n);
+        h->groupCls.push_back(cls);
         h->groupPlan.push_back(e);
         h->groupM.push_back(M);
         h->groupTileBegin.push_back((uint32_t)tiles.size());
         const uint32_t first = (uint32_t)offsByGroup.size();
         for (uint32_t i : kv.second) offsByGroup.push_back(offset[i]);
         const uint32_t cnt = (uint32_t)kv.second.size();
-        for (uint32_t b = 0; b < cnt; b += M) tiles.push_back(MixedTile{g, first + b, std::min(M, cnt - b), 0});
+        for (uint32_t b = 0; b < cnt; b += M) {
+            const uint32_t c = std::min(M, cnt - b);
+            tiles.push_back(MixedTile{g, first + b, c, tile_flags(&offsByGroup[first + b], c, n)});
+        }
         h->groupTileEnd.push_back((uint32_t)tiles.size());
     }
     h->numTiles = (uint32_t)tiles.size();
-    // persistent order: most expensive tiles first (groups are already in
-    // decreasing length; within a group full tiles first)
-    std::vector<MixedTile> lpt = tiles;
-    std::stable_sort(lpt.begin(), lpt.end(), [&](const MixedTile& a, const MixedTile& b) {
-        const double ca = (double)h->groupN[a.group] * a.count, cb = (double)h->groupN[b.group] * b.count;
-        return ca > cb;
-    });
+    // persistent order, per class: most expensive tiles first (groups are
+    // already in decreasing length; within a group full tiles first)
+    std::vector<MixedTile> lpt;
+    for (int cls = 0; cls < kMixedClasses; ++cls) {
+        h->clsTileBegin[cls] = (uint32_t)lpt.size();
+        for (const MixedTile& t : tiles)
+            if (h->groupCls[t.group] == cls) lpt.push_back(t);
+        std::stable_sort(lpt.begin() + h->clsTileBegin[cls], lpt.end(), [&](const MixedTile& a, const MixedTile& b) {
+            const double ca = (double)h->groupN[a.group] * a.count, cb = (double)h->groupN[b.group] * b.count;
+            return ca > cb;
+        });
+        h->clsTiles[cls] = (uint32_t)lpt.size() - h->clsTileBegin[cls];
+    }
     cudaError_t err = cudaSuccess;
     auto upload = [&](void** dst, const void* src, size_t bytes) {
         if (err != cudaSuccess) return;
@@ -253,17 +328,23 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
     upload((void**)&h->dTiles, lpt.data(), lpt.size() * sizeof(MixedTile));
     upload((void**)&h->dTilesByGroup, tiles.data(), tiles.size() * sizeof(MixedTile));
     upload((void**)&h->dOffsets, offsByGroup.data(), offsByGroup.size() * sizeof(uint64_t));
-    if (err == cudaSuccess) err = cudaMalloc(&h->dCounter, sizeof(uint32_t));
-    int resident = 0, sms = 0;
-    if (err == cudaSuccess) err = mixed_configure(h->smem, &resident);
-    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    for (int cls = 0; cls < kMixedClasses && err == cudaSuccess; ++cls) {
+        if (h->clsTiles[cls]) err = class_grid(cls, h->clsStage[cls], h->device, &h->clsGrid[cls]);
+    }
+    // per-size launches use the largest stage of any group with both classes
+    for (int cls = 0; cls < kMixedClasses && err == cudaSuccess; ++cls) {
+        uint32_t unused = 0;
+        if (h->clsTiles[cls]) err = class_grid(cls, h->groupStage, h->device, &unused);
+    }
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&h->capture, cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
     if (err == cudaSuccess) err = cudaStreamSynchronize(s);
     if (err != cudaSuccess) {
         release(h);
         return cuda_fail(err, "mixed plan");
     }
-    h->grid = (uint32_t)std::max(1, resident * sms);
     *handle = h;
     return FFTLIB_SUCCESS;
 }
@@ -274,6 +355,10 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_exec(FFTLIB_b200_mixedHandle h, const FFTLIB_
     if (!h || !pX || !pY) return FFTLIB_ERR_NULL_POINTER;
     if (h->numTiles == 0) return FFTLIB_SUCCESS;
     DeviceScope scope(h->device);
+    if (take_device_error()) {
+        set_error("a device-side wait of an earlier launch timed out");
+        return FFTLIB_ERR_FAILURE;
+    }
     cudaError_t err = cudaSuccess;
     if (!h->exec || h->gx != pX || h->gy != pY) {
         // capture the counter reset and the persistent launch for these buffers
@@ -283,7 +368,7 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_exec(FFTLIB_b200_mixedHandle h, const FFTLIB_
         h->graph = nullptr;
         err = cudaStreamBeginCapture(h->capture, cudaStreamCaptureModeThreadLocal);
         if (err == cudaSuccess) {
-            cudaError_t le = launch_mixed(launch_desc(h, h->dTiles, h->numTiles, pX, pY), h->capture);
+            cudaError_t le = enqueue_classes(h, pX, pY, h->capture);
             err = cudaStreamEndCapture(h->capture, &h->graph);
             if (err == cudaSuccess) err = le;
         }
@@ -303,7 +388,10 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_execPerSize(FFTLIB_b200_mixedHandle h, const 
     DeviceScope scope(h->device);
     for (size_t g = 0; g < h->groupN.size(); ++g) {
         const uint32_t b = h->groupTileBegin[g], e = h->groupTileEnd[g];
-        cudaError_t err = launch_mixed(launch_desc(h, h->dTilesByGroup + b, e - b, pX, pY), (cudaStream_t)stream);
+        const int cls = h->groupCls[g];
+        cudaError_t err = launch_mixed(class_launch(cls, h->dGroups, h->dTilesByGroup + b, e - b, h->dOffsets, pX, pY,
+                                                    h->groupStage, h->clsGrid[cls]),
+                                       (cudaStream_t)stream);
         if (err != cudaSuccess) return cuda_fail(err, "mixed per-size launch");
     }
     return FFTLIB_SUCCESS;
@@ -313,8 +401,11 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_describe(FFTLIB_b200_mixedHandle h, char* buf
 {
     if (!h || !buf || len == 0) return FFTLIB_ERR_NULL_POINTER;
     std::ostringstream os;
-    os << h->count << " transforms, " << h->groupN.size() << " lengths, " << h->numTiles << " tiles, grid "
-       << h->grid << ", smem " << h->smem;
+    os << h->count << " transforms, " << h->groupN.size() << " lengths, " << h->numTiles << " tiles";
+    for (int cls = 0; cls < kMixedClasses; ++cls)
+        if (h->clsTiles[cls])
+            os << "; class E" << mixed_class_emax(cls) << ": " << h->clsTiles[cls] << " tiles, grid " << h->clsGrid[cls]
+               << ", stage " << h->clsStage[cls] * 8u << " B";
     for (size_t g = 0; g < h->groupN.size(); ++g)
         os << "; " << describe(h->groupPlan[g]) << " M=" << h->groupM[g] << " tiles="
            << (h->groupTileEnd[g] - h->groupTileBegin[g]);

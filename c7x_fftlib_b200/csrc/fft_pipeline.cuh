@@ -34,6 +34,12 @@ FFT_DEV void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
                  : "memory");
 }
 
+// Plain arrival (no transaction bytes): completes a phase of count 1.
+FFT_DEV void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 FFT_DEV bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 {
     uint32_t done;
@@ -248,9 +254,9 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
     if (s_fail && tid == 0) {
         *(volatile uint32_t*)a.err = kErrPipelineTimeout;
         // drain every copy still in flight (bounded): the failed one and the
-        // STAGES-2 issued after it
-        for (int k = 0; k + 1 < STAGES; ++k) {
-            const uint32_t itk = it + (uint32_t)k;
+        // STAGES-2 issued after it, or at it = 0 every initial stage
+        const uint32_t last = it == 0 ? (uint32_t)STAGES - 1u : it + (uint32_t)STAGES - 2u;
+        for (uint32_t itk = it; itk <= last; ++itk) {
             const uint32_t tile = blockIdx.x + itk * G;
             if (tile < tiles) mbar_wait_bounded(&bar[itk % STAGES], (itk / STAGES) & 1u);
         }

@@ -103,10 +103,11 @@ FFT_DEV uint32_t swz_step(uint32_t swzBase, uint32_t idx0, uint32_t q, uint32_t 
 }
 
 // raw: when not null, the first pass reads its input from this unpadded
-// shared-memory copy of the transform (filled by a bulk async copy).
+// shared-memory copy of the transform (filled by a bulk async copy);
+// RAW_FIRST: raw is never null (only that path is compiled).
 // afterGather runs right after the barrier that ends the pass's reads.
 // rowIn / rowOut: this lane's transform in HBM (first / last pass).
-template <int EMAX, int R, class Hook = NoHook>
+template <int EMAX, int R, class Hook = NoHook, bool RAW_FIRST = false>
 FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, const bool last,
                       const uint32_t T, float2 (&v)[EMAX], float2* sm, uint32_t t, bool active,
                       const float2* rowIn, float2* rowOut, const float2* raw = nullptr,
@@ -123,10 +124,10 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
             static_for<R>([&](auto q) {
                 const uint32_t idx = j + (uint32_t)q * nb;
                 float2 z;
-                if (first && raw) {
+                if (first && (RAW_FIRST || raw)) {
                     z = raw[idx];
                     if (a.conjIn) z = cconj(z);
-                } else if (first) {
+                } else if (first && !RAW_FIRST) {
                     z = (active || a.staged) ? load_in(a, rowIn, idx, sm) : make_float2(0.f, 0.f);
                 } else {
                     z = sm[swz_step(sj, j, (uint32_t)q, nb)];
@@ -171,7 +172,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
         }
         return;
     }
-    if (!first || a.staged || raw) {
+    if (!first || a.staged || RAW_FIRST || raw) {
         __syncthreads(); // every read of this pass is done
         afterGather();
     }

@@ -105,11 +105,6 @@ FFT_DEV void tmem_ld8(uint32_t taddr, float (&f)[8])
     for (int i = 0; i < 8; ++i) f[i] = __uint_as_float(r[i]);
 }
 
-FFT_DEV void mbar_arrive(uint64_t* bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-
 // Named barrier over `count` threads that also ORs a predicate across them:
 // every participant returns the same value.
 FFT_DEV bool group_sync_or(uint32_t id, uint32_t count, bool pred)

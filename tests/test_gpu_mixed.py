@@ -98,3 +98,19 @@ def test_mixed_autotuned(torch, tmp_path, monkeypatch):
     check_all(x, Y.cpu().numpy(), lengths)
     assert os.path.exists(tmp_path / "tune.txt")
     assert len(open(tmp_path / "tune.txt").read().splitlines()) >= len(set(lengths.tolist())) - 1
+
+
+def test_mixed_buffers_off_16_byte_boundary(torch):
+    """pX and pY 8 bytes past a 16-byte boundary: no tile may be bulk-copied,
+    the threads copy every tile in; results as for aligned buffers."""
+    lengths = np.array([4096, 60, 60, 12, 3888, 960, 1536, 240] * 11, np.uint32)
+    total = int(lengths.sum())
+    x = O.uniform_c2c(total, 1, seed=21)
+    X = torch.zeros(2 * total + 4, device="cuda")
+    X[2:2 + 2 * total] = torch.from_numpy(x).cuda()
+    Y = torch.zeros_like(X)
+    mb = F.MixedBatch(lengths)
+    mb.exec(X.data_ptr() + 8, Y.data_ptr() + 8)
+    torch.cuda.synchronize()
+    check_all(x, Y[2:2 + 2 * total].cpu().numpy(), lengths)
+    mb.close()
