@@ -6,6 +6,7 @@
 #include <string>
 
 #include "capi_common.h"
+#include "fft_engine.h"
 #include "fft_c7x.h"
 #include "fft_i16.h"
 #include "fftlib_b200_ext.h"
@@ -95,7 +96,8 @@ FFTLIB_STATUS FFTLIB_b200_describePlan(uint32_t numPoints, char* buf, uint32_t l
     int G = 0;
     uint32_t R[kMaxGlobal];
     if (plan_engine(numPoints, &e)) {
-        s = describe(e);
+        s = describe(e) + (static_max_threads(numPoints, e.emax, e.T, e.P, e.R) ? " (fixed-size kernel)"
+                                                                              : " (runtime-radix engine)");
     } else if (split_global(numPoints, &G, R)) {
         s = "global passes";
         for (int g = 0; g < G; ++g) {

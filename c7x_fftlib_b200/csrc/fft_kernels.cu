@@ -53,6 +53,14 @@ int engine_max_threads(int emax)
 void register_static_a(std::vector<StaticEntry>& out);
 void register_static_b(std::vector<StaticEntry>& out);
 void register_static_c(std::vector<StaticEntry>& out);
+void register_static_d(std::vector<StaticEntry>& out);
+void register_static_e(std::vector<StaticEntry>& out);
+void register_static_f(std::vector<StaticEntry>& out);
+void register_static_g(std::vector<StaticEntry>& out);
+void register_static_h(std::vector<StaticEntry>& out);
+void register_static_i(std::vector<StaticEntry>& out);
+void register_static_j(std::vector<StaticEntry>& out);
+void register_static_k(std::vector<StaticEntry>& out);
 
 const std::vector<StaticEntry>& static_schedules()
 {
@@ -61,6 +69,14 @@ const std::vector<StaticEntry>& static_schedules()
         register_static_a(t);
         register_static_b(t);
         register_static_c(t);
+        register_static_d(t);
+        register_static_e(t);
+        register_static_f(t);
+        register_static_g(t);
+        register_static_h(t);
+        register_static_i(t);
+        register_static_j(t);
+        register_static_k(t);
         return t;
     }();
     return table;
@@ -102,7 +118,7 @@ cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
                             (a.ioMode == IO_C2R_SPLIT && !a.realMode && a.inBatch == (int64_t)a.N + 1 && a.N >= 64u);
         const bool pipelinable = st->launchPipelined && a.err && rowsOk && !a.batchMinor && !a.perCh &&
                                  a.inElem == 1 && a.outElem == 1 && ((uintptr_t)a.in & 15u) == 0 &&
-                                 (a.N % 2u) == 0;
+                                 ((a.N % 2u) == 0 || a.ioMode == IO_C2C);
         if (pipelinable) {
             FftArgs b = a;
             b.staged = 0;

@@ -100,12 +100,19 @@ __host__ __device__ constexpr size_t pipe_smem_bytes(uint32_t n, int stages, int
 __host__ __device__ constexpr int pipe_tile(int t) { return t >= 128 ? 1 : (256 / t < 1 ? 1 : 256 / t); }
 
 // CTAs per SM the kernel is compiled for: as many as the shared memory
-// (228 KB per SM, 1 KB reserved per CTA) and 2048 threads allow, at most 8.
-__host__ __device__ constexpr int pipe_min_blocks(uint32_t n, int threads, int stages, int m = 1)
+// (228 KB per SM, 1 KB reserved per CTA) and 2048 threads allow, at most 8;
+// with regFloor > 0 also few enough to leave every thread that many of the
+// SM's 65,536 registers (schedules with radix-9/12 passes need about 100 and
+// spill when the shared-memory bound alone caps them near 40).
+__host__ __device__ constexpr int pipe_min_blocks(uint32_t n, int threads, int stages, int m = 1, int regFloor = 0)
 {
     const int bySmem = (int)((228u * 1024u) / (pipe_smem_bytes(n, stages, m) + 1024u));
     const int byThreads = 2048 / threads;
-    const int b = bySmem < byThreads ? bySmem : byThreads;
+    int b = bySmem < byThreads ? bySmem : byThreads;
+    if (regFloor > 0) {
+        const int byRegs = 65536 / (((threads + 31) / 32) * 32 * regFloor);
+        b = b < byRegs ? b : byRegs;
+    }
     return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
 

@@ -45,8 +45,9 @@ cudaError_t launch_static(const FftArgs& a, cudaStream_t s)
     return cudaGetLastError();
 }
 
-template <class S, int STAGES>
-__global__ void __launch_bounds__(S::T * pipe_tile(S::T), pipe_min_blocks(S::N, S::T * pipe_tile(S::T), STAGES, pipe_tile(S::T)))
+template <class S, int STAGES, int REGFLOOR = 0>
+__global__ void __launch_bounds__(S::T * pipe_tile(S::T),
+                                  pipe_min_blocks(S::N, S::T * pipe_tile(S::T), STAGES, pipe_tile(S::T), REGFLOOR))
     k_fft_pipe(const __grid_constant__ FftArgs a)
 {
     fft_pipeline<S, STAGES, pipe_tile(S::T)>(a);
@@ -54,7 +55,7 @@ __global__ void __launch_bounds__(S::T * pipe_tile(S::T), pipe_min_blocks(S::N, 
 
 // Persistent pipelined launch (pipe_tile(T) transforms per tile): as many
 // CTAs as are resident on the device.
-template <class S, int STAGES>
+template <class S, int STAGES, int REGFLOOR = 0>
 cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
 {
     constexpr int M = pipe_tile(S::T);
@@ -74,9 +75,11 @@ cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
         std::lock_guard<std::mutex> lock(mu);
         Cfg& c = cfg[dev & 63];
         if (c.blocks < 0) {
-            e = cudaFuncSetAttribute(k_fft_pipe<S, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            e = cudaFuncSetAttribute(k_fft_pipe<S, STAGES, REGFLOOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
             if (e != cudaSuccess) return e;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.blocks, k_fft_pipe<S, STAGES>, S::T * M, smem);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.blocks, k_fft_pipe<S, STAGES, REGFLOOR>, S::T * M,
+                                                              smem);
             if (e != cudaSuccess) return e;
             e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev);
             if (e != cudaSuccess) return e;
@@ -86,11 +89,12 @@ cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
     }
     const uint32_t tiles = (a.batch + (uint32_t)M - 1u) / (uint32_t)M;
     const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)std::max(1, resident * sms));
-    k_fft_pipe<S, STAGES><<<grid, S::T * M, smem, s>>>(a);
+    k_fft_pipe<S, STAGES, REGFLOOR><<<grid, S::T * M, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-template <class S>
+// REGFLOOR: see pipe_min_blocks (0 for the schedules tuned by hand).
+template <class S, int REGFLOOR = 0>
 StaticEntry static_entry()
 {
     StaticEntry e{};
@@ -103,8 +107,10 @@ StaticEntry static_entry()
     e.maxThreads = maxt;
     e.launch = &launch_static<S, maxt>;
     // the stage ring and exchange buffer must fit one CTA's shared memory
-    if constexpr (S::P >= 2 && (S::N % 2) == 0 && pipe_smem_bytes(S::N, 2, pipe_tile(S::T)) <= 227u * 1024u) {
-        e.launchPipelined = &launch_pipe<S, 2>;
+    // (odd lengths too: a tile's copy starts at the even element at or below
+    // its first value, see tile_span)
+    if constexpr (S::P >= 2 && pipe_smem_bytes(S::N, 2, pipe_tile(S::T)) <= 227u * 1024u) {
+        e.launchPipelined = &launch_pipe<S, 2, REGFLOOR>;
     } else {
         e.launchPipelined = nullptr;
     }

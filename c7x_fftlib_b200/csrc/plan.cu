@@ -75,9 +75,10 @@ bool evaluate(uint32_t n, const int* seq, int len, int emax, EnginePlan* e, bool
     // for lengths nothing narrower can plan
     score += emax == 32 ? 2.5 : emax == 16 ? 0.15 : 0.0;
     // a one-pass schedule cannot run in the bulk-copy pipelined kernel (its
-    // first pass is its last): at N = 8 and 16 it measured 2.7 TB/s, so the
-    // two-pass schedules with fixed-size pipelined kernels (4x2, 8x2) win
-    if (pipelined && len == 1 && (n == 8u || n == 16u)) score += 1.5;
+    // first pass is its last): at N = 8 and 16 it measured 2.7 TB/s, at 9,
+    // 10 and 12 2.1 TB/s, against 4.2-4.3 TB/s for the two-pass pipelined
+    // N = 18, 20, so from N = 8 up two-pass schedules win
+    if (pipelined && len == 1 && n >= 8u) score += 1.5;
     e->n = n;
     e->emax = emax;
     e->T = T;

@@ -272,7 +272,15 @@ def test_planner_covers_every_235_length_up_to_16384():
 
 
 def test_planner_headline_schedule():
-    assert F.describe_plan(4096) == "N=4096 E=16 T=256 radices=16x16x16"
+    assert F.describe_plan(4096) == "N=4096 E=16 T=256 radices=16x16x16 (fixed-size kernel)"
+
+
+def test_every_length_from_8_to_4096_has_a_fixed_size_kernel():
+    """Every 2^a 3^b 5^c length in [8, 4096] runs a kernel compiled for its
+    planned schedule (the runtime-radix engine serves the rest)."""
+    for n in _sizes_235(4096):
+        if n >= 8:
+            assert F.describe_plan(n).endswith("(fixed-size kernel)"), (n, F.describe_plan(n))
 
 
 def test_planner_rejects_other_primes():

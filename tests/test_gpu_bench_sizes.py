@@ -181,3 +181,53 @@ def test_tc_dft_bench_rows_every_transform(torch, n, rows):
     torch.cuda.synchronize()
     overall, worst = O.gpu_check_c2c(x, y, n, rows)
     assert overall <= REL_L2 and worst <= REL_L2, (overall, worst)
+
+
+def _lengths_235(nmax):
+    return sorted({2 ** a * 3 ** b * 5 ** c for a in range(13) for b in range(9) for c in range(7)
+                   if 2 ** a * 3 ** b * 5 ** c <= nmax})
+
+
+@pytest.mark.parametrize("kind", ["c2c", "ifft"])
+def test_every_length_up_to_4096_every_transform(torch, kind):
+    """Each 2^a 3^b 5^c length up to 4096 (its fixed-size kernel, pipelined
+    where the rows allow) on a batch of a few hundred thousand points with a
+    partial last tile, every transform against the GPU FP64 oracle."""
+    g = torch.Generator(device="cuda").manual_seed(77)
+    for n in _lengths_235(4096):
+        ch = 7 + (1 << 18) // n
+        x = torch.rand(2 * n * ch, device="cuda", generator=g) * 2 - 1
+        y = _c2c(torch, kind, x, n, ch)
+        overall, worst = O.gpu_check_c2c(x, y, n, ch, inverse=(kind == "ifft"))
+        assert overall <= REL_L2 and worst <= REL_L2, (n, overall, worst)
+
+
+def test_lengths_up_to_4096_output_off_16_byte_boundary(torch):
+    """pY 8 bytes past a 16-byte boundary (the last pass stores 8-byte
+    values), then pX too: results as for aligned buffers, odd lengths
+    included."""
+    g = torch.Generator(device="cuda").manual_seed(78)
+    base_name = F.KERNELS["c2c"]
+    for n in (12, 15, 60, 96, 243, 720, 1000, 2187, 3072, 3645, 4096):
+        ch = 5 + (1 << 16) // n
+        x = torch.rand(2 * n * ch, device="cuda", generator=g) * 2 - 1
+        src = x.clone()  # the kernel may use pX as its work buffer
+        w = torch.zeros(2 * n, device="cuda")
+        bX, bW = F.bp(F.FFTLIB_FLOAT32, 2 * n * ch), F.bp(F.FFTLIB_FLOAT32, 2 * n)
+        out = torch.zeros(2 * n * ch + 2, device="cuda")
+        yv = out[2:]
+        pb = F.pblock("c2c")
+        F.check(F.fn(base_name + "_init")(F.ptr(src), bX, F.ptr(w), bW, F.ptr(yv), bX, n, ch, pb))
+        F.check(F.fn(base_name + "_kernel")(F.ptr(src), bX, F.ptr(w), bW, F.ptr(yv), bX, n, ch, pb))
+        overall, worst = O.gpu_check_c2c(x, yv, n, ch)
+        assert overall <= REL_L2 and worst <= REL_L2, (n, overall, worst)
+        # pX off a 16-byte boundary: _init refuses it as the reference's
+        # optimized check does; _kernel (which, like the reference's, does not
+        # re-check) runs the kernels without bulk copies
+        xo = torch.zeros(2 * n * ch + 2, device="cuda")
+        xo[2:] = x
+        assert F.fn(base_name + "_init")(F.ptr(xo.data_ptr() + 8), bX, F.ptr(w), bW, F.ptr(yv), bX, n, ch,
+                                         F.pblock("c2c")) == 8
+        F.check(F.fn(base_name + "_kernel")(F.ptr(xo.data_ptr() + 8), bX, F.ptr(w), bW, F.ptr(yv), bX, n, ch, pb))
+        overall, worst = O.gpu_check_c2c(x, yv, n, ch)
+        assert overall <= REL_L2 and worst <= REL_L2, (n, "pX off 16 B", overall, worst)
