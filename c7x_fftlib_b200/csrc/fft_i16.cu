@@ -26,27 +26,6 @@ namespace fftb200 {
 
 __device__ __forceinline__ int16_t wrap16(int v) { return (int16_t)(uint16_t)(unsigned)v; }
 
-// Q15 product with the reference's rounding and saturation: x = a*b +/- c*d
-// formed exactly, then ((x + 0x4000) << 1) clamped to [-2^31, 0x7FFF0000]
-// and shifted right by 16, which equals clamp((x + 0x4000) >> 15) to
-// [-32768, 32767] ((2u) >> 16 == u >> 15 with floor semantics, and the clamp
-// bounds map onto each other). Products of int16 values lie in
-// [-(2^30 - 2^15), 2^30], and 2^30 only for (-32768)^2, so a difference
-// always fits in int32 and a sum does too except for 2^31 exactly (all four
-// factors -32768), which wraps to INT_MIN and saturates to 32767. Elsewhere
-// |x| <= 2^31 - 2^15, so x + 0x4000 cannot overflow.
-__device__ __forceinline__ int16_t q15_round(int x)
-{
-    const int u = (x + 0x4000) >> 15;
-    return (int16_t)max(-32768, min(32767, u));
-}
-__device__ __forceinline__ int16_t q15_dot_sub(int a, int b, int c, int d) { return q15_round(a * b - c * d); }
-__device__ __forceinline__ int16_t q15_dot_add(int a, int b, int c, int d)
-{
-    const int x = (int)((unsigned)(a * b) + (unsigned)(c * d));
-    return x == (int)0x80000000 ? (int16_t)32767 : q15_round(x);
-}
-
 // -im with the VCROT90H saturation of -(-32768) to 32767.
 __device__ __forceinline__ int16_t rot90_re(int16_t im)
 {
@@ -64,26 +43,59 @@ __device__ __forceinline__ int16_t shift_round(int16_t v, uint32_t shift)
     return wrap16(((vi & (int)mask) != 0) ? ((vi >> s) + 1) : (vi >> s));
 }
 
-// The same rounding shift with the per-stage constants precomputed: the
-// value is shifted by `s` and, when the reference's mask is non-zero (shift
-// in 1..16), bit `s - 1` is added back.
+// The same rounding shift with the per-stage constants precomputed. When
+// the reference's mask is non-zero (shift in 1..16) it adds bit s - 1 back
+// after the shift; (v >> s) + bit_{s-1}(v) = (v + 2^(s-1)) >> s for an int16 v
+// (floor division), so one add and one shift do it; otherwise it is v >> s.
+// apply = false: the stage is not followed by a shift (the 8-point stage).
+//
+// A Q15 product is rounded before that shift. With
+// f(v) = floor((v + add) / 2^s), non-decreasing, f(clamp(u)) =
+// clamp(f(u), f(-32768), f(32767)), and nested floor divisions compose:
+// f(floor((x + 2^14) / 2^15)) = floor((x + K) / 2^(15+s)), K = 2^14 + add 2^15.
+// K is even, so that is floor((floor(x / 2) + K / 2) / 2^(14+s)), which stays
+// in 32 bits (|x| <= 2^31 - 2^15 outside the one saturating sum); for
+// 14 + s >= 31 every such quotient is 0 or -1 and a shift by 31 gives it.
 struct ShiftRound {
-    int s, rb, rm;
-    __device__ __forceinline__ explicit ShiftRound(uint32_t shift)
+    int s, add;
+    int k2, sh, lo, hi;  // the product path: K / 2, 14 + s (at most 31), f(-32768), f(32767)
+    __device__ __forceinline__ explicit ShiftRound(uint32_t shift, bool apply = true)
     {
+        if (!apply) shift = 0;
         s = (int)(shift & 31u);
-        const bool rounds = (uint16_t)(1u << ((shift - 1u) & 31u)) != 0;
-        rb = rounds ? (int)((shift - 1u) & 31u) : 0;
-        rm = rounds ? 1 : 0;
+        const uint32_t rb = (shift - 1u) & 31u;
+        add = rb < 16u ? (int)(1u << rb) : 0;  // the mask narrowed to int16 is non-zero
+        k2 = 0x2000 + add * 16384;
+        sh = min(14 + s, 31);
+        lo = (-32768 + add) >> s;
+        hi = (32767 + add) >> s;
     }
-    // (v >> s) plus the rounding bit always fits in int16 (for s = 0 no bit
-    // is added), so no wrap is needed
-    __device__ __forceinline__ int16_t operator()(int16_t v) const
-    {
-        const int vi = v;
-        return (int16_t)((vi >> s) + ((vi >> rb) & rm));
-    }
+    // the result always fits in int16 (for s = 0 nothing is added), so no
+    // wrap is needed
+    __device__ __forceinline__ int16_t operator()(int16_t v) const { return (int16_t)(((int)v + add) >> s); }
+    // the Q15 rounding clamp((x + 0x4000) >> 15) followed by the shift
+    __device__ __forceinline__ int16_t q15(int x) const { return (int16_t)max(lo, min(hi, ((x >> 1) + k2) >> sh)); }
 };
+
+// Q15 product with the reference's rounding and saturation: x = a*b +/- c*d
+// formed exactly, then ((x + 0x4000) << 1) clamped to [-2^31, 0x7FFF0000]
+// and shifted right by 16, which equals clamp((x + 0x4000) >> 15) to
+// [-32768, 32767] ((2u) >> 16 == u >> 15 with floor semantics, and the clamp
+// bounds map onto each other). Products of int16 values lie in
+// [-(2^30 - 2^15), 2^30], and 2^30 only for (-32768)^2, so a difference
+// always fits in int32 and a sum does too except for 2^31 exactly (all four
+// factors -32768), which wraps to INT_MIN and saturates to 32767. Elsewhere
+// |x| <= 2^31 - 2^15, so x + 0x4000 cannot overflow.
+// The products are then rounded and shifted in one step (ShiftRound::q15).
+__device__ __forceinline__ int16_t q15s_dot_sub(int a, int b, int c, int d, const ShiftRound& sr)
+{
+    return sr.q15(a * b - c * d);
+}
+__device__ __forceinline__ int16_t q15s_dot_add(int a, int b, int c, int d, const ShiftRound& sr)
+{
+    const int x = (int)((unsigned)(a * b) + (unsigned)(c * d));
+    return x == (int)0x80000000 ? (int16_t)sr.hi : sr.q15(x);  // 2^31 saturates to 32767, then shifted
+}
 
 struct C16 {
     int16_t re, im;
@@ -93,15 +105,15 @@ __device__ __forceinline__ C16 ld(const short2* p) { short2 v = *p; return C16{v
 __device__ __forceinline__ void st(short2* p, C16 c) { *p = make_short2(c.re, c.im); }
 
 // One 4-point butterfly on p[0..3] (stride q apart in the stage), outputs
-// written back as bins 0,2,1,3 (the reference's slot order).
+// written back as bins 0,2,1,3 (the reference's slot order), each followed
+// by the stage's shift sr (the identity for the 8-point stage).
 // tw: the three Q15 twiddles (x1, x2, x3) unless notw.
 // Sums and differences are formed in int32 and wrapped to int16 only where
 // the reference's value is used non-linearly: the j-rotation's saturation
 // test and the four outputs (wrapping is linear modulo 2^16, so delaying it
 // gives the same bits).
 __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool notw,
-                                      const short2* tw, uint32_t k, uint32_t q, bool doShift,
-                                      const ShiftRound& sr)
+                                      const short2* tw, uint32_t k, uint32_t q, const ShiftRound& sr)
 {
     const int s1r = p0.re + p2.re, s1i = p0.im + p2.im;
     const int s2r = p1.re + p3.re, s2i = p1.im + p3.im;
@@ -113,17 +125,16 @@ __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool n
     C16 x1{wrap16(d1r - jr), wrap16(d1i - ji)};
     C16 x2{wrap16(s1r - s2r), wrap16(s1i - s2i)};
     C16 x3{wrap16(d1r + jr), wrap16(d1i + ji)};
+    // x0's Q15 product with 32767+1 (the reference's 0x7FFF0000 >> 16 scale
+    // of x0 by 2^15) rounds back to x0 exactly: only the shift applies
+    x0 = C16{sr(x0.re), sr(x0.im)};
     if (!notw) {
-        // x0's Q15 product with 32767+1 (the reference's 0x7FFF0000 >> 16
-        // scale of x0 by 2^15) rounds back to x0 exactly: no change
         const short2 w1 = tw[k], w2 = tw[q + k], w3 = tw[2 * q + k];
         const C16 a = x1, b = x2, c = x3;
-        x1 = C16{q15_dot_sub(a.re, w1.x, a.im, w1.y), q15_dot_add(a.re, w1.y, a.im, w1.x)};
-        x2 = C16{q15_dot_sub(b.re, w2.x, b.im, w2.y), q15_dot_add(b.re, w2.y, b.im, w2.x)};
-        x3 = C16{q15_dot_sub(c.re, w3.x, c.im, w3.y), q15_dot_add(c.re, w3.y, c.im, w3.x)};
-    }
-    if (doShift) {
-        x0 = C16{sr(x0.re), sr(x0.im)};
+        x1 = C16{q15s_dot_sub(a.re, w1.x, a.im, w1.y, sr), q15s_dot_add(a.re, w1.y, a.im, w1.x, sr)};
+        x2 = C16{q15s_dot_sub(b.re, w2.x, b.im, w2.y, sr), q15s_dot_add(b.re, w2.y, b.im, w2.x, sr)};
+        x3 = C16{q15s_dot_sub(c.re, w3.x, c.im, w3.y, sr), q15s_dot_add(c.re, w3.y, c.im, w3.x, sr)};
+    } else {
         x1 = C16{sr(x1.re), sr(x1.im)};
         x2 = C16{sr(x2.re), sr(x2.im)};
         x3 = C16{sr(x3.re), sr(x3.im)};
@@ -135,12 +146,13 @@ __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool n
     p3 = x3;
 }
 
-// Stage with block size m (q = m/4) on the 4 points {k + b*m + i*q}.
+// Stage with block size m (q = m/4) on the 4 points {k + b*m + i*q}; sr
+// is the identity for m = 8.
 __device__ __forceinline__ void stage_bfly(C16* pt, uint32_t m, uint32_t k, const short2* tw, const ShiftRound& sr)
 {
     const uint32_t q = m / 4u;
     const bool notw = (m == 4u) || (m == 8u && k == 0u);
-    bfly4(pt[0], pt[1], pt[2], pt[3], notw, tw, k, q, m != 8u, sr);
+    bfly4(pt[0], pt[1], pt[2], pt[3], notw, tw, k, q, sr);
 }
 
 // Shared-memory index with one pad word per 16: the 16-point gathers of the
@@ -151,7 +163,7 @@ __device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
 // time (its own padded shared-memory region) and the CTA walks the batch G
 // transforms at a step. The caller's twiddle table and the shift vector are
 // copied into shared memory once per CTA.
-__global__ void __launch_bounds__(256) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
+__global__ void __launch_bounds__(256, 3) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
                                                  const short2* __restrict__ w,
                                                  const uint32_t* __restrict__ shifts, uint32_t nsh, uint32_t n,
                                                  uint32_t logn, uint32_t batch, uint32_t tg, bool vec)
@@ -195,7 +207,7 @@ __global__ void __launch_bounds__(256) k_fft_i16(const short2* __restrict__ x, s
             const uint32_t shiftA = s_shift[stage];
             const uint32_t m2 = m / 4u;
             const uint32_t shiftB = s_shift[stage + 1];
-            const ShiftRound srA(shiftA), srB(shiftB);
+            const ShiftRound srA(shiftA, m != 8u), srB(shiftB, m2 != 8u);
             const short2* tw2 = tw + 3u * (m / 4u);
             const uint32_t s16 = m / 16u;
             const uint32_t groups = n / 16u; // (block, k0) pairs
@@ -240,7 +252,7 @@ __global__ void __launch_bounds__(256) k_fft_i16(const short2* __restrict__ x, s
                     const uint32_t base = blk * m + k;
                     C16 q4[4] = {ld(sx + pad16(base)), ld(sx + pad16(base + q)), ld(sx + pad16(base + 2 * q)),
                                  ld(sx + pad16(base + 3 * q))};
-                    stage_bfly(q4, m, k, tw, ShiftRound(shift));
+                    stage_bfly(q4, m, k, tw, ShiftRound(shift, m != 8u));
                     st(sx + pad16(base), q4[0]);
                     st(sx + pad16(base + q), q4[1]);
                     st(sx + pad16(base + 2 * q), q4[2]);
