@@ -113,7 +113,7 @@ __device__ __forceinline__ void st(short2* p, C16 c) { *p = make_short2(c.re, c.
 // test and the four outputs (wrapping is linear modulo 2^16, so delaying it
 // gives the same bits).
 __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool notw,
-                                      const short2* tw, uint32_t k, uint32_t q, const ShiftRound& sr)
+                                      const int2* tw, uint32_t k, uint32_t q, const ShiftRound& sr)
 {
     const int s1r = p0.re + p2.re, s1i = p0.im + p2.im;
     const int s2r = p1.re + p3.re, s2i = p1.im + p3.im;
@@ -129,7 +129,7 @@ __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool n
     // of x0 by 2^15) rounds back to x0 exactly: only the shift applies
     x0 = C16{sr(x0.re), sr(x0.im)};
     if (!notw) {
-        const short2 w1 = tw[k], w2 = tw[q + k], w3 = tw[2 * q + k];
+        const int2 w1 = tw[k], w2 = tw[q + k], w3 = tw[2 * q + k];
         const C16 a = x1, b = x2, c = x3;
         x1 = C16{q15s_dot_sub(a.re, w1.x, a.im, w1.y, sr), q15s_dot_add(a.re, w1.y, a.im, w1.x, sr)};
         x2 = C16{q15s_dot_sub(b.re, w2.x, b.im, w2.y, sr), q15s_dot_add(b.re, w2.y, b.im, w2.x, sr)};
@@ -148,7 +148,7 @@ __device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool n
 
 // Stage with block size m (q = m/4) on the 4 points {k + b*m + i*q}; sr
 // is the identity for m = 8.
-__device__ __forceinline__ void stage_bfly(C16* pt, uint32_t m, uint32_t k, const short2* tw, const ShiftRound& sr)
+__device__ __forceinline__ void stage_bfly(C16* pt, uint32_t m, uint32_t k, const int2* tw, const ShiftRound& sr)
 {
     const uint32_t q = m / 4u;
     const bool notw = (m == 4u) || (m == 8u && k == 0u);
@@ -168,14 +168,20 @@ __global__ void __launch_bounds__(256, 3) k_fft_i16(const short2* __restrict__ x
                                                  const uint32_t* __restrict__ shifts, uint32_t nsh, uint32_t n,
                                                  uint32_t logn, uint32_t batch, uint32_t tg, bool vec)
 {
-    extern __shared__ short2 smem[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t s_shift[8];
     const uint32_t padn = n + (n >> 4);
     const uint32_t G = blockDim.x / tg;
     const uint32_t g = threadIdx.x / tg, t = threadIdx.x - g * tg;
-    short2* stw = smem;
-    short2* sx = smem + n + g * padn;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) stw[i] = w[i];
+    // the caller's Q15 table as 32-bit pairs (one load per twiddle, no
+    // extraction), then the transforms' padded regions
+    int2* stw = reinterpret_cast<int2*>(smem_raw);
+    short2* smem = reinterpret_cast<short2*>(stw + n);
+    short2* sx = smem + g * padn;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const short2 v = w[i];
+        stw[i] = make_int2(v.x, v.y);
+    }
     if (threadIdx.x < nsh && threadIdx.x < 8u) s_shift[threadIdx.x] = shifts[threadIdx.x];
     __syncthreads();
 
@@ -201,14 +207,14 @@ __global__ void __launch_bounds__(256, 3) k_fft_i16(const short2* __restrict__ x
         __syncthreads();
 
         uint32_t m = n, stage = 0, shift = 0;
-        const short2* tw = stw;
+        const int2* tw = stw;
         // pairs of radix-4 stages fused in registers: 16 points per thread
         while (m >= 16u) {
             const uint32_t shiftA = s_shift[stage];
             const uint32_t m2 = m / 4u;
             const uint32_t shiftB = s_shift[stage + 1];
             const ShiftRound srA(shiftA, m != 8u), srB(shiftB, m2 != 8u);
-            const short2* tw2 = tw + 3u * (m / 4u);
+            const int2* tw2 = tw + 3u * (m / 4u);
             const uint32_t s16 = m / 16u;
             const uint32_t groups = n / 16u; // (block, k0) pairs
             if (active) {
@@ -303,7 +309,7 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
     const uint32_t tg = n >= 4096u ? 256u : (n / 16u >= 1u ? n / 16u : 1u);
     const uint32_t G = 256u / tg;
     const uint32_t threads = tg * G;
-    const size_t smem = ((size_t)n + (size_t)G * (n + (n >> 4))) * sizeof(short2);
+    const size_t smem = (size_t)n * sizeof(int2) + (size_t)G * (n + (n >> 4)) * sizeof(short2);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
