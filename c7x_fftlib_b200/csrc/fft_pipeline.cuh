@@ -235,8 +235,11 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
                 for (uint32_t i = t; i <= N / 2u; i += (uint32_t)S::T) {
                     const uint32_t ip = N - i;
                     const float2 xi = row[i], xp = row[ip];
-                    row[i] = c2r_z(xi, xp, __ldg(&a.twSplit[i]));
-                    if (i != 0u && ip != i) row[ip] = c2r_z(xp, xi, __ldg(&a.twSplit[ip]));
+                    // W_{2h}^(h-i) = -conj(W_{2h}^i): one table load serves the
+                    // pair, with the accuracy of the table's own entry
+                    const float2 w = __ldg(&a.twSplit[i]);
+                    row[i] = c2r_z(xi, xp, w);
+                    if (i != 0u && ip != i) row[ip] = c2r_z(xp, xi, make_float2(-w.x, w.y));
                 }
             }
             __syncthreads();

@@ -218,11 +218,14 @@ FFT_DEV void r2c_epilogue(const FftArgs& a, const float2* sm, uint32_t t, float2
         }
         const uint32_t ip = h - i;
         const float2 zi = sm[smem_swz(i)], zp = sm[smem_swz(ip)];
-        const float2 yi = r2c_split(zi, zp, __ldg(&a.twSplit[i]));
+        // W_{2h}^(h-i) = -conj(W_{2h}^i): one table load serves the pair,
+        // with the accuracy of the table's own entry (FP64 rounded to FP32)
+        const float2 w = __ldg(&a.twSplit[i]);
+        const float2 yi = r2c_split(zi, zp, w);
         row[i] = yi;
         if (a.realMode) row[2 * h - i] = cconj(yi);
         if (ip != i) {
-            const float2 yp = r2c_split(zp, zi, __ldg(&a.twSplit[ip]));
+            const float2 yp = r2c_split(zp, zi, make_float2(-w.x, w.y));
             row[ip] = yp;
             if (a.realMode) row[2 * h - ip] = cconj(yp);
         }
