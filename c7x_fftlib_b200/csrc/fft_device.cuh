@@ -16,6 +16,11 @@
 #include "fft_args.h"
 
 #define FFT_DEV __device__ __forceinline__
+// For the lambdas of static_for in the hot paths: a lambda's call operator
+// is only implicitly inline, and when many instantiations of one pass share
+// it the compiler may emit it as a function of its own (a call with a stack
+// frame per butterfly); this keeps every body inlined.
+#define FFT_INL __attribute__((always_inline))
 
 namespace fftb200 {
 
@@ -210,17 +215,17 @@ FFT_DEV void dft(float2* v)
     constexpr int Q = R / P;
     static_assert(P * Q == R && Q > 1, "dft<R>: R must be 2^a 3^b 5^c");
     float2 t[R];
-    static_for<Q>([&](auto n2) {
+    static_for<Q>([&](auto n2) FFT_INL {
         float2 a[P];
-        static_for<P>([&](auto n1) { a[n1] = v[Q * n1 + n2]; });
+        static_for<P>([&](auto n1) FFT_INL { a[n1] = v[Q * n1 + n2]; });
         dft<P>(a);
-        static_for<P>([&](auto k1) { t[k1 * Q + n2] = cmul_w<R, decltype(n2)::value * decltype(k1)::value>(a[k1]); });
+        static_for<P>([&](auto k1) FFT_INL { t[k1 * Q + n2] = cmul_w<R, decltype(n2)::value * decltype(k1)::value>(a[k1]); });
     });
-    static_for<P>([&](auto k1) {
+    static_for<P>([&](auto k1) FFT_INL {
         float2 b[Q];
-        static_for<Q>([&](auto n2) { b[n2] = t[k1 * Q + n2]; });
+        static_for<Q>([&](auto n2) FFT_INL { b[n2] = t[k1 * Q + n2]; });
         dft<Q>(b);
-        static_for<Q>([&](auto k2) { v[k1 + P * k2] = b[k2]; });
+        static_for<Q>([&](auto k2) FFT_INL { v[k1 + P * k2] = b[k2]; });
     });
 }
 

@@ -244,7 +244,7 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
             }
             __syncthreads();
         }
-        static_for<S::P>([&](auto p) {
+        static_for<S::P>([&](auto p) FFT_INL {
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
             if constexpr (P == 0) {

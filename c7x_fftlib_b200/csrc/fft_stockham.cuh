@@ -34,7 +34,7 @@ __host__ __device__ constexpr int engine_min_radix(int emax) { return emax >= 32
 template <int EMAX, class F>
 FFT_DEV void dispatch_radix(int r, F&& f)
 {
-    static_for<EMAX + 1>([&](auto d) {
+    static_for<EMAX + 1>([&](auto d) FFT_INL {
         constexpr int D = decltype(d)::value;
         constexpr bool ok235 = [] {
             int x = D;
@@ -117,11 +117,11 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
     const uint32_t nb = pi.stride; // butterflies in this pass: N / R
 
     // gather
-    static_for<BMAX>([&](auto i) {
+    static_for<BMAX>([&](auto i) FFT_INL {
         const uint32_t j = t + (uint32_t)i * T;
         if (j < nb) {
             const uint32_t sj = smem_swz(j);
-            static_for<R>([&](auto q) {
+            static_for<R>([&](auto q) FFT_INL {
                 const uint32_t idx = j + (uint32_t)q * nb;
                 float2 z;
                 if (first && (RAW_FIRST || raw)) {
@@ -138,7 +138,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
     });
 
     // twiddle and butterfly
-    static_for<BMAX>([&](auto i) {
+    static_for<BMAX>([&](auto i) FFT_INL {
         const uint32_t j = t + (uint32_t)i * T;
         if (j < nb) {
             if (!first) {
@@ -146,7 +146,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
                 const uint32_t k = j - g * pi.Ns;
                 // lanes of a warp read consecutive k: coalesced twiddle loads
                 const float2* tw = a.tw + pi.twOffset + k;
-                static_for<R - 1>([&](auto q1) {
+                static_for<R - 1>([&](auto q1) FFT_INL {
                     constexpr int q = decltype(q1)::value + 1;
                     v[i * R + q] = cmul(v[i * R + q], __ldg(&tw[(q - 1) * pi.Ns]));
                 });
@@ -160,10 +160,10 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
     if (direct) {
         if (active) {
             float2* row = rowOut;
-            static_for<BMAX>([&](auto i) {
+            static_for<BMAX>([&](auto i) FFT_INL {
                 const uint32_t j = t + (uint32_t)i * T;
                 if (j < nb) {
-                    static_for<R>([&](auto q) {
+                    static_for<R>([&](auto q) FFT_INL {
                         const uint32_t idx = j + (uint32_t)q * nb;
                         row[(int64_t)idx * a.outElem] = finish(a, v[i * R + q]);
                     });
@@ -176,7 +176,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
         __syncthreads(); // every read of this pass is done
         afterGather();
     }
-    static_for<BMAX>([&](auto i) {
+    static_for<BMAX>([&](auto i) FFT_INL {
         const uint32_t j = t + (uint32_t)i * T;
         if (j < nb) {
             const uint32_t g = fastdiv(j, pi.Ns, pi.nsMagic);
@@ -185,7 +185,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
             const uint32_t sb = smem_swz(base);
             // Ns = 1 with R = 16: base is a multiple of 16 and q < 16 share its pad
             const bool contiguous16 = pi.Ns == 1u && R == 16;
-            static_for<R>([&](auto q) {
+            static_for<R>([&](auto q) FFT_INL {
                 const uint32_t d = contiguous16 ? sb + (uint32_t)q : swz_step(sb, base, (uint32_t)q, pi.Ns);
                 sm[d] = v[i * R + q];
             });
@@ -273,7 +273,7 @@ FFT_DEV void stage_in(const FftArgs& a, float2* smem, uint32_t b0)
         const uint32_t step = blockDim.x;
         for (uint32_t e0 = threadIdx.x; e0 < total; e0 += U * step) {
             float2 z[U], wl[U], wh[U];
-            static_for<U>([&](auto u) {
+            static_for<U>([&](auto u) FFT_INL {
                 const uint32_t e = e0 + (uint32_t)u * step;
                 if (e < total) {
                     const uint32_t i = fastdiv(e, a.M, a.mMagic);
@@ -286,7 +286,7 @@ FFT_DEV void stage_in(const FftArgs& a, float2* smem, uint32_t b0)
                     }
                 }
             });
-            static_for<U>([&](auto u) {
+            static_for<U>([&](auto u) FFT_INL {
                 const uint32_t e = e0 + (uint32_t)u * step;
                 if (e < total) {
                     const uint32_t i = fastdiv(e, a.M, a.mMagic);
@@ -422,7 +422,7 @@ FFT_DEV void fft_tile_static(const FftArgs& a, float2* smem, uint32_t b0)
         const float2* rowIn = a.in + row_in(a, b);
         float2* rowOut = a.out + row_out(a, b);
         float2 v[S::EMAX];
-        static_for<S::P>([&](auto p) {
+        static_for<S::P>([&](auto p) FFT_INL {
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
             run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, active, rowIn,
