@@ -247,12 +247,14 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
         static_for<S::P>([&](auto p) FFT_INL {
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
+            constexpr int L0 = first_boundary_layout(S::R[0]);
             if constexpr (P == 0) {
-                run_pass<S::EMAX, S::R[P]>(a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t,
-                                           active, nullptr, rowOut, st + shift + m * (uint32_t)IC, refill);
+                run_pass<S::EMAX, S::R[P], decltype(refill), false, kPad16, L0>(
+                    a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut,
+                    st + shift + m * (uint32_t)IC, refill);
             } else {
-                run_pass<S::EMAX, S::R[P]>(a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t,
-                                           active, nullptr, rowOut);
+                run_pass<S::EMAX, S::R[P], NoHook, false, P == 1 ? L0 : kPad16, kPad16>(
+                    a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut);
             }
         });
         // r2c: the last pass left Z in natural order in the padded layout;

@@ -102,12 +102,38 @@ FFT_DEV uint32_t swz_step(uint32_t swzBase, uint32_t idx0, uint32_t q, uint32_t 
     return (step & 15u) == 0u ? swzBase + q * (step + (step >> 4)) : smem_swz(idx0 + q * step);
 }
 
+// Exchange layouts between two passes: kPad16, one pad slot per 16 values
+// (smem_swz; conflict-free for the power-of-two strides of radix-2^k
+// scatters), or kNoPad, the plain index: a first pass of odd radix R
+// scatters with stride R (Ns = 1), which is conflict-free unpadded but
+// collides in banks with the pad, and the next pass gathers consecutive
+// values either way.
+constexpr int kPad16 = 0, kNoPad = 1;
+
+template <int L>
+FFT_DEV uint32_t lay(uint32_t idx)
+{
+    return L == kNoPad ? idx : smem_swz(idx);
+}
+// lay<L>(idx0 + q * step) from base = lay<L>(idx0)
+template <int L>
+FFT_DEV uint32_t lay_step(uint32_t base, uint32_t idx0, uint32_t q, uint32_t step)
+{
+    return L == kNoPad ? base + q * step : swz_step(base, idx0, q, step);
+}
+
+// The layout of the boundary after pass 0 of a compile-time schedule whose
+// first radix is R0 (the boundaries after later passes keep kPad16).
+__host__ __device__ constexpr int first_boundary_layout(int r0) { return (r0 % 2) ? kNoPad : kPad16; }
+
 // raw: when not null, the first pass reads its input from this unpadded
 // shared-memory copy of the transform (filled by a bulk async copy);
 // RAW_FIRST: raw is never null (only that path is compiled).
+// LIN / LOUT: the exchange layout this pass gathers from (when it is not the
+// first) and scatters to.
 // afterGather runs right after the barrier that ends the pass's reads.
 // rowIn / rowOut: this lane's transform in HBM (first / last pass).
-template <int EMAX, int R, class Hook = NoHook, bool RAW_FIRST = false>
+template <int EMAX, int R, class Hook = NoHook, bool RAW_FIRST = false, int LIN = kPad16, int LOUT = kPad16>
 FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, const bool last,
                       const uint32_t T, float2 (&v)[EMAX], float2* sm, uint32_t t, bool active,
                       const float2* rowIn, float2* rowOut, const float2* raw = nullptr,
@@ -120,7 +146,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
     static_for<BMAX>([&](auto i) FFT_INL {
         const uint32_t j = t + (uint32_t)i * T;
         if (j < nb) {
-            const uint32_t sj = smem_swz(j);
+            const uint32_t sj = lay<LIN>(j);
             static_for<R>([&](auto q) FFT_INL {
                 const uint32_t idx = j + (uint32_t)q * nb;
                 float2 z;
@@ -130,7 +156,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
                 } else if (first && !RAW_FIRST) {
                     z = (active || a.staged) ? load_in(a, rowIn, idx, sm) : make_float2(0.f, 0.f);
                 } else {
-                    z = sm[swz_step(sj, j, (uint32_t)q, nb)];
+                    z = sm[lay_step<LIN>(sj, j, (uint32_t)q, nb)];
                 }
                 v[i * R + q] = z;
             });
@@ -182,11 +208,11 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
             const uint32_t g = fastdiv(j, pi.Ns, pi.nsMagic);
             const uint32_t k = j - g * pi.Ns;
             const uint32_t base = g * pi.Ns * (uint32_t)R + k;
-            const uint32_t sb = smem_swz(base);
+            const uint32_t sb = lay<LOUT>(base);
             // Ns = 1 with R = 16: base is a multiple of 16 and q < 16 share its pad
-            const bool contiguous16 = pi.Ns == 1u && R == 16;
+            const bool contiguous16 = LOUT == kPad16 && pi.Ns == 1u && R == 16;
             static_for<R>([&](auto q) FFT_INL {
-                const uint32_t d = contiguous16 ? sb + (uint32_t)q : swz_step(sb, base, (uint32_t)q, pi.Ns);
+                const uint32_t d = contiguous16 ? sb + (uint32_t)q : lay_step<LOUT>(sb, base, (uint32_t)q, pi.Ns);
                 sm[d] = v[i * R + q];
             });
         }
@@ -425,8 +451,11 @@ FFT_DEV void fft_tile_static(const FftArgs& a, float2* smem, uint32_t b0)
         static_for<S::P>([&](auto p) FFT_INL {
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
-            run_pass<S::EMAX, S::R[P]>(a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, active, rowIn,
-                                       rowOut);
+            // (a one-pass schedule's only boundary is read by the r2c
+            // epilogue or the staged store, in the padded layout)
+            constexpr int L0 = S::P > 1 ? first_boundary_layout(S::R[0]) : kPad16;
+            run_pass<S::EMAX, S::R[P], NoHook, false, P == 1 ? L0 : kPad16, P == 0 ? L0 : kPad16>(
+                a, pi, P == 0, P + 1 == S::P, (uint32_t)S::T, v, sm, t, active, rowIn, rowOut);
         });
         if (a.ioMode == IO_R2C_SPLIT) r2c_epilogue(a, sm, t, rowOut, active);
     }
