@@ -134,10 +134,26 @@ __global__ void __launch_bounds__(kMixedBlock, MINB)
         float2* sm = st + m * a.slen;
         const float2* raw = st + (size_t)m * N;  // this transform's inputs in the stage
         const int P = (int)a.P;
+        // an odd first radix scatters with an odd stride: the boundary after
+        // pass 0 is unpadded (kNoPad, see run_pass)
+        const bool noPad0 = P > 1 && (a.pass[0].R & 1);
         for (int p = 0; p < P; ++p) {
             dispatch_radix<EMAX>(a.pass[p].R, [&](auto r) {
-                run_pass<EMAX, decltype(r)::value, NoHook, true>(a, a.pass[p], p == 0, p + 1 == P, T, v, sm, t,
-                                                                 active, rowIn, rowOut, raw);
+                constexpr int RR = decltype(r)::value;
+                if constexpr (RR % 2 == 1) {
+                    if (p == 0 && noPad0) {
+                        run_pass<EMAX, RR, NoHook, true, kPad16, kNoPad>(a, a.pass[p], true, false, T, v, sm, t,
+                                                                         active, rowIn, rowOut, raw);
+                        return;
+                    }
+                }
+                if (p == 1 && noPad0) {
+                    run_pass<EMAX, RR, NoHook, true, kNoPad, kPad16>(a, a.pass[p], false, p + 1 == P, T, v, sm, t,
+                                                                     active, rowIn, rowOut, raw);
+                    return;
+                }
+                run_pass<EMAX, RR, NoHook, true>(a, a.pass[p], p == 0, p + 1 == P, T, v, sm, t, active, rowIn,
+                                                 rowOut, raw);
             });
         }
     }
