@@ -450,6 +450,10 @@ def secondary_configs(args):
     ym = torch.empty_like(xm)
     mb = F.MixedBatch(lengths)
     ms_graph = _time_launches(torch, stream, lambda: mb.exec(xm, ym, sp), steps)
+    # every group in the single persistent kernel (runtime-radix passes)
+    mbp = F.MixedBatch(lengths, persistent_only=True)
+    ms_persistent = _time_launches(torch, stream, lambda: mbp.exec(xm, ym, sp), steps)
+    mbp.close()
     ms_per = _time_launches(torch, stream, lambda: mb.exec_per_size(xm, ym, sp), steps)
     # the regular batched API, one call per length (fixed-size kernels where compiled)
     uniq, counts = np.unique(lengths, return_counts=True)
@@ -490,8 +494,12 @@ def secondary_configs(args):
     parity_check("mixed_20000 sampled rel-L2", mixed_rel <= REL_L2_BOUND, mixed_rel)
     mbytes = 16.0 * total
     res["mixed_20000"] = {"lengths": len(uniq), "total_points": total,
+                          "launch": "one graph: each length group's persistent fixed-size kernel on a grid "
+                                    "share, parallel branches",
                           "persistent_graph_ms": round(ms_graph, 4),
                           "persistent_graph_GBps": round(mbytes / ms_graph / 1e6, 1),
+                          "single_persistent_kernel_ms": round(ms_persistent, 4),
+                          "single_persistent_kernel_GBps": round(mbytes / ms_persistent / 1e6, 1),
                           "per_length_same_kernel_ms": round(ms_per, 4),
                           "per_length_batched_api_ms": round(ms_api, 4),
                           "speedup_vs_per_length_api": round(ms_api / ms_graph, 3),

@@ -294,17 +294,19 @@ def describe_plan(n: int) -> str:
 
 MIXED_INVERSE = 1
 MIXED_AUTOTUNE = 2
+MIXED_PERSISTENT_ONLY = 4
 
 
 class MixedBatch:
     """FFTLIB_b200_fftMixed_*: uneven-length c2c batch (device buffers)."""
 
-    def __init__(self, lengths, inverse=False, autotune=False):
+    def __init__(self, lengths, inverse=False, autotune=False, persistent_only=False):
         import numpy as _np
 
         self.lengths = _np.ascontiguousarray(lengths, _np.uint32)
         self.h = C.c_void_p()
-        flags = (MIXED_INVERSE if inverse else 0) | (MIXED_AUTOTUNE if autotune else 0)
+        flags = (MIXED_INVERSE if inverse else 0) | (MIXED_AUTOTUNE if autotune else 0) | \
+            (MIXED_PERSISTENT_ONLY if persistent_only else 0)
         arr = self.lengths.ctypes.data_as(C.POINTER(C.c_uint32))
         check(lib().FFTLIB_b200_fftMixed_create(arr, len(self.lengths), flags, C.byref(self.h)), "fftMixed_create")
 

@@ -1,22 +1,29 @@
 // capi_mixed.cu -- uneven-length FP32 c2c batches in one persistent launch
 // (include/fftlib_b200/fftlib_b200_ext.h, FFTLIB_b200_fftMixed_*).
 //
-// create() groups the transforms by length, chooses a schedule per group
-// (heuristic, or timed by the autotuner), builds the device tables (group
-// schedules, tiles ordered by cost, per-transform offsets) and the group
-// twiddle tables. exec() replays a CUDA graph holding the counter reset and
-// persistent launches (one per kernel class present, on parallel branches);
-// execPerSize() launches the same kernels once per distinct length, for
-// comparison.
+// create() groups the transforms by length. A group whose transforms lie
+// back to back and whose length has a persistent pipelined fixed-size kernel
+// (every 2^a 3^b 5^c length from 8 to 4096) is a "fixed group": it runs that
+// kernel with a grid proportional to its share of the batch, so that all
+// groups run side by side on one partition of the GPU each and finish
+// together. Every other group gets a runtime-radix schedule (heuristic, or
+// timed by the autotuner) in the persistent mixed kernel (fft_mixed.cu),
+// which walks a device-resident tile table ordered by cost. exec() replays a
+// CUDA graph with all of these launches on parallel branches;
+// FFTLIB_B200_MIXED_PERSISTENT_ONLY puts every group in the persistent
+// kernel. execPerSize() launches the persistent kernel once per distinct
+// length, for comparison.
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <sstream>
 #include <string>
 #include <vector>
 
 #include "capi_common.h"
+#include "fft_engine.h"
 #include "fft_mixed.h"
 #include "fftlib_b200_ext.h"
 #include "plan.h"
@@ -31,6 +38,7 @@ struct FFTLIB_b200_mixed {
     std::vector<int> groupCls;
     std::vector<EnginePlan> groupPlan;
     std::vector<uint32_t> groupM;
+    std::vector<uint32_t> groupCount;
     std::vector<uint32_t> groupTileBegin, groupTileEnd; // ranges in dTilesByGroup
     std::vector<float2*> groupTw;
     MixedGroup* dGroups = nullptr;
@@ -43,8 +51,22 @@ struct FFTLIB_b200_mixed {
     uint32_t clsStage[kMixedClasses] = {};
     uint32_t groupStage = 0;            // largest stage of any group (per-size launches)
     uint32_t clsGrid[kMixedClasses] = {};
-    cudaStream_t capture = nullptr, side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    // fixed groups: the regular plan's fixed-size kernel on a grid share
+    struct Fixed {
+        uint32_t n, count;
+        uint64_t offset;       // complex elements
+        ComplexPlan* plan;
+        uint32_t grid;
+        uint32_t branch;
+    };
+    std::vector<Fixed> fixed;           // ordered by branch
+    uint64_t fixedPoints = 0;
+    uint32_t fixedBranches = 0;
+    // one graph branch per fixed group and per class with tiles
+    std::vector<cudaStream_t> branches;
+    std::vector<cudaEvent_t> joins;
+    cudaStream_t capture = nullptr;
+    cudaEvent_t fork = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     const void* gx = nullptr;
@@ -199,9 +221,9 @@ void release(FFTLIB_b200_mixed* h)
     if (h->exec) cudaGraphExecDestroy(h->exec);
     if (h->graph) cudaGraphDestroy(h->graph);
     if (h->capture) cudaStreamDestroy(h->capture);
-    if (h->side) cudaStreamDestroy(h->side);
+    for (cudaStream_t b : h->branches) cudaStreamDestroy(b);
+    for (cudaEvent_t e : h->joins) cudaEventDestroy(e);
     if (h->fork) cudaEventDestroy(h->fork);
-    if (h->join) cudaEventDestroy(h->join);
     for (float2* t : h->groupTw) cudaFree(t);
     cudaFree(h->dGroups);
     cudaFree(h->dTiles);
@@ -210,26 +232,31 @@ void release(FFTLIB_b200_mixed* h)
     delete h;
 }
 
-// The persistent launches of every class that has tiles: the W20 class (few
-// lengths) on a side branch, the W16 class on the main one, joined again.
-cudaError_t enqueue_classes(FFTLIB_b200_mixed* h, const float* x, float* y, cudaStream_t s)
+// Every launch of the batch on its own branch: the fixed groups' kernels
+// and the persistent kernel of every class that has tiles, forked from and
+// joined back into s.
+cudaError_t enqueue_all(FFTLIB_b200_mixed* h, const float* x, float* y, cudaStream_t s)
 {
-    const bool both = h->clsTiles[kMixedW16] && h->clsTiles[kMixedW20];
-    cudaError_t err = cudaSuccess;
-    if (both) {
-        err = cudaEventRecord(h->fork, s);
-        if (err == cudaSuccess) err = cudaStreamWaitEvent(h->side, h->fork, 0);
+    const bool inverse = h->flags & FFTLIB_B200_MIXED_INVERSE;
+    cudaError_t err = cudaEventRecord(h->fork, s);
+    for (cudaStream_t b : h->branches)
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(b, h->fork, 0);
+    for (const auto& f : h->fixed) {
+        if (err != cudaSuccess) break;
+        float2* in = const_cast<float2*>(reinterpret_cast<const float2*>(x)) + f.offset;
+        err = run_c2c(f.plan, in, reinterpret_cast<float2*>(y) + f.offset, f.count, inverse, h->branches[f.branch],
+                      f.grid);
     }
+    size_t br = h->fixedBranches;
     for (int cls = kMixedClasses - 1; cls >= 0 && err == cudaSuccess; --cls) {
         if (!h->clsTiles[cls]) continue;
-        const cudaStream_t cs = (both && cls == kMixedW20) ? h->side : s;
         err = launch_mixed(class_launch(cls, h->dGroups, h->dTiles + h->clsTileBegin[cls], h->clsTiles[cls],
                                         h->dOffsets, x, y, h->clsStage[cls], h->clsGrid[cls]),
-                           cs);
+                           h->branches[br++]);
     }
-    if (both && err == cudaSuccess) {
-        err = cudaEventRecord(h->join, h->side);
-        if (err == cudaSuccess) err = cudaStreamWaitEvent(s, h->join, 0);
+    for (size_t b = 0; b < h->branches.size() && err == cudaSuccess; ++b) {
+        err = cudaEventRecord(h->joins[b], h->branches[b]);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(s, h->joins[b], 0);
     }
     return err;
 }
@@ -267,9 +294,28 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
     std::vector<MixedGroup> groups;
     std::vector<MixedTile> tiles;
     std::vector<uint64_t> offsByGroup;
+    std::vector<char> groupFixed;
     cudaStream_t s = cudaStreamPerThread;
     for (auto& kv : byN) {
         const uint32_t n = kv.first;
+        // a fixed group: its transforms back to back, its length with a
+        // persistent pipelined fixed-size kernel
+        // (moving the small groups into the persistent kernel measured slower:
+        // on a reduced share it becomes the batch's tail)
+        bool isFixed = !(flags & FFTLIB_B200_MIXED_PERSISTENT_ONLY);
+        for (size_t k = 0; isFixed && k < kv.second.size(); ++k)
+            isFixed = offset[kv.second[k]] == offset[kv.second[0]] + (uint64_t)k * n;
+        if (isFixed) {
+            cudaError_t perr = cudaSuccess;
+            ComplexPlan* cp = get_complex_plan(n, false, &perr);
+            isFixed = cp && !cp->multiPass &&
+                      static_pipelined_resident(n, cp->eng.emax, cp->eng.T, cp->eng.P, cp->eng.R) > 0;
+            if (isFixed)
+                h->fixed.push_back(
+                    FFTLIB_b200_mixed::Fixed{n, (uint32_t)kv.second.size(), offset[kv.second[0]], cp, 0, 0});
+            if (perr != cudaSuccess) cudaGetLastError();
+        }
+        groupFixed.push_back(isFixed ? 1 : 0);
         EnginePlan e;
         if (!mixed_schedule(n, (uint32_t)kv.second.size(), tune, &e)) {
             set_error("length %u is not 2^a 3^b 5^c up to %u threads per transform", n, kMixedMaxT);
@@ -294,6 +340,7 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
         h->groupCls.push_back(cls);
         h->groupPlan.push_back(e);
         h->groupM.push_back(M);
+        h->groupCount.push_back((uint32_t)kv.second.size());
         h->groupTileBegin.push_back((uint32_t)tiles.size());
         const uint32_t first = (uint32_t)offsByGroup.size();
         for (uint32_t i : kv.second) offsByGroup.push_back(offset[i]);
@@ -311,7 +358,7 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
     for (int cls = 0; cls < kMixedClasses; ++cls) {
         h->clsTileBegin[cls] = (uint32_t)lpt.size();
         for (const MixedTile& t : tiles)
-            if (h->groupCls[t.group] == cls) lpt.push_back(t);
+            if (h->groupCls[t.group] == cls && !groupFixed[t.group]) lpt.push_back(t);
         std::stable_sort(lpt.begin() + h->clsTileBegin[cls], lpt.end(), [&](const MixedTile& a, const MixedTile& b) {
             const double ca = (double)h->groupN[a.group] * a.count, cb = (double)h->groupN[b.group] * b.count;
             return ca > cb;
@@ -336,10 +383,66 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
         uint32_t unused = 0;
         if (h->clsTiles[cls]) err = class_grid(cls, h->groupStage, h->device, &unused);
     }
+    // Branches: the device runs kernels of at most kMaxBranches streams side
+    // by side (its default number of hardware work queues), so the fixed
+    // groups are packed into that many branches, largest work first onto the
+    // least loaded; each class with tiles takes a branch of its own. Every
+    // branch gets the fraction of the device (SMs times a kernel's CTAs per
+    // SM) that its work is of the batch's and runs its launches back to back
+    // on it; the runtime-radix passes of the persistent kernel count twice
+    // per byte.
+    constexpr size_t kMaxBranches = 8;
+    size_t classBranches = 0;
+    for (int cls = 0; cls < kMixedClasses; ++cls) classBranches += h->clsTiles[cls] ? 1 : 0;
+    size_t fixedBranches = 0;
+    if (err == cudaSuccess && !h->fixed.empty()) {
+        int sms = 0;
+        err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+        double total = 0.0, clsW[kMixedClasses] = {};
+        for (const auto& f : h->fixed) total += (double)f.n * f.count;
+        for (size_t g = 0; g < groupFixed.size(); ++g)
+            if (!groupFixed[g]) clsW[h->groupCls[g]] += 2.0 * h->groupN[g] * h->groupCount[g];
+        for (int cls = 0; cls < kMixedClasses; ++cls) total += clsW[cls];
+        fixedBranches = std::max<size_t>(1, std::min(h->fixed.size(), kMaxBranches - std::min(classBranches, kMaxBranches - 1)));
+        std::vector<double> load(fixedBranches, 0.0);
+        std::vector<size_t> order(h->fixed.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+            return (double)h->fixed[a].n * h->fixed[a].count > (double)h->fixed[b].n * h->fixed[b].count;
+        });
+        for (size_t i : order) {
+            const size_t b = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+            h->fixed[i].branch = (uint32_t)b;
+            load[b] += (double)h->fixed[i].n * h->fixed[i].count;
+        }
+        for (auto& f : h->fixed) {
+            const int res = static_pipelined_resident(f.n, f.plan->eng.emax, f.plan->eng.T, f.plan->eng.P,
+                                                      f.plan->eng.R);
+            f.grid = (uint32_t)std::max(1.0, std::round((double)sms * res * load[f.branch] / total));
+            h->fixedPoints += (uint64_t)f.n * f.count;
+        }
+        // launches of a branch in its order: largest first
+        std::stable_sort(h->fixed.begin(), h->fixed.end(), [](const FFTLIB_b200_mixed::Fixed& a,
+                                                              const FFTLIB_b200_mixed::Fixed& b) {
+            return a.branch < b.branch;
+        });
+        for (int cls = 0; cls < kMixedClasses; ++cls)
+            if (h->clsTiles[cls])
+                h->clsGrid[cls] =
+                    std::max(1u, std::min(h->clsGrid[cls], (uint32_t)std::round(h->clsGrid[cls] * clsW[cls] / total)));
+    }
+    h->fixedBranches = (uint32_t)fixedBranches;
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&h->capture, cudaStreamNonBlocking);
-    if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
     if (err == cudaSuccess) err = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
-    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
+    const size_t nb = fixedBranches + classBranches;
+    for (size_t b = 0; b < nb && err == cudaSuccess; ++b) {
+        cudaStream_t bs = nullptr;
+        cudaEvent_t be = nullptr;
+        err = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking);
+        if (err == cudaSuccess) h->branches.push_back(bs);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&be, cudaEventDisableTiming);
+        if (err == cudaSuccess) h->joins.push_back(be);
+    }
     if (err == cudaSuccess) err = cudaStreamSynchronize(s);
     if (err != cudaSuccess) {
         release(h);
@@ -368,7 +471,7 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_exec(FFTLIB_b200_mixedHandle h, const FFTLIB_
         h->graph = nullptr;
         err = cudaStreamBeginCapture(h->capture, cudaStreamCaptureModeThreadLocal);
         if (err == cudaSuccess) {
-            cudaError_t le = enqueue_classes(h, pX, pY, h->capture);
+            cudaError_t le = enqueue_all(h, pX, pY, h->capture);
             err = cudaStreamEndCapture(h->capture, &h->graph);
             if (err == cudaSuccess) err = le;
         }
@@ -401,7 +504,10 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_describe(FFTLIB_b200_mixedHandle h, char* buf
 {
     if (!h || !buf || len == 0) return FFTLIB_ERR_NULL_POINTER;
     std::ostringstream os;
-    os << h->count << " transforms, " << h->groupN.size() << " lengths, " << h->numTiles << " tiles";
+    os << h->count << " transforms, " << h->groupN.size() << " lengths, " << h->fixed.size()
+       << " fixed-size groups (" << h->fixedPoints << " points, grids";
+    for (const auto& f : h->fixed) os << " " << f.n << ":" << f.branch << "/" << f.grid;
+    os << "), " << h->numTiles << " tiles";
     for (int cls = 0; cls < kMixedClasses; ++cls)
         if (h->clsTiles[cls])
             os << "; class E" << mixed_class_emax(cls) << ": " << h->clsTiles[cls] << " tiles, grid " << h->clsGrid[cls]

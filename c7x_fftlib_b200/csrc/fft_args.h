@@ -92,6 +92,9 @@ struct FftArgs {
     // 0: Mc = M); mMagic = fastdiv_magic(M)
     uint32_t Mc;
     uint32_t mMagic;
+    // host-side launch hint of the persistent kernels: at most this many CTAs
+    // (0: as many as are resident); no kernel reads it
+    uint32_t gridCap;
 };
 
 // Transforms one CTA computes at a time (its threads: T of them each).

@@ -32,10 +32,15 @@ struct StaticEntry {
     // persistent TMA-pipelined variant (M == 1, contiguous 16-byte aligned
     // rows, complex in and out), or null
     cudaError_t (*launchPipelined)(const FftArgs&, cudaStream_t);
+    // CTAs per SM of that variant on the current device, or null
+    int (*residentPipelined)();
 };
 const std::vector<StaticEntry>& static_schedules();
 // maxThreads of the compiled fixed-size kernel for this schedule, or 0.
 int static_max_threads(uint32_t n, int emax, uint32_t T, int P, const int* R);
+// CTAs per SM of its persistent pipelined variant on the current device, or
+// 0 when the schedule has none.
+int static_pipelined_resident(uint32_t n, int emax, uint32_t T, int P, const int* R);
 
 // W[i] = exp(-2 pi i (i stride mod n) / n), i < count, computed in FP64.
 cudaError_t launch_twiddle(float2* w, uint32_t n, uint32_t count, cudaStream_t s, uint32_t stride = 1);

@@ -106,6 +106,17 @@ int static_max_threads(uint32_t n, int emax, uint32_t T, int P, const int* R)
     return 0;
 }
 
+int static_pipelined_resident(uint32_t n, int emax, uint32_t T, int P, const int* R)
+{
+    for (const StaticEntry& e : static_schedules()) {
+        if (e.n != n || e.emax != emax || e.T != T || e.P != P) continue;
+        bool same = true;
+        for (int p = 0; p < P; ++p) same = same && (e.R[p] == R[p]);
+        if (same) return e.residentPipelined ? e.residentPipelined() : 0;
+    }
+    return 0;
+}
+
 cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
 {
     if (a.batch == 0) return cudaSuccess;

@@ -88,9 +88,27 @@ cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
         sms = c.sms;
     }
     const uint32_t tiles = (a.batch + (uint32_t)M - 1u) / (uint32_t)M;
-    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)std::max(1, resident * sms));
+    uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)std::max(1, resident * sms));
+    if (a.gridCap) grid = std::max(1u, std::min(grid, a.gridCap));
     k_fft_pipe<S, STAGES, REGFLOOR><<<grid, S::T * M, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+// CTAs per SM of the persistent pipelined kernel.
+template <class S, int STAGES, int REGFLOOR>
+int resident_pipe()
+{
+    constexpr int M = pipe_tile(S::T);
+    const size_t smem = pipe_smem_bytes((uint32_t)S::N, STAGES, M);
+    int blocks = 0;
+    if (cudaFuncSetAttribute(k_fft_pipe<S, STAGES, REGFLOOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_fft_pipe<S, STAGES, REGFLOOR>, S::T * M, smem) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return blocks;
 }
 
 // REGFLOOR: see pipe_min_blocks (0 for the schedules tuned by hand).
@@ -111,8 +129,10 @@ StaticEntry static_entry()
     // its first value, see tile_span)
     if constexpr (S::P >= 2 && pipe_smem_bytes(S::N, 2, pipe_tile(S::T)) <= 227u * 1024u) {
         e.launchPipelined = &launch_pipe<S, 2, REGFLOOR>;
+        e.residentPipelined = &resident_pipe<S, 2, REGFLOOR>;
     } else {
         e.launchPipelined = nullptr;
+        e.residentPipelined = nullptr;
     }
     return e;
 }

@@ -543,7 +543,8 @@ cudaError_t run_global(const ComplexPlan* p, float2* in, float2* out, uint32_t b
 
 } // namespace
 
-cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse, cudaStream_t s)
+cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse, cudaStream_t s,
+                    uint32_t gridCap)
 {
     if (batch == 0) return cudaSuccess;
     if (p->multiPass) return run_global(p, in, out, batch, inverse, s);
@@ -559,6 +560,7 @@ cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batc
     a.outElem = 1;
     a.conjIn = a.conjOut = inverse ? 1 : 0;
     a.scale = inverse ? 1.0f / (float)n : 1.0f;
+    a.gridCap = gridCap;
     finalize_launch(a, p->eng, true, true);
     return launch_fft(a, p->eng.emax, s);
 }

@@ -86,21 +86,27 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc(FFTLIB_F3
                                                                        uint32_t numPoints, uint32_t numChannels,
                                                                        void *stream);
 
-/* Batches of FP32 complex-to-complex transforms of uneven lengths, run by a
- * single persistent kernel launch replayed from a CUDA graph. No counterpart
- * in the reference library (its batched kernels take one length per call).
- * Transform i has length numPoints[i] (2^a 3^b 5^c, at most 4096) and occupies
- * 2 * numPoints[i] floats of pX and of pY, the transforms packed back to back
- * in the order given. create() groups the transforms by length, picks each
- * group's radix schedule (timed by the autotuner when FFTLIB_B200_MIXED_AUTOTUNE
- * is set or $FFTLIB_B200_AUTOTUNE is non-zero; results cached in
- * $FFTLIB_B200_TUNE_CACHE, default $HOME/.cache/fftlib_b200_tune.txt) and
- * uploads the schedule and tile tables. exec() enqueues the transform on
- * `stream` (device buffers) and returns; execPerSize() runs the same work as
- * one launch per distinct length, for comparison. */
+/* Batches of FP32 complex-to-complex transforms of uneven lengths, replayed
+ * from one CUDA graph. No counterpart in the reference library (its batched
+ * kernels take one length per call). Transform i has length numPoints[i]
+ * (2^a 3^b 5^c, at most 4096) and occupies 2 * numPoints[i] floats of pX and
+ * of pY, the transforms packed back to back in the order given. create()
+ * groups the transforms by length. A group whose transforms lie back to back
+ * runs its length's persistent fixed-size kernel on a grid proportional to
+ * its share of the batch, every group on its own graph branch, so that the
+ * groups run side by side and finish together; the other groups (or all,
+ * with FFTLIB_B200_MIXED_PERSISTENT_ONLY) run in one persistent kernel over a
+ * device-resident tile table, with radix schedules picked by the planner or
+ * timed by the autotuner (FFTLIB_B200_MIXED_AUTOTUNE, or $FFTLIB_B200_AUTOTUNE
+ * non-zero; results cached in $FFTLIB_B200_TUNE_CACHE, default
+ * $HOME/.cache/fftlib_b200_tune.txt). exec() enqueues the transform on `stream`
+ * (device buffers) and returns; execPerSize() runs the persistent kernel once
+ * per distinct length, for comparison. */
 typedef struct FFTLIB_b200_mixed *FFTLIB_b200_mixedHandle;
 #define FFTLIB_B200_MIXED_INVERSE  1u
 #define FFTLIB_B200_MIXED_AUTOTUNE 2u
+/* every group in the single persistent kernel (no fixed-size groups) */
+#define FFTLIB_B200_MIXED_PERSISTENT_ONLY 4u
 FFTLIB_STATUS FFTLIB_b200_fftMixed_supported(uint32_t numPoints);
 FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t *numPoints, uint32_t count, uint32_t flags,
                                           FFTLIB_b200_mixedHandle *handle);

@@ -139,14 +139,15 @@ def test_r2c_c2r_n4096_x8192_every_channel(torch):
     assert float((e / d).max()) <= REL_L2
 
 
+@pytest.mark.parametrize("persistent_only", [False, True])
 @pytest.mark.parametrize("inverse", [False, True])
-def test_mixed_20000_bench_set_every_transform(torch, inverse):
+def test_mixed_20000_bench_set_every_transform(torch, inverse, persistent_only):
     lengths = np.sort(fftcall.mixed_lengths(20000, seed=2024))[::-1].copy()
     total = int(lengths.sum())
     g = torch.Generator(device="cuda").manual_seed(7)
     x = torch.rand(2 * total, device="cuda", generator=g) * 2 - 1
     y = torch.empty_like(x)
-    mb = F.MixedBatch(lengths, inverse=inverse)
+    mb = F.MixedBatch(lengths, inverse=inverse, persistent_only=persistent_only)
     st = torch.cuda.current_stream().cuda_stream
     for _ in range(2):  # the graph is replayed, as in the bench
         mb.exec(x, y, F.ptr(st))

@@ -114,3 +114,21 @@ def test_mixed_buffers_off_16_byte_boundary(torch):
     torch.cuda.synchronize()
     check_all(x, Y[2:2 + 2 * total].cpu().numpy(), lengths)
     mb.close()
+
+
+@pytest.mark.parametrize("inverse", [False, True])
+def test_mixed_grouped_and_persistent_agree(torch, inverse):
+    """Lengths stored grouped (fixed-size kernels on grid shares) and the same
+    batch in the single persistent kernel: both against FP64."""
+    lengths = np.sort(fftcall.mixed_lengths(2000, seed=31))[::-1].copy()
+    total = int(lengths.sum())
+    x = O.uniform_c2c(total, 1, seed=32)
+    X = torch.from_numpy(x).cuda()
+    for po in (False, True):
+        Y = torch.zeros_like(X)
+        mb = F.MixedBatch(lengths, inverse=inverse, persistent_only=po)
+        assert ("fixed-size groups" in mb.describe())
+        mb.exec(X, Y)
+        torch.cuda.synchronize()
+        check_all(x, Y.cpu().numpy(), lengths, inverse)
+        mb.close()
