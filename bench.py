@@ -329,7 +329,8 @@ def our_arm(args, world, rank, local):
         "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "numPoints": n, "numChannels_per_gpu": ch, "parallelism": f"replicas{world}",
-                   "plan": F.describe_plan(n), "l2": "inputs (256 MiB) larger than L2, no flush",
+                   "plan": F.describe_block(pb), "autotune": autotune_on(),
+                   "l2": "inputs (256 MiB) larger than L2, no flush",
                    "transforms_per_s": round(ch * world / (ms_step * 1e-3), 1)},
         "roofline": {"bound": "hbm", "achieved": round(per_gpu_gbs, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(per_gpu_gbs / peak, 4), "peak_source": peak_kind,
@@ -349,6 +350,11 @@ def our_arm(args, world, rank, local):
     print(json.dumps(out))
     if PARITY_FAILURES:
         sys.exit(1)
+
+
+def autotune_on():
+    v = os.environ.get("FFTLIB_B200_AUTOTUNE", "")
+    return bool(v) and v != "0"
 
 
 def _time_launches(torch, stream, fn, steps, warmup=3):
@@ -410,7 +416,8 @@ def secondary_configs(args):
     xs = x[: 2 * n * k16].cpu().numpy()
     exact16 = bool(np.array_equal(y[: 2 * n * k16].cpu().numpy(), O.fft_c2c_i16(xs, n, k16, [2] * 5)))
     parity_check("int16_c2c_1024 bit-exact sample", exact16)
-    res["int16_c2c_n1024_x4096"] = {"ms": round(ms, 4), "GBps": round(8.0 * n * ch / ms / 1e6, 1),
+    res["int16_c2c_n1024_x4096"] = {"plan": F.describe_block(pb), "ms": round(ms, 4),
+                                     "GBps": round(8.0 * n * ch / ms / 1e6, 1),
                                      "transforms_per_s": round(ch / ms * 1e3, 1), "bit_exact_sample": exact16}
 
     # r2c then c2r, N=4096 x 8192 reals (128 MiB), outmode / inMode 0
@@ -438,7 +445,8 @@ def secondary_configs(args):
     fwd = float(np.linalg.norm(got[..., 0] + 1j * got[..., 1] - want) / np.linalg.norm(want))
     parity_check("r2c_4096 sampled rel-L2", fwd <= REL_L2_BOUND, fwd)
     parity_check("r2c->c2r round trip rel-L2", rt <= REL_L2_BOUND, rt)
-    res["r2c_c2r_n4096_x8192"] = {"r2c_ms": round(ms_r, 4), "r2c_GBps": round(bytes_rc / ms_r / 1e6, 1),
+    res["r2c_c2r_n4096_x8192"] = {"r2c_plan": F.describe_block(pr), "c2r_plan": F.describe_block(pc),
+                                  "r2c_ms": round(ms_r, 4), "r2c_GBps": round(bytes_rc / ms_r / 1e6, 1),
                                   "c2r_ms": round(ms_c, 4), "c2r_GBps": round(bytes_rc / ms_c / 1e6, 1),
                                   "r2c_rel_l2_vs_fp64_sampled": fwd, "roundtrip_rel_l2": rt}
 
@@ -883,10 +891,19 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--channels", type=int, default=CHANNELS, help="channels per GPU (default: the workload's 8192)")
     ap.add_argument("--quick", action="store_true", help="time the kernel only (for profiler captures)")
+    ap.add_argument("--autotune", type=int, choices=[0, 1], default=0,
+                    help="1: every _init times its launch candidates (FFTLIB_B200_AUTOTUNE=1), with a fresh "
+                         "cache file unless FFTLIB_B200_TUNE_CACHE names one")
     ap.add_argument("--case", default=None,
                     help="time one kernel only, for profiler captures: tc:N:batch (tensor-core DFT), "
                          "fft:N:batch (CUDA-core FFT through the same coordinator API)")
     args = ap.parse_args()
+    if args.autotune:
+        import tempfile
+
+        os.environ["FFTLIB_B200_AUTOTUNE"] = "1"
+        if "FFTLIB_B200_TUNE_CACHE" not in os.environ:
+            os.environ["FFTLIB_B200_TUNE_CACHE"] = os.path.join(tempfile.mkdtemp(prefix="fftlib_tune_"), "tune.txt")
     if args.case:
         run_case(args)
         return

@@ -180,6 +180,8 @@ def lib() -> C.CDLL:
     L.FFTLIB_b200_version.restype = C.c_int
     L.FFTLIB_b200_describePlan.argtypes = [_u32, C.c_char_p, _u32]
     L.FFTLIB_b200_describePlan.restype = C.c_int
+    L.FFTLIB_b200_describeBlock.argtypes = [_vp, C.c_char_p, _u32]
+    L.FFTLIB_b200_describeBlock.restype = C.c_int
     L.FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync.argtypes = [_vp, _vp, _u32, _u32, _vp, _vp]
     L.FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32fc_kernelAsync.argtypes = [_vp, _vp, _u32, _u32, _vp, _vp]
     L.FFTLIB_b200_fft1dBatched_i32f_c32fc_o32fc_kernelAsync.argtypes = [_vp, _vp, _vp, _u32, _u32, _u8, _vp, _vp]
@@ -289,6 +291,13 @@ def check(status: int, what: str = "FFTLIB call") -> None:
 def describe_plan(n: int) -> str:
     buf = C.create_string_buffer(256)
     check(lib().FFTLIB_b200_describePlan(n, buf, 256), "describePlan")
+    return buf.value.decode()
+
+
+def describe_block(pblock) -> str:
+    """The launch an _init recorded in pblock ("tuned: ..." or "planner: ...")."""
+    buf = C.create_string_buffer(256)
+    check(lib().FFTLIB_b200_describeBlock(ptr(pblock), buf, 256), "describeBlock")
     return buf.value.decode()
 
 

@@ -113,6 +113,31 @@ FFTLIB_STATUS FFTLIB_b200_describePlan(uint32_t numPoints, char* buf, uint32_t l
     return FFTLIB_SUCCESS;
 }
 
+FFTLIB_STATUS FFTLIB_b200_describeBlock(const void* pBlock, char* buf, uint32_t len)
+{
+    if (!pBlock || !buf || len == 0) return FFTLIB_ERR_NULL_POINTER;
+    PlanRecord r;
+    memcpy(&r, pBlock, sizeof(r));
+    if (r.magic != kRecordMagic) {
+        set_error("pBlock was not initialised by an _init");
+        return FFTLIB_ERR_FAILURE;
+    }
+    std::string s;
+    if (r.kind == REC_I16 || r.kind == REC_1D_I16) {
+        const uint32_t tg = r.i16Tg ? r.i16Tg : i16_default_tg(r.numPoints);
+        s = std::string(r.i16Tuned ? "tuned: " : "planner: ") + "int16 radix-4, " + std::to_string(tg) +
+            " threads per transform, " + std::to_string(256u / tg) + " transforms per CTA";
+        if (r.i16GridCap) s += ", " + std::to_string(r.i16GridCap) + " CTAs";
+    } else if (r.plan) {
+        s = describe_plan(r.plan);
+    } else {
+        return FFTLIB_ERR_FAILURE;
+    }
+    strncpy(buf, s.c_str(), len - 1);
+    buf[len - 1] = '\0';
+    return FFTLIB_SUCCESS;
+}
+
 FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync(FFTLIB_F32* pX, FFTLIB_F32* pY,
                                                                      uint32_t numPoints, uint32_t numChannels,
                                                                      void* pBlock, void* stream)
@@ -173,7 +198,8 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync(int16_t* pX
     if (st != FFTLIB_SUCCESS) return st;
     if (!pX || !pW || !pY || !pShift) return FFTLIB_ERR_NULL_POINTER;
     if (numShifts < i16_num_shifts(numPoints)) return FFTLIB_ERR_INVALID_DIMENSION;
-    return launched(launch_fft_i16(pX, pY, pW, pShift, numPoints, numChannels, (cudaStream_t)stream),
+    return launched(launch_fft_i16(pX, pY, pW, pShift, numPoints, numChannels, (cudaStream_t)stream, r.i16Tg,
+                                   r.i16GridCap),
                     "fft1dBatched int16");
 }
 

@@ -207,7 +207,7 @@ FFTLIB_STATUS exec_c2r(float* pX, float* pXFFT, float* pY, uint32_t n, uint32_t 
 }
 
 FFTLIB_STATUS exec_i16(int16_t* pX, const int16_t* pW, int16_t* pY, const uint32_t* pShift, uint32_t numShifts,
-                       uint32_t n, uint32_t c)
+                       uint32_t n, uint32_t c, uint32_t tg, uint32_t gridCap)
 {
     if (n == 0 || (n & (n - 1u)) || n > 16384u) {
         set_error("int16 numPoints %u must be a power of two <= 16384", n);
@@ -226,7 +226,8 @@ FFTLIB_STATUS exec_i16(int16_t* pX, const int16_t* pW, int16_t* pY, const uint32
     const size_t bytes = (size_t)n * 2u * sizeof(int16_t);
     std::vector<ChannelBuf> bufs = {{pX, bytes, true, false}, {pY, bytes, false, true}};
     e = run_channels(bufs, c, [&](const std::vector<void*>& d, uint32_t, uint32_t cnt, cudaStream_t s) {
-        return launch_fft_i16((const int16_t*)d[0], (int16_t*)d[1], (const int16_t*)dW, (const uint32_t*)dS, n, cnt, s);
+        return launch_fft_i16((const int16_t*)d[0], (int16_t*)d[1], (const int16_t*)dW, (const uint32_t*)dS, n, cnt, s,
+                              tg, gridCap);
     });
     if (e != cudaSuccess) return cuda_fail(e, "fft1dBatched int16");
     return FFTLIB_SUCCESS;
@@ -239,7 +240,16 @@ FFTLIB_STATUS init_fp32(void* pBlock, uint32_t kind, uint32_t n, uint32_t c, uin
         return FFTLIB_ERR_INVALID_DIMENSION;
     }
     cudaError_t e;
-    ComplexPlan* plan = get_complex_plan(real ? n / 2u : n, real, &e);
+    const uint32_t len = real ? n / 2u : n;
+    // the batched kinds take the autotuner's choice when it is enabled
+    ComplexPlan* plan;
+    switch (kind) {
+    case REC_C2C: plan = get_batched_plan(len, real, TUNE_C2C, 0, c, &e); break;
+    case REC_IFFT: plan = get_batched_plan(len, real, TUNE_IFFT, 0, c, &e); break;
+    case REC_R2C: plan = get_batched_plan(len, real, TUNE_R2C, (int)mode, c, &e); break;
+    case REC_C2R: plan = get_batched_plan(len, real, TUNE_C2R, (int)mode, c, &e); break;
+    default: plan = get_complex_plan(len, real, &e); break;
+    }
     if (!plan) return cuda_fail(e, "plan creation");
     return write_record(pBlock, kind, n, c, mode, plan);
 }
@@ -535,7 +545,17 @@ FFTLIB_STATUS FFTLIB_fft1dBatched_i16sc_c16sc_o16sc_init(int16_t* pX, FFTLIB_buf
         set_error("int16 numPoints %u must be a power of two <= 16384", numPoints);
         return FFTLIB_ERR_INVALID_DIMENSION;
     }
-    return write_record(pBlock, REC_I16, numPoints, numChannels, 0, nullptr);
+    st = write_record(pBlock, REC_I16, numPoints, numChannels, 0, nullptr);
+    I16Choice ch{};
+    if (st == FFTLIB_SUCCESS && autotune_enabled() && tune_i16(numPoints, numChannels, &ch)) {
+        PlanRecord r;
+        memcpy(&r, pBlock, sizeof(r));
+        r.i16Tg = ch.tg;
+        r.i16GridCap = ch.gridCap;
+        r.i16Tuned = 1u;
+        memcpy(pBlock, &r, sizeof(r));
+    }
+    return st;
 }
 
 FFTLIB_STATUS FFTLIB_fft1dBatched_i16sc_c16sc_o16sc_kernel(int16_t* pX, FFTLIB_bufParams1D_t* bufParamsX,
@@ -550,7 +570,7 @@ FFTLIB_STATUS FFTLIB_fft1dBatched_i16sc_c16sc_o16sc_kernel(int16_t* pX, FFTLIB_b
     if (st != FFTLIB_SUCCESS) return st;
     if (!pX || !pW || !pY || !pShift || !bufParamsShift) return FFTLIB_ERR_NULL_POINTER;
     DeviceScope scope(r.device);
-    return exec_i16(pX, pW, pY, pShift, bufParamsShift->dim_x, numPoints, numChannels);
+    return exec_i16(pX, pW, pY, pShift, bufParamsShift->dim_x, numPoints, numChannels, r.i16Tg, r.i16GridCap);
 }
 
 FFTLIB_STATUS FFTLIB_fft1dBatched_i16sc_c16sc_o16sc_cn(int16_t* pX, FFTLIB_bufParams1D_t* bufParamsX,

@@ -92,9 +92,12 @@ struct FftArgs {
     // 0: Mc = M); mMagic = fastdiv_magic(M)
     uint32_t Mc;
     uint32_t mMagic;
-    // host-side launch hint of the persistent kernels: at most this many CTAs
-    // (0: as many as are resident); no kernel reads it
+    // host-side launch hints, read by no kernel: at most gridCap CTAs for the
+    // persistent kernels (0: as many as are resident); noPipe != 0 runs a
+    // fixed-size schedule's one-tile-per-CTA kernel instead of its persistent
+    // pipelined one
     uint32_t gridCap;
+    uint32_t noPipe;
 };
 
 // Transforms one CTA computes at a time (its threads: T of them each).

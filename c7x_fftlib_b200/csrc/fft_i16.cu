@@ -18,6 +18,7 @@
 // traffic and barriers.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <mutex>
 #include <stdint.h>
 
 #include "fft_i16.h"
@@ -300,30 +301,69 @@ uint32_t i16_num_shifts(uint32_t n)
     return s;
 }
 
+uint32_t i16_default_tg(uint32_t n) { return n >= 4096u ? 256u : (n / 16u >= 1u ? n / 16u : 1u); }
+
+size_t i16_smem_bytes(uint32_t n, uint32_t tg)
+{
+    const uint32_t G = 256u / tg;
+    return (size_t)n * sizeof(int2) + (size_t)G * (n + (n >> 4)) * sizeof(short2);
+}
+
+namespace {
+
+cudaError_t i16_configure(size_t smem)
+{
+    static std::mutex mu;
+    static size_t configured[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (smem <= 48u * 1024u) return cudaSuccess;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && configured[dev] >= smem) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_fft_i16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && dev < 64) configured[dev] = smem;
+    return e;
+}
+
+} // namespace
+
+int i16_resident(uint32_t n, uint32_t tg)
+{
+    const size_t smem = i16_smem_bytes(n, tg);
+    int perSm = 0;
+    if (i16_configure(smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_fft_i16, 256, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return perSm;
+}
+
 cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const uint32_t* shifts,
-                           uint32_t n, uint32_t batch, cudaStream_t s)
+                           uint32_t n, uint32_t batch, cudaStream_t s, uint32_t tg, uint32_t gridCap)
 {
     if (batch == 0) return cudaSuccess;
     uint32_t logn = 0;
     while ((1u << logn) < n) ++logn;
-    const uint32_t tg = n >= 4096u ? 256u : (n / 16u >= 1u ? n / 16u : 1u);
+    if (tg == 0) tg = i16_default_tg(n);
+    if (tg > 256u || (tg & (tg - 1u))) return cudaErrorInvalidValue;
     const uint32_t G = 256u / tg;
     const uint32_t threads = tg * G;
-    const size_t smem = (size_t)n * sizeof(int2) + (size_t)G * (n + (n >> 4)) * sizeof(short2);
+    const size_t smem = i16_smem_bytes(n, tg);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (smem > 48u * 1024u) {
-        e = cudaFuncSetAttribute(k_fft_i16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
+    e = i16_configure(smem);
+    if (e != cudaSuccess) return e;
     int perSm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_fft_i16, (int)threads, smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
     const uint64_t steps = (batch + G - 1u) / G;
-    const uint32_t grid = (uint32_t)std::min<uint64_t>(steps, (uint64_t)std::max(1, perSm) * (uint64_t)sms);
+    uint32_t grid = (uint32_t)std::min<uint64_t>(steps, (uint64_t)std::max(1, perSm) * (uint64_t)sms);
+    if (gridCap) grid = std::max(1u, std::min(grid, gridCap));
     const bool vec = (((uintptr_t)x & 15u) == 0) && (n % 4u) == 0;
     k_fft_i16<<<grid, threads, smem, s>>>((const short2*)x, (short2*)y, (const short2*)w, shifts, i16_num_shifts(n),
                                           n, logn, batch, tg, vec);

@@ -127,8 +127,8 @@ cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
         // the stage holds beside its padded exchange layout for N >= 64)
         const bool rowsOk = ((a.ioMode == IO_C2C || a.ioMode == IO_R2C_SPLIT) && a.inBatch == (int64_t)a.N) ||
                             (a.ioMode == IO_C2R_SPLIT && !a.realMode && a.inBatch == (int64_t)a.N + 1 && a.N >= 64u);
-        const bool pipelinable = st->launchPipelined && a.err && rowsOk && !a.batchMinor && !a.perCh &&
-                                 a.inElem == 1 && a.outElem == 1 && ((uintptr_t)a.in & 15u) == 0 &&
+        const bool pipelinable = st->launchPipelined && !a.noPipe && a.err && rowsOk && !a.batchMinor &&
+                                 !a.perCh && a.inElem == 1 && a.outElem == 1 && ((uintptr_t)a.in & 15u) == 0 &&
                                  ((a.N % 2u) == 0 || a.ioMode == IO_C2C);
         if (pipelinable) {
             FftArgs b = a;

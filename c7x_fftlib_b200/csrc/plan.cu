@@ -375,8 +375,6 @@ ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err)
         p->n = n;
         cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, dev);
         if (n <= kMaxSingleN && plan_engine(n, &p->eng)) {
-            EnginePlan tuned;
-            if (autotune_enabled() && tune_schedule(n, 4096, 0, 0, &tuned)) p->eng = tuned;
             *err = make_pass_table(&p->tw, p->eng, s);
         } else if (split_global(n, &p->G, p->R)) {
             p->multiPass = true;
@@ -421,23 +419,99 @@ ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err)
     return slot;
 }
 
+namespace {
+
+// Tuned plans, per (device, length and choice).
+std::map<std::pair<int, std::string>, ComplexPlan*> g_tuned_plans;
+
+std::string choice_key(uint32_t n, const BatchedChoice& c)
+{
+    return std::to_string(n) + " " + describe(c.eng) + " g" + std::to_string(c.gridCap) + " m" +
+           std::to_string(c.tileM) + (c.noPipe ? " np" : "");
+}
+
+void free_plan(ComplexPlan* p)
+{
+    cudaSetDevice(p->device);
+    cudaFree(p->tw);
+    for (float2* t : p->twG) cudaFree(t);
+    cudaFree(p->twLo);
+    cudaFree(p->twHi);
+    cudaFree(p->twSplit);
+    delete p;
+}
+
+} // namespace
+
+ComplexPlan* get_batched_plan(uint32_t n, bool needSplit, int kind, int mode, uint32_t batch, cudaError_t* err)
+{
+    ComplexPlan* base = get_complex_plan(n, needSplit, err);
+    if (!base || base->multiPass || !autotune_enabled()) return base;
+    BatchedChoice c;
+    if (!tune_batched(base, kind, mode, batch, &c)) return base;
+    std::lock_guard<std::mutex> lock(g_mu);
+    ComplexPlan*& slot = g_tuned_plans[{base->device, choice_key(n, c)}];
+    cudaStream_t s = cudaStreamPerThread;
+    if (!slot) {
+        ComplexPlan* p = new ComplexPlan();
+        p->device = base->device;
+        p->sms = base->sms;
+        p->n = n;
+        p->eng = c.eng;
+        p->gridCap = c.gridCap;
+        p->tileM = c.tileM;
+        p->noPipe = c.noPipe;
+        p->tuned = true;
+        *err = make_pass_table(&p->tw, p->eng, s);
+        if (*err == cudaSuccess) *err = cudaStreamSynchronize(s);
+        if (*err != cudaSuccess) {
+            free_plan(p);
+            g_tuned_plans.erase({base->device, choice_key(n, c)});
+            return nullptr;
+        }
+        slot = p;
+    }
+    if (needSplit && !slot->twSplit) {
+        *err = make_table(&slot->twSplit, 2u * n, n, s);
+        if (*err == cudaSuccess) *err = cudaStreamSynchronize(s);
+        if (*err != cudaSuccess) {
+            cudaFree(slot->twSplit);
+            slot->twSplit = nullptr;
+            return nullptr;
+        }
+    }
+    return slot;
+}
+
+std::string describe_plan(const ComplexPlan* p)
+{
+    if (p->multiPass) {
+        std::string s = "planner: global passes";
+        for (int g = 0; g < p->G; ++g)
+            s += (g ? " x " : " ") + std::to_string(p->R[g]) + " [" + describe(p->engG[g]) + "]";
+        return s;
+    }
+    const EnginePlan& e = p->eng;
+    const bool fixed = static_max_threads(p->n, e.emax, e.T, e.P, e.R) != 0;
+    const bool pipe = fixed && !p->noPipe && static_pipelined_resident(p->n, e.emax, e.T, e.P, e.R) > 0;
+    std::string s = std::string(p->tuned ? "tuned: " : "planner: ") + describe(e);
+    s += fixed ? (pipe ? " (fixed-size pipelined kernel" : " (fixed-size kernel") : " (runtime-radix engine";
+    if (pipe && p->gridCap) s += ", " + std::to_string(p->gridCap) + " CTAs";
+    if (!pipe && p->tileM) s += ", " + std::to_string(p->tileM) + " transforms per CTA";
+    return s + ")";
+}
+
 void release_all_plans()
 {
     std::lock_guard<std::mutex> lock(g_mu);
     int cur = 0;
     cudaGetDevice(&cur);
-    for (auto& kv : g_plans) {
-        ComplexPlan* p = kv.second;
-        if (!p) continue;
-        cudaSetDevice(p->device);
-        cudaFree(p->tw);
-        for (float2* t : p->twG) cudaFree(t);
-        cudaFree(p->twLo);
-        cudaFree(p->twHi);
-        cudaFree(p->twSplit);
-        delete p;
-    }
+    for (auto& kv : g_plans)
+        if (kv.second) free_plan(kv.second);
+    for (auto& kv : g_tuned_plans)
+        if (kv.second) free_plan(kv.second);
     g_plans.clear();
+    g_tuned_plans.clear();
     cudaSetDevice(cur);
 }
 
@@ -543,6 +617,19 @@ cudaError_t run_global(const ComplexPlan* p, float2* in, float2* out, uint32_t b
 
 } // namespace
 
+namespace {
+
+// The plan's launch choices on top of finalize_launch's (tileM only lowers
+// the transforms per CTA, so the tile still fits where the planner's did).
+void apply_choice(FftArgs& a, const ComplexPlan* p)
+{
+    a.gridCap = p->gridCap;
+    a.noPipe = p->noPipe ? 1u : 0u;
+    if (p->tileM && p->tileM < a.M) a.M = p->tileM;
+}
+
+} // namespace
+
 cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse, cudaStream_t s,
                     uint32_t gridCap)
 {
@@ -560,8 +647,9 @@ cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batc
     a.outElem = 1;
     a.conjIn = a.conjOut = inverse ? 1 : 0;
     a.scale = inverse ? 1.0f / (float)n : 1.0f;
-    a.gridCap = gridCap;
     finalize_launch(a, p->eng, true, true);
+    apply_choice(a, p);
+    if (gridCap) a.gridCap = gridCap;
     return launch_fft(a, p->eng.emax, s);
 }
 
@@ -589,6 +677,7 @@ cudaError_t run_r2c(const ComplexPlan* p, float* x, float2* scratch, float2* y, 
     a.realMode = outmode ? 1 : 0;
     a.twSplit = p->twSplit;
     finalize_launch(a, p->eng, true, false);
+    apply_choice(a, p);
     return launch_fft(a, p->eng.emax, s);
 }
 
@@ -647,6 +736,7 @@ cudaError_t run_c2r(const ComplexPlan* p, const float2* x, float2* scratch, floa
     a.inMagic = fastdiv_magic(inCount);
     a.slen = smem_len(std::max(h, inCount));
     finalize_launch(a, p->eng, true, true);
+    apply_choice(a, p);
     return launch_fft(a, p->eng.emax, s);
 }
 

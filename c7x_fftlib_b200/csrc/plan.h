@@ -40,10 +40,10 @@ bool plan_engine(uint32_t n, EnginePlan* out);
 // Per-pass twiddle blocks of a schedule, allocated and filled on the device.
 cudaError_t make_pass_table(float2** p, const EnginePlan& e, cudaStream_t s);
 
-// Autotuner: times the heuristic's best candidates for (n, batch) through
-// the real launch path and returns the fastest; results are cached per
-// device, length and batch bucket in memory and in a text file
-// ($FFTLIB_B200_TUNE_CACHE, default $HOME/.cache/fftlib_b200_tune.txt).
+// Autotuner of the mixed-length kernel's schedules: times the heuristic's
+// best candidates for (n, batch) and returns the fastest; results are cached
+// per device, length, batch bucket and width constraints in memory and in a
+// text file ($FFTLIB_B200_TUNE_CACHE, default $HOME/.cache/fftlib_b200_tune.txt).
 // timer(e, x, y, batch, stream, &ok): average milliseconds of one launch of
 // schedule e over `batch` transforms x -> y; the default times launch_fft.
 using ScheduleTimer = float (*)(const EnginePlan&, float2*, float2*, uint32_t, cudaStream_t, bool*);
@@ -51,6 +51,23 @@ bool tune_schedule(uint32_t n, uint32_t batch, int emaxOnly, uint32_t maxT, Engi
                    ScheduleTimer timer = nullptr);
 // True when $FFTLIB_B200_AUTOTUNE is set to a non-zero value.
 bool autotune_enabled();
+// Batch bucket of the tuning keys: the power of four at or above batch.
+uint32_t tune_bucket(uint32_t batch);
+
+// Transform kinds of the batched entry points, as tuning keys see them.
+enum TuneKind : int { TUNE_C2C = 0, TUNE_IFFT = 1, TUNE_R2C = 2, TUNE_C2R = 3 };
+
+// What the batched-path autotuner picks for one FP32 call shape: a radix
+// schedule (its threads per transform included), transforms per CTA for the
+// one-tile-per-CTA kernels (tileM, 0: the planner's), and for a fixed-size
+// schedule whether its persistent pipelined kernel runs (noPipe false) and
+// with how many CTAs (gridCap, 0: all that are resident).
+struct BatchedChoice {
+    EnginePlan eng;
+    uint32_t gridCap = 0;
+    uint32_t tileM = 0;
+    bool noPipe = false;
+};
 std::string describe(const EnginePlan& e);
 // Global Stockham passes for n > kMaxSingleN: n = R[0] R[1] ... R[G-1],
 // each R <= kMaxGlobalRadix a single-kernel length, balanced and ordered so
@@ -74,7 +91,20 @@ struct ComplexPlan {
     float2* twHi = nullptr;          //   W_n^(2^twLoBits q), q < n / 2^twLoBits
     uint32_t twLoBits = 0;
     float2* twSplit = nullptr;       // W_{2n}^i, i < n (real-input kernels)
+    // launch choices of the single kernel (the autotuner's; all 0 otherwise)
+    uint32_t gridCap = 0;            //   CTAs of the persistent kernels (0: all resident)
+    uint32_t tileM = 0;              //   transforms per CTA of the other kernels (0: planner's)
+    bool noPipe = false;             //   one tile per CTA instead of the pipelined kernel
+    bool tuned = false;              //   chosen by timing, for one kind and batch bucket
 };
+
+// Times the batched-path candidates of length base->n for `kind` (r2c / c2r
+// with output / input mode `mode`) over a batch of about `batch` transforms
+// through run_c2c / run_r2c / run_c2r, and returns the fastest: from the
+// in-memory or on-disk cache when this (device, n, kind, dtype, mode, batch
+// bucket) was timed before. base: the planner's plan of that length (its
+// twSplit present for the real kinds). False if nothing could be timed.
+bool tune_batched(const ComplexPlan* base, int kind, int mode, uint32_t batch, BatchedChoice* out);
 
 // Host-visible error word of the current device (mapped pinned memory):
 // kernels with bounded waits write a nonzero code there instead of hanging.
@@ -89,6 +119,13 @@ uint32_t take_device_error();
 // Cached per (current device, n). needSplit also creates twSplit.
 // Returns nullptr (and sets *err) if n is not 2^a 3^b 5^c or on CUDA errors.
 ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err);
+// Plan of a batched _init: get_complex_plan's, or with $FFTLIB_B200_AUTOTUNE
+// set and n a single-kernel length, a plan with the autotuner's choice for
+// (kind, mode, batch) (shared by every call shape that tunes to the same
+// choice; the planner's when timing fails).
+ComplexPlan* get_batched_plan(uint32_t n, bool needSplit, int kind, int mode, uint32_t batch, cudaError_t* err);
+// "tuned" / "planner" plus the schedule and launch choices of p.
+std::string describe_plan(const ComplexPlan* p);
 void release_all_plans();
 
 // Pick transforms-per-CTA and the staged-I/O mode for a launch.

@@ -31,6 +31,14 @@ void FFTLIB_b200_releasePlans(void);
  * (radices per pass, threads per transform, or the four-step split) into buf. */
 FFTLIB_STATUS FFTLIB_b200_describePlan(uint32_t numPoints, char *buf, uint32_t len);
 
+/* Writes the launch an _init recorded in pBlock into buf: "tuned: " when the
+ * autotuner chose it (FFTLIB_B200_AUTOTUNE set to a non-zero value when
+ * _init ran), "planner: " otherwise, then the radix schedule, the kernel
+ * (fixed-size pipelined, fixed-size, or runtime-radix engine) and any CTA or
+ * transforms-per-CTA choice; for int16, the threads per transform. No
+ * reference counterpart (the reference keeps its plan in pBlock opaquely). */
+FFTLIB_STATUS FFTLIB_b200_describeBlock(const void *pBlock, char *buf, uint32_t len);
+
 /* Asynchronous variants of the _kernel calls: every buffer must be device
  * (or managed) memory; the work is enqueued on `stream` (a cudaStream_t;
  * NULL is the legacy default stream) and the call returns without waiting.
