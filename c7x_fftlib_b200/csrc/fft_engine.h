@@ -34,6 +34,9 @@ struct StaticEntry {
     cudaError_t (*launchPipelined)(const FftArgs&, cudaStream_t);
     // CTAs per SM of that variant on the current device, or null
     int (*residentPipelined)();
+    // measured on B200 to beat the planner's heuristic schedule for this
+    // length: plan_engine returns it instead
+    bool preferred;
 };
 const std::vector<StaticEntry>& static_schedules();
 // maxThreads of the compiled fixed-size kernel for this schedule, or 0.

@@ -61,6 +61,11 @@ void register_static_h(std::vector<StaticEntry>& out);
 void register_static_i(std::vector<StaticEntry>& out);
 void register_static_j(std::vector<StaticEntry>& out);
 void register_static_k(std::vector<StaticEntry>& out);
+void register_static_l(std::vector<StaticEntry>& out);
+void register_static_m(std::vector<StaticEntry>& out);
+void register_static_n(std::vector<StaticEntry>& out);
+void register_static_o(std::vector<StaticEntry>& out);
+void register_static_p(std::vector<StaticEntry>& out);
 
 const std::vector<StaticEntry>& static_schedules()
 {
@@ -77,6 +82,11 @@ const std::vector<StaticEntry>& static_schedules()
         register_static_i(t);
         register_static_j(t);
         register_static_k(t);
+        register_static_l(t);
+        register_static_m(t);
+        register_static_n(t);
+        register_static_o(t);
+        register_static_p(t);
         return t;
     }();
     return table;

@@ -249,11 +249,11 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
             constexpr PassInfo pi = S::pass(P);
             constexpr int L0 = first_boundary_layout(S::R[0]);
             if constexpr (P == 0) {
-                run_pass<S::EMAX, S::R[P], decltype(refill), false, kPad16, L0>(
+                run_pass<S::EMAX, S::R[P], decltype(refill), false, kPad16, L0, true>(
                     a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut,
                     st + shift + m * (uint32_t)IC, refill);
             } else {
-                run_pass<S::EMAX, S::R[P], NoHook, false, P == 1 ? L0 : kPad16, kPad16>(
+                run_pass<S::EMAX, S::R[P], NoHook, false, P == 1 ? L0 : kPad16, kPad16, true>(
                     a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut);
             }
         });

@@ -112,10 +112,12 @@ int resident_pipe()
 }
 
 // REGFLOOR: see pipe_min_blocks (0 for the schedules tuned by hand).
-template <class S, int REGFLOOR = 0>
+// PREFERRED: the planner's choice for its length (see StaticEntry).
+template <class S, int REGFLOOR = 0, bool PREFERRED = false>
 StaticEntry static_entry()
 {
     StaticEntry e{};
+    e.preferred = PREFERRED;
     e.n = (uint32_t)S::N;
     e.emax = S::EMAX;
     e.T = (uint32_t)S::T;

@@ -133,7 +133,10 @@ __host__ __device__ constexpr int first_boundary_layout(int r0) { return (r0 % 2
 // first) and scatters to.
 // afterGather runs right after the barrier that ends the pass's reads.
 // rowIn / rowOut: this lane's transform in HBM (first / last pass).
-template <int EMAX, int R, class Hook = NoHook, bool RAW_FIRST = false, int LIN = kPad16, int LOUT = kPad16>
+// UNIT: the caller guarantees outElem == 1 (rows of contiguous values), so
+// the last pass's stores take constant offsets from rowOut.
+template <int EMAX, int R, class Hook = NoHook, bool RAW_FIRST = false, int LIN = kPad16, int LOUT = kPad16,
+          bool UNIT = false>
 FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, const bool last,
                       const uint32_t T, float2 (&v)[EMAX], float2* sm, uint32_t t, bool active,
                       const float2* rowIn, float2* rowOut, const float2* raw = nullptr,
@@ -151,8 +154,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
                 const uint32_t idx = j + (uint32_t)q * nb;
                 float2 z;
                 if (first && (RAW_FIRST || raw)) {
-                    z = raw[idx];
-                    if (a.conjIn) z = cconj(z);
+                    z = raw[idx];  // conjugated below, once for the whole gather
                 } else if (first && !RAW_FIRST) {
                     z = (active || a.staged) ? load_in(a, rowIn, idx, sm) : make_float2(0.f, 0.f);
                 } else {
@@ -162,6 +164,10 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
             });
         }
     });
+    // one uniform branch around the input conjugation of the inverse
+    if (first && (RAW_FIRST || raw) && a.conjIn) {
+        static_for<BMAX * R>([&](auto e) FFT_INL { v[e] = cconj(v[e]); });
+    }
 
     // twiddle and butterfly
     static_for<BMAX>([&](auto i) FFT_INL {
@@ -186,12 +192,18 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
     if (direct) {
         if (active) {
             float2* row = rowOut;
+            // conjugation and scale of the inverse in one uniform branch (the
+            // forward transform stores the butterfly outputs as they are)
+            if (a.conjOut || a.scale != 1.0f) {
+                static_for<BMAX * R>([&](auto e) FFT_INL { v[e] = finish(a, v[e]); });
+            }
             static_for<BMAX>([&](auto i) FFT_INL {
                 const uint32_t j = t + (uint32_t)i * T;
                 if (j < nb) {
                     static_for<R>([&](auto q) FFT_INL {
                         const uint32_t idx = j + (uint32_t)q * nb;
-                        row[(int64_t)idx * a.outElem] = finish(a, v[i * R + q]);
+                        if constexpr (UNIT) row[idx] = v[i * R + q];
+                        else row[(int64_t)idx * a.outElem] = v[i * R + q];
                     });
                 }
             });

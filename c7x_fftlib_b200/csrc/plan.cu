@@ -160,6 +160,18 @@ bool plan_engine(uint32_t n, EnginePlan* out)
         *out = e;
         return true;
     }
+    // a fixed-size schedule measured faster than the heuristic's pick
+    for (const StaticEntry& st : static_schedules()) {
+        if (st.n != n || !st.preferred) continue;
+        EnginePlan e;
+        e.n = n;
+        e.emax = st.emax;
+        e.T = st.T;
+        e.P = st.P;
+        for (int i = 0; i < st.P; ++i) e.R[i] = st.R[i];
+        *out = e;
+        return true;
+    }
     int seq[kMaxPasses];
     bool found = false;
     EnginePlan best;

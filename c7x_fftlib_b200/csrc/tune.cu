@@ -254,8 +254,8 @@ struct TuneBuffers {
 };
 
 // The batched FP32 launch choices worth timing for length n, best guess
-// first: the planner's top schedules (a fixed-size one among the first
-// eight always included); for a fixed-size schedule whose persistent
+// first: the planner's top three schedules and every other schedule of n
+// that has a fixed-size kernel; for a fixed-size schedule whose persistent
 // pipelined kernel takes this kind, that kernel with all resident CTAs, with
 // 1 and 2 per SM, and the one-tile-per-CTA kernel; for the others the
 // planner's transforms per CTA and half as many.
@@ -264,13 +264,18 @@ std::vector<BatchedChoice> batched_candidates(uint32_t n, int kind, int mode, in
     std::vector<EnginePlan> all = engine_candidates(n);
     std::vector<EnginePlan> scheds;
     for (size_t i = 0; i < all.size() && scheds.size() < 3; ++i) scheds.push_back(all[i]);
-    bool haveFixed = false;
-    for (const EnginePlan& e : scheds) haveFixed = haveFixed || static_max_threads(n, e.emax, e.T, e.P, e.R) != 0;
-    for (size_t i = scheds.size(); i < all.size() && i < 8 && !haveFixed; ++i)
-        if (static_max_threads(n, all[i].emax, all[i].T, all[i].P, all[i].R)) {
-            scheds.push_back(all[i]);
-            haveFixed = true;
-        }
+    for (const StaticEntry& st : static_schedules()) {
+        if (st.n != n) continue;
+        EnginePlan e;
+        e.n = n;
+        e.emax = st.emax;
+        e.T = st.T;
+        e.P = st.P;
+        for (int i = 0; i < st.P; ++i) e.R[i] = st.R[i];
+        bool seen = false;
+        for (const EnginePlan& s : scheds) seen = seen || same_schedule(s, e);
+        if (!seen) scheds.push_back(e);
+    }
     // the pipelined kernel's row conditions (launch_fft)
     const bool kindPipes = kind == TUNE_C2C || kind == TUNE_IFFT || (kind == TUNE_R2C && n % 2u == 0) ||
                            (kind == TUNE_C2R && mode == 0 && n % 2u == 0 && n >= 64u);
@@ -366,6 +371,14 @@ std::vector<uint32_t> i16_tg_candidates(uint32_t n)
     return out;
 }
 
+// $FFTLIB_B200_TUNE_VERBOSE set to a non-zero value: every timed candidate
+// is reported on stderr.
+bool tune_verbose()
+{
+    const char* v = getenv("FFTLIB_B200_TUNE_VERBOSE");
+    return v && *v && strcmp(v, "0") != 0;
+}
+
 } // namespace
 
 uint32_t tune_bucket(uint32_t batch)
@@ -443,7 +456,9 @@ bool tune_batched(const ComplexPlan* base, int kind, int mode, uint32_t batch, B
         std::istringstream is(val);
         BatchedChoice c;
         int np = 0;
-        if (decode(is, n, engine_candidates(n), &c.eng) && (is >> c.gridCap >> c.tileM >> np)) {
+        std::vector<EnginePlan> schedules;
+        for (const BatchedChoice& k : cands) schedules.push_back(k.eng);
+        if (decode(is, n, schedules, &c.eng) && (is >> c.gridCap >> c.tileM >> np)) {
             c.noPipe = np != 0;
             for (const BatchedChoice& k : cands)
                 if (same_choice(k, c)) {
@@ -469,9 +484,13 @@ bool tune_batched(const ComplexPlan* base, int kind, int mode, uint32_t batch, B
     k_fill<<<(unsigned)((count + 255) / 256), 256, 0, b.s>>>((float2*)x, count, 12345u);
     float best = 0.f;
     int bestIdx = -1;
+    const bool verbose = tune_verbose();
     for (size_t i = 0; i < cands.size(); ++i) {
         bool ok = false;
         const float ms = time_batched(base, cands[i], kind, mode, x, y, scratch, (uint32_t)tb, b.s, &ok);
+        if (verbose)
+            fprintf(stderr, "fftlib_b200 tune %s: %s -> %s\n", key.c_str(), encode(cands[i]).c_str(),
+                    ok ? (std::to_string(ms * 1e3f) + " us").c_str() : "failed");
         if (ok && (bestIdx < 0 || ms < best)) {
             best = ms;
             bestIdx = (int)i;
@@ -533,6 +552,7 @@ bool tune_i16(uint32_t n, uint32_t batch, I16Choice* out)
     k_fill_i16<<<(unsigned)((count + 255) / 256), 256, 0, b.s>>>(x, count, 12345u);
     float best = 0.f;
     int bestIdx = -1;
+    const bool verbose = tune_verbose();
     for (size_t i = 0; i < cands.size(); ++i) {
         bool ok = false;
         const I16Choice c = cands[i];
@@ -541,6 +561,9 @@ bool tune_i16(uint32_t n, uint32_t batch, I16Choice* out)
                 return launch_fft_i16((const int16_t*)x, (int16_t*)y, w, sh, n, (uint32_t)tb, b.s, c.tg, c.gridCap);
             },
             b.s, &ok);
+        if (verbose)
+            fprintf(stderr, "fftlib_b200 tune %s: %u %u -> %s\n", key.c_str(), c.tg, c.gridCap,
+                    ok ? (std::to_string(ms * 1e3f) + " us").c_str() : "failed");
         if (ok && (bestIdx < 0 || ms < best)) {
             best = ms;
             bestIdx = (int)i;

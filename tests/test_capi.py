@@ -272,7 +272,21 @@ def test_planner_covers_every_235_length_up_to_16384():
 
 
 def test_planner_headline_schedule():
-    assert F.describe_plan(4096) == "N=4096 E=16 T=256 radices=16x16x16 (fixed-size kernel)"
+    """N=4096: three radix-16 passes, 32 values per thread (128 threads), the
+    fixed-size schedule measured fastest on B200."""
+    assert F.describe_plan(4096) == "N=4096 E=32 T=128 radices=16x16x16 (fixed-size kernel)"
+
+
+def test_planner_prefers_the_measured_wide_schedules():
+    """Lengths whose 32-wide fixed-size schedule (fewer passes, radices up to
+    27 and 32) measured faster than the heuristic pick run that schedule."""
+    want = {250: "25x10", 576: "24x24", 864: "32x27", 2000: "25x10x8", 3645: "27x15x9", 4050: "27x15x10"}
+    for n, radices in want.items():
+        d = F.describe_plan(n)
+        assert d.startswith(f"N={n} E=32 ") and f"radices={radices} " in d, d
+    # and the heuristic keeps the lengths where the 16-wide schedule won
+    for n in (1024, 2048, 3000, 3600):
+        assert " E=16 " in F.describe_plan(n), F.describe_plan(n)
 
 
 def test_every_length_from_8_to_4096_has_a_fixed_size_kernel():
