@@ -13,6 +13,7 @@
 // FFTLIB_B200_MIXED_PERSISTENT_ONLY puts every group in the persistent
 // kernel. execPerSize() launches the persistent kernel once per distinct
 // length, for comparison.
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -241,11 +242,14 @@ cudaError_t enqueue_all(FFTLIB_b200_mixed* h, const float* x, float* y, cudaStre
     cudaError_t err = cudaEventRecord(h->fork, s);
     for (cudaStream_t b : h->branches)
         if (err == cudaSuccess) err = cudaStreamWaitEvent(b, h->fork, 0);
-    for (const auto& f : h->fixed) {
-        if (err != cudaSuccess) break;
+    // the groups of a branch touch disjoint parts of x and y, so each launch
+    // after a branch's first may start while its predecessor drains
+    for (size_t i = 0; i < h->fixed.size() && err == cudaSuccess; ++i) {
+        const auto& f = h->fixed[i];
+        const bool follows = i > 0 && h->fixed[i - 1].branch == f.branch;
         float2* in = const_cast<float2*>(reinterpret_cast<const float2*>(x)) + f.offset;
         err = run_c2c(f.plan, in, reinterpret_cast<float2*>(y) + f.offset, f.count, inverse, h->branches[f.branch],
-                      f.grid);
+                      f.grid, follows);
     }
     size_t br = h->fixedBranches;
     for (int cls = kMixedClasses - 1; cls >= 0 && err == cudaSuccess; --cls) {
@@ -383,15 +387,22 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
         uint32_t unused = 0;
         if (h->clsTiles[cls]) err = class_grid(cls, h->groupStage, h->device, &unused);
     }
-    // Branches: the device runs kernels of at most kMaxBranches streams side
-    // by side (its default number of hardware work queues), so the fixed
-    // groups are packed into that many branches, largest work first onto the
-    // least loaded; each class with tiles takes a branch of its own. Every
-    // branch gets the fraction of the device (SMs times a kernel's CTAs per
-    // SM) that its work is of the batch's and runs its launches back to back
-    // on it; the runtime-radix passes of the persistent kernel count twice
-    // per byte.
-    constexpr size_t kMaxBranches = 8;
+    // Branches: the fixed groups are packed into kMaxBranches branches,
+    // largest work first onto the least loaded; each class with tiles takes a
+    // branch of its own. Every branch gets the fraction of the device (SMs
+    // times a kernel's CTAs per SM) that its work is of the batch's and runs
+    // its launches back to back on it, each launch after the first starting
+    // while its predecessor drains (programmatic dependent launch); the
+    // runtime-radix passes of the persistent kernel count twice per byte.
+    // One branch measured best on B200 (the launches then stream through the
+    // device one after another: 0.093 ms for the 20,000-transform set against
+    // 0.097-0.099 ms on 2 to 8 branches); $FFTLIB_B200_MIXED_BRANCHES (1-8)
+    // sets another count (at most 8: the device's hardware work queues).
+    size_t kMaxBranches = 1;
+    if (const char* v = getenv("FFTLIB_B200_MIXED_BRANCHES")) {
+        const long b = strtol(v, nullptr, 10);
+        if (b >= 1 && b <= 8) kMaxBranches = (size_t)b;
+    }
     size_t classBranches = 0;
     for (int cls = 0; cls < kMixedClasses; ++cls) classBranches += h->clsTiles[cls] ? 1 : 0;
     size_t fixedBranches = 0;

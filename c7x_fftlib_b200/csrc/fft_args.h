@@ -95,9 +95,13 @@ struct FftArgs {
     // host-side launch hints, read by no kernel: at most gridCap CTAs for the
     // persistent kernels (0: as many as are resident); noPipe != 0 runs a
     // fixed-size schedule's one-tile-per-CTA kernel instead of its persistent
-    // pipelined one
+    // pipelined one; overlapPrev != 0 lets the persistent pipelined kernel
+    // start while the previous kernel of its stream is still running
+    // (programmatic dependent launch: only for launches whose inputs and
+    // outputs no earlier kernel of the stream touches)
     uint32_t gridCap;
     uint32_t noPipe;
+    uint32_t overlapPrev;
 };
 
 // Transforms one CTA computes at a time (its threads: T of them each).

@@ -173,6 +173,9 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
     const uint32_t t = tid - m * (uint32_t)S::T;
     const uint32_t tiles = (a.batch + (uint32_t)M - 1u) / (uint32_t)M;
     const uint32_t G = gridDim.x;
+    // a kernel launched after this one with programmatic stream
+    // serialization may start now (a no-op for every other launch)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
     // a tile's inputs are count * IC contiguous complex values (IC = the
     // input row length: N, or N + 1 bins for c2r); see tile_span

@@ -90,6 +90,19 @@ cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
     const uint32_t tiles = (a.batch + (uint32_t)M - 1u) / (uint32_t)M;
     uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)std::max(1, resident * sms));
     if (a.gridCap) grid = std::max(1u, std::min(grid, a.gridCap));
+    if (a.overlapPrev) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3((unsigned)(S::T * M));
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, k_fft_pipe<S, STAGES, REGFLOOR>, a);
+    }
     k_fft_pipe<S, STAGES, REGFLOOR><<<grid, S::T * M, smem, s>>>(a);
     return cudaGetLastError();
 }

@@ -643,7 +643,7 @@ void apply_choice(FftArgs& a, const ComplexPlan* p)
 } // namespace
 
 cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse, cudaStream_t s,
-                    uint32_t gridCap)
+                    uint32_t gridCap, bool overlapPrev)
 {
     if (batch == 0) return cudaSuccess;
     if (p->multiPass) return run_global(p, in, out, batch, inverse, s);
@@ -662,6 +662,7 @@ cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batc
     finalize_launch(a, p->eng, true, true);
     apply_choice(a, p);
     if (gridCap) a.gridCap = gridCap;
+    a.overlapPrev = overlapPrev ? 1u : 0u;
     return launch_fft(a, p->eng.emax, s);
 }
 

@@ -135,8 +135,10 @@ FftArgs engine_args(const EnginePlan& e, const float2* tw);
 // Launch sequences (device pointers, stream s, no synchronization).
 // run_c2c may overwrite `in` (work buffer of the passes when G > 2).
 // gridCap: at most that many CTAs for the persistent kernels (0: all resident).
+// overlapPrev: the launch may start while the stream's previous kernel runs
+// (see FftArgs::overlapPrev; the caller guarantees that they are independent).
 cudaError_t run_c2c(const ComplexPlan* p, float2* in, float2* out, uint32_t batch, bool inverse,
-                    cudaStream_t s, uint32_t gridCap = 0);
+                    cudaStream_t s, uint32_t gridCap = 0, bool overlapPrev = false);
 // h = p->n = numPoints / 2; x: batch x 2h reals; scratch: batch x h complex
 // (needed only for global passes); y: batch x (h+1) or x 2h bins.
 cudaError_t run_r2c(const ComplexPlan* p, float* x, float2* scratch, float2* y, uint32_t batch, int outmode,
