@@ -4,12 +4,13 @@
 // create() groups the transforms by length. A group whose transforms lie
 // back to back and whose length has a persistent pipelined fixed-size kernel
 // (every 2^a 3^b 5^c length from 8 to 4096) is a "fixed group": it runs that
-// kernel with a grid proportional to its share of the batch, so that all
-// groups run side by side on one partition of the GPU each and finish
-// together. Every other group gets a runtime-radix schedule (heuristic, or
-// timed by the autotuner) in the persistent mixed kernel (fft_mixed.cu),
-// which walks a device-resident tile table ordered by cost. exec() replays a
-// CUDA graph with all of these launches on parallel branches;
+// kernel, the fixed groups' launches back to back, each one starting while its
+// predecessor drains (programmatic dependent launch), or spread over up to 8
+// graph branches with grids proportional to their shares of the batch. Every
+// other group gets a runtime-radix schedule (heuristic, or timed by the
+// autotuner) in the persistent mixed kernel (fft_mixed.cu), which walks a
+// device-resident tile table ordered by cost. exec() replays a CUDA graph of
+// these launches, the persistent kernel's on a branch of its own;
 // FFTLIB_B200_MIXED_PERSISTENT_ONLY puts every group in the persistent
 // kernel. execPerSize() launches the persistent kernel once per distinct
 // length, for comparison.
@@ -63,7 +64,7 @@ struct FFTLIB_b200_mixed {
     std::vector<Fixed> fixed;           // ordered by branch
     uint64_t fixedPoints = 0;
     uint32_t fixedBranches = 0;
-    // one graph branch per fixed group and per class with tiles
+    // the fixed groups' graph branches, then one per class with tiles
     std::vector<cudaStream_t> branches;
     std::vector<cudaEvent_t> joins;
     cudaStream_t capture = nullptr;

@@ -100,9 +100,11 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc(FFTLIB_F3
  * (2^a 3^b 5^c, at most 4096) and occupies 2 * numPoints[i] floats of pX and
  * of pY, the transforms packed back to back in the order given. create()
  * groups the transforms by length. A group whose transforms lie back to back
- * runs its length's persistent fixed-size kernel on a grid proportional to
- * its share of the batch, every group on its own graph branch, so that the
- * groups run side by side and finish together; the other groups (or all,
+ * runs its length's persistent fixed-size kernel; these launches follow one
+ * another, each starting while the previous one drains (programmatic
+ * dependent launch; $FFTLIB_B200_MIXED_BRANCHES = 2..8 spreads them over that
+ * many parallel graph branches, each on a share of the GPU proportional to
+ * its work); the other groups (or all,
  * with FFTLIB_B200_MIXED_PERSISTENT_ONLY) run in one persistent kernel over a
  * device-resident tile table, with radix schedules picked by the planner or
  * timed by the autotuner (FFTLIB_B200_MIXED_AUTOTUNE, or $FFTLIB_B200_AUTOTUNE
