@@ -29,14 +29,19 @@ struct StaticEntry {
     int R[kMaxPasses];
     int maxThreads;
     cudaError_t (*launch)(const FftArgs&, cudaStream_t);
-    // persistent TMA-pipelined variant (M == 1, contiguous 16-byte aligned
-    // rows, complex in and out), or null
-    cudaError_t (*launchPipelined)(const FftArgs&, cudaStream_t);
-    // CTAs per SM of that variant on the current device, or null
-    int (*residentPipelined)();
+    // persistent bulk-copy pipelined variants (contiguous 16-byte aligned
+    // rows), one per transform kind (indexed by IO_C2C, IO_R2C_SPLIT,
+    // IO_C2R_SPLIT), or null
+    cudaError_t (*launchPipelined[3])(const FftArgs&, cudaStream_t);
+    // CTAs per SM of each variant on the current device, or null
+    int (*residentPipelined[3])();
     // measured on B200 to beat the planner's heuristic schedule for this
     // length: plan_engine returns it instead
     bool preferred;
+    // the pipelined variant splits c2r inputs in its first pass / r2c outputs
+    // in its last pass in registers (two butterflies per thread, T = N/R/2)
+    bool mirrorFirst;
+    bool mirrorLast;
 };
 const std::vector<StaticEntry>& static_schedules();
 // maxThreads of the compiled fixed-size kernel for this schedule, or 0.

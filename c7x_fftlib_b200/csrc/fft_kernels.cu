@@ -122,7 +122,7 @@ int static_pipelined_resident(uint32_t n, int emax, uint32_t T, int P, const int
         if (e.n != n || e.emax != emax || e.T != T || e.P != P) continue;
         bool same = true;
         for (int p = 0; p < P; ++p) same = same && (e.R[p] == R[p]);
-        if (same) return e.residentPipelined ? e.residentPipelined() : 0;
+        if (same) return e.residentPipelined[IO_C2C] ? e.residentPipelined[IO_C2C]() : 0;
     }
     return 0;
 }
@@ -137,13 +137,13 @@ cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
         // the stage holds beside its padded exchange layout for N >= 64)
         const bool rowsOk = ((a.ioMode == IO_C2C || a.ioMode == IO_R2C_SPLIT) && a.inBatch == (int64_t)a.N) ||
                             (a.ioMode == IO_C2R_SPLIT && !a.realMode && a.inBatch == (int64_t)a.N + 1 && a.N >= 64u);
-        const bool pipelinable = st->launchPipelined && !a.noPipe && a.err && rowsOk && !a.batchMinor &&
-                                 !a.perCh && a.inElem == 1 && a.outElem == 1 && ((uintptr_t)a.in & 15u) == 0 &&
-                                 ((a.N % 2u) == 0 || a.ioMode == IO_C2C);
+        const auto pipe = a.ioMode >= 0 && a.ioMode <= IO_C2R_SPLIT ? st->launchPipelined[a.ioMode] : nullptr;
+        const bool pipelinable = pipe && !a.noPipe && a.err && rowsOk && !a.batchMinor && !a.perCh &&
+                                 a.inElem == 1 && a.outElem == 1 && ((uintptr_t)a.in & 15u) == 0;
         if (pipelinable) {
             FftArgs b = a;
             b.staged = 0;
-            return st->launchPipelined(b, s);
+            return pipe(b, s);
         }
         return st->launch(a, s);
     }

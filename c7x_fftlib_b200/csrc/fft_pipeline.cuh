@@ -116,14 +116,12 @@ __host__ __device__ constexpr int pipe_min_blocks(uint32_t n, int threads, int s
     return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
 
-// c2r split of bin x against the mirrored bin xm: ((x + y) + i conj(w) (x - y)) / 2,
-// y = conj(xm).
-FFT_DEV float2 c2r_z(float2 x, float2 xm, float2 w)
+// Whether pass p of schedule S can run mirrored (two butterflies per thread,
+// T = N / R / 2; see run_pass).
+template <class S>
+__host__ __device__ constexpr bool pipe_mirrorable(int p)
 {
-    const float2 y = cconj(xm);
-    const float2 sum = cadd(x, y), d = csub(x, y);
-    const float2 icw = make_float2(w.y, w.x);  // i * conj(w)
-    return cscale(cadd(sum, cmul(icw, d)), 0.5f);
+    return S::EMAX / S::R[p] == 2 && 2 * S::T == S::N / S::R[p];
 }
 
 // Input span of a tile of m transforms with input rows of ic complex values:
@@ -155,8 +153,10 @@ FFT_DEV TileSpan tile_span(uint32_t tile, uint32_t m, uint32_t batch, uint64_t i
 // transform m reads its input from there and (after the CTA-wide barrier
 // inside the pass, when every input has been read) writes its outputs in the
 // padded layout at m * SL, and so on; the stage is refilled once the first
-// pass has read it.
-template <class S, int STAGES, int M>
+// pass has read it. IO (IO_C2C, IO_R2C_SPLIT or IO_C2R_SPLIT) is the one
+// transform kind the instantiation serves, so that none of them carries the
+// others' code (a.ioMode equals it).
+template <class S, int STAGES, int M, int IO>
 FFT_DEV void fft_pipeline(const FftArgs& a)
 {
     static_assert(S::P >= 2, "the pipelined kernel needs at least two passes");
@@ -229,7 +229,11 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
             }
         };
         float2* rowOut = a.out + (size_t)gidx * (size_t)a.outBatch;
-        if (a.ioMode == IO_C2R_SPLIT) {
+        // a schedule whose first (last) pass can run mirrored splits the
+        // c2r input (r2c output) there, in registers
+        constexpr bool kC2RMirror = IO == IO_C2R_SPLIT && pipe_mirrorable<S>(0);
+        constexpr bool kR2CMirror = IO == IO_R2C_SPLIT && pipe_mirrorable<S>(S::P - 1);
+        if constexpr (IO == IO_C2R_SPLIT && !kC2RMirror) {
             // c2r (inMode 0): turn the h + 1 bins into the h-point input Z in
             // place, Z[i] = ((X[i] + y) + i conj(W) (X[i] - y)) / 2 with
             // y = conj(X[h - i]); each thread owns the pair (i, h - i)
@@ -240,9 +244,10 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
                     const float2 xi = row[i], xp = row[ip];
                     // W_{2h}^(h-i) = -conj(W_{2h}^i): one table load serves the
                     // pair, with the accuracy of the table's own entry
-                    const float2 w = __ldg(&a.twSplit[i]);
-                    row[i] = c2r_z(xi, xp, w);
-                    if (i != 0u && ip != i) row[ip] = c2r_z(xp, xi, make_float2(-w.x, w.y));
+                    float2 zi, zp;
+                    c2r_split_pair(xi, xp, __ldg(&a.twSplit[i]), zi, zp);
+                    row[i] = zi;
+                    if (i != 0u && ip != i) row[ip] = zp;
                 }
             }
             __syncthreads();
@@ -251,19 +256,33 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
             constexpr int P = decltype(p)::value;
             constexpr PassInfo pi = S::pass(P);
             constexpr int L0 = first_boundary_layout(S::R[0]);
+            const float2* raw = st + shift + m * (uint32_t)IC;
             if constexpr (P == 0) {
-                run_pass<S::EMAX, S::R[P], decltype(refill), false, kPad16, L0, true>(
-                    a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut,
-                    st + shift + m * (uint32_t)IC, refill);
+                if constexpr (kC2RMirror)
+                    run_pass<S::EMAX, S::R[P], decltype(refill), false, kPad16, L0, true, kMirrorC2R>(
+                        a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut, raw,
+                        refill);
+                else
+                    run_pass<S::EMAX, S::R[P], decltype(refill), false, kPad16, L0, true>(
+                        a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut, raw,
+                        refill);
+            } else if constexpr (P + 1 == S::P) {
+                if constexpr (kR2CMirror)
+                    run_pass<S::EMAX, S::R[P], NoHook, false, P == 1 ? L0 : kPad16, kPad16, true, kMirrorR2C>(
+                        a, pi, false, true, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut);
+                else
+                    run_pass<S::EMAX, S::R[P], NoHook, false, P == 1 ? L0 : kPad16, kPad16, true>(
+                        a, pi, false, true, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut);
             } else {
                 run_pass<S::EMAX, S::R[P], NoHook, false, P == 1 ? L0 : kPad16, kPad16, true>(
-                    a, pi, false, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut);
+                    a, pi, false, false, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut);
             }
         });
-        // r2c: the last pass left Z in natural order in the padded layout;
-        // the split writes the h + 1 (or 2h) bins. The stage is refilled only
-        // after the next iteration's first barrier, when this has finished.
-        if (a.ioMode == IO_R2C_SPLIT) r2c_epilogue(a, st + m * SL, t, rowOut, active);
+        // r2c without the mirrored last pass: that pass left Z in natural
+        // order in the padded layout; the split writes the h + 1 (or 2h)
+        // bins. The stage is refilled only after the next iteration's first
+        // barrier, when this has finished.
+        if constexpr (IO == IO_R2C_SPLIT && !kR2CMirror) r2c_epilogue(a, st + m * SL, t, rowOut, active);
     }
 
     if (s_fail && tid == 0) {

@@ -45,21 +45,22 @@ cudaError_t launch_static(const FftArgs& a, cudaStream_t s)
     return cudaGetLastError();
 }
 
-template <class S, int STAGES, int REGFLOOR = 0>
+template <class S, int STAGES, int REGFLOOR, int IO>
 __global__ void __launch_bounds__(S::T * pipe_tile(S::T),
                                   pipe_min_blocks(S::N, S::T * pipe_tile(S::T), STAGES, pipe_tile(S::T), REGFLOOR))
     k_fft_pipe(const __grid_constant__ FftArgs a)
 {
-    fft_pipeline<S, STAGES, pipe_tile(S::T)>(a);
+    fft_pipeline<S, STAGES, pipe_tile(S::T), IO>(a);
 }
 
-// Persistent pipelined launch (pipe_tile(T) transforms per tile): as many
-// CTAs as are resident on the device.
-template <class S, int STAGES, int REGFLOOR = 0>
+// Persistent pipelined launch (pipe_tile(T) transforms per tile) of the
+// instantiation for transform kind IO: as many CTAs as are resident on the
+// device, at most a.gridCap.
+template <class S, int STAGES, int REGFLOOR, int IO>
 cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
 {
     constexpr int M = pipe_tile(S::T);
-    if (a.T != (uint32_t)S::T) return cudaErrorInvalidConfiguration;
+    if (a.T != (uint32_t)S::T || a.ioMode != IO) return cudaErrorInvalidConfiguration;
     const size_t smem = pipe_smem_bytes((uint32_t)S::N, STAGES, M);
     struct Cfg {
         int blocks = -1;
@@ -75,11 +76,11 @@ cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
         std::lock_guard<std::mutex> lock(mu);
         Cfg& c = cfg[dev & 63];
         if (c.blocks < 0) {
-            e = cudaFuncSetAttribute(k_fft_pipe<S, STAGES, REGFLOOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem);
+            e = cudaFuncSetAttribute(k_fft_pipe<S, STAGES, REGFLOOR, IO>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.blocks, k_fft_pipe<S, STAGES, REGFLOOR>, S::T * M,
-                                                              smem);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c.blocks, k_fft_pipe<S, STAGES, REGFLOOR, IO>,
+                                                              S::T * M, smem);
             if (e != cudaSuccess) return e;
             e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev);
             if (e != cudaSuccess) return e;
@@ -91,33 +92,33 @@ cudaError_t launch_pipe(const FftArgs& a, cudaStream_t s)
     uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)std::max(1, resident * sms));
     if (a.gridCap) grid = std::max(1u, std::min(grid, a.gridCap));
     if (a.overlapPrev) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(grid);
-        cfg.blockDim = dim3((unsigned)(S::T * M));
-        cfg.dynamicSmemBytes = smem;
-        cfg.stream = s;
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(grid);
+        lc.blockDim = dim3((unsigned)(S::T * M));
+        lc.dynamicSmemBytes = smem;
+        lc.stream = s;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
         attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, k_fft_pipe<S, STAGES, REGFLOOR>, a);
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        return cudaLaunchKernelEx(&lc, k_fft_pipe<S, STAGES, REGFLOOR, IO>, a);
     }
-    k_fft_pipe<S, STAGES, REGFLOOR><<<grid, S::T * M, smem, s>>>(a);
+    k_fft_pipe<S, STAGES, REGFLOOR, IO><<<grid, S::T * M, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 // CTAs per SM of the persistent pipelined kernel.
-template <class S, int STAGES, int REGFLOOR>
+template <class S, int STAGES, int REGFLOOR, int IO>
 int resident_pipe()
 {
     constexpr int M = pipe_tile(S::T);
     const size_t smem = pipe_smem_bytes((uint32_t)S::N, STAGES, M);
     int blocks = 0;
-    if (cudaFuncSetAttribute(k_fft_pipe<S, STAGES, REGFLOOR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_fft_pipe<S, STAGES, REGFLOOR, IO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_fft_pipe<S, STAGES, REGFLOOR>, S::T * M, smem) !=
-            cudaSuccess) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_fft_pipe<S, STAGES, REGFLOOR, IO>, S::T * M,
+                                                      smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -141,13 +142,22 @@ StaticEntry static_entry()
     e.launch = &launch_static<S, maxt>;
     // the stage ring and exchange buffer must fit one CTA's shared memory
     // (odd lengths too: a tile's copy starts at the even element at or below
-    // its first value, see tile_span)
+    // its first value, see tile_span); one instantiation per transform kind:
+    // c2c for every length, r2c for even ones, c2r for even ones from 64 up
+    // (whose stage holds the N + 1 bins beside the exchange layout)
     if constexpr (S::P >= 2 && pipe_smem_bytes(S::N, 2, pipe_tile(S::T)) <= 227u * 1024u) {
-        e.launchPipelined = &launch_pipe<S, 2, REGFLOOR>;
-        e.residentPipelined = &resident_pipe<S, 2, REGFLOOR>;
-    } else {
-        e.launchPipelined = nullptr;
-        e.residentPipelined = nullptr;
+        e.launchPipelined[IO_C2C] = &launch_pipe<S, 2, REGFLOOR, IO_C2C>;
+        e.residentPipelined[IO_C2C] = &resident_pipe<S, 2, REGFLOOR, IO_C2C>;
+        if constexpr (S::N % 2 == 0) {
+            e.launchPipelined[IO_R2C_SPLIT] = &launch_pipe<S, 2, REGFLOOR, IO_R2C_SPLIT>;
+            e.residentPipelined[IO_R2C_SPLIT] = &resident_pipe<S, 2, REGFLOOR, IO_R2C_SPLIT>;
+            e.mirrorLast = pipe_mirrorable<S>(S::P - 1);
+        }
+        if constexpr (S::N % 2 == 0 && S::N >= 64) {
+            e.launchPipelined[IO_C2R_SPLIT] = &launch_pipe<S, 2, REGFLOOR, IO_C2R_SPLIT>;
+            e.residentPipelined[IO_C2R_SPLIT] = &resident_pipe<S, 2, REGFLOOR, IO_C2R_SPLIT>;
+            e.mirrorFirst = pipe_mirrorable<S>(0);
+        }
     }
     return e;
 }

@@ -135,19 +135,41 @@ __host__ __device__ constexpr int first_boundary_layout(int r0) { return (r0 % 2
 // rowIn / rowOut: this lane's transform in HBM (first / last pass).
 // UNIT: the caller guarantees outElem == 1 (rows of contiguous values), so
 // the last pass's stores take constant offsets from rowOut.
+// MIRROR (kMirrorC2R on a first pass, kMirrorR2C on a last pass; the caller
+// guarantees two butterflies per thread and T = nb / 2): thread t takes the
+// butterflies t and nb - t (thread 0: 0 and nb / 2), whose values are the
+// mirror images h - i of each other, so the real-signal split runs in
+// registers: kMirrorC2R turns the raw h + 1 bins into the half-length input
+// Z before the butterflies, kMirrorR2C writes the h + 1 (or 2h) bins from the
+// butterfly outputs instead of scattering them.
+constexpr int kMirrorNone = 0, kMirrorC2R = 1, kMirrorR2C = 2;
+
+FFT_DEV uint32_t mirror_j(uint32_t t, int i, uint32_t nb) { return i == 0 ? t : (t == 0 ? nb / 2u : nb - t); }
+
+FFT_DEV float2 r2c_split(float2 z, float2 zp, float2 w);
+FFT_DEV void r2c_split_pair(float2 z, float2 zm, float2 w, float2& y, float2& ym);
+FFT_DEV float2 c2r_split(float2 x, float2 xm, float2 w);
+FFT_DEV void c2r_split_pair(float2 x, float2 xm, float2 w, float2& z, float2& zm);
+template <int R>
+FFT_DEV void c2r_mirror_split(const FftArgs& a, float2* v, uint32_t t, uint32_t nb, const float2* raw);
+template <int R>
+FFT_DEV void r2c_mirror_store(const FftArgs& a, const float2* v, uint32_t t, uint32_t nb, float2* row);
+
 template <int EMAX, int R, class Hook = NoHook, bool RAW_FIRST = false, int LIN = kPad16, int LOUT = kPad16,
-          bool UNIT = false>
+          bool UNIT = false, int MIRROR = kMirrorNone>
 FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, const bool last,
                       const uint32_t T, float2 (&v)[EMAX], float2* sm, uint32_t t, bool active,
                       const float2* rowIn, float2* rowOut, const float2* raw = nullptr,
                       Hook afterGather = Hook())
 {
     constexpr int BMAX = EMAX / R;
+    static_assert(MIRROR == kMirrorNone || BMAX == 2, "the mirrored passes hold two butterflies per thread");
     const uint32_t nb = pi.stride; // butterflies in this pass: N / R
+    auto bfly = [&](int i) FFT_INL { return MIRROR ? mirror_j(t, i, nb) : t + (uint32_t)i * T; };
 
     // gather
     static_for<BMAX>([&](auto i) FFT_INL {
-        const uint32_t j = t + (uint32_t)i * T;
+        const uint32_t j = bfly(i);
         if (j < nb) {
             const uint32_t sj = lay<LIN>(j);
             static_for<R>([&](auto q) FFT_INL {
@@ -164,6 +186,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
             });
         }
     });
+    if constexpr (MIRROR == kMirrorC2R) c2r_mirror_split<R>(a, v, t, nb, raw);
     // one uniform branch around the input conjugation of the inverse
     if (first && (RAW_FIRST || raw) && a.conjIn) {
         static_for<BMAX * R>([&](auto e) FFT_INL { v[e] = cconj(v[e]); });
@@ -171,7 +194,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
 
     // twiddle and butterfly
     static_for<BMAX>([&](auto i) FFT_INL {
-        const uint32_t j = t + (uint32_t)i * T;
+        const uint32_t j = bfly(i);
         if (j < nb) {
             if (!first) {
                 const uint32_t g = fastdiv(j, pi.Ns, pi.nsMagic);
@@ -187,6 +210,11 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
         }
     });
 
+    if constexpr (MIRROR == kMirrorR2C) {
+        if (active) r2c_mirror_store<R>(a, v, t, nb, rowOut);
+        return;
+    }
+
     // scatter
     const bool direct = last && !a.staged && a.ioMode != IO_R2C_SPLIT;
     if (direct) {
@@ -198,7 +226,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
                 static_for<BMAX * R>([&](auto e) FFT_INL { v[e] = finish(a, v[e]); });
             }
             static_for<BMAX>([&](auto i) FFT_INL {
-                const uint32_t j = t + (uint32_t)i * T;
+                const uint32_t j = bfly(i);
                 if (j < nb) {
                     static_for<R>([&](auto q) FFT_INL {
                         const uint32_t idx = j + (uint32_t)q * nb;
@@ -215,7 +243,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
         afterGather();
     }
     static_for<BMAX>([&](auto i) FFT_INL {
-        const uint32_t j = t + (uint32_t)i * T;
+        const uint32_t j = bfly(i);
         if (j < nb) {
             const uint32_t g = fastdiv(j, pi.Ns, pi.nsMagic);
             const uint32_t k = j - g * pi.Ns;
@@ -243,6 +271,119 @@ FFT_DEV float2 r2c_split(float2 z, float2 zp, float2 w)
     return cadd(e, cmul(miw, o));
 }
 
+// Both bins of the pair (i, h - i) at once: y = e + q and ym = conj(e - q),
+// q = -i w o, the mirrored bin's twiddle W_{2h}^(h-i) = -conj(w) folded into
+// the conjugate (16 floating-point operations for the two).
+FFT_DEV void r2c_split_pair(float2 z, float2 zm, float2 w, float2& y, float2& ym)
+{
+    const float2 e = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+    const float2 o = make_float2(0.5f * (z.x - zm.x), 0.5f * (z.y + zm.y));
+    const float2 q = make_float2(fmaf(w.x, o.y, w.y * o.x), fmaf(w.y, o.y, -w.x * o.x));
+    y = make_float2(e.x + q.x, e.y + q.y);
+    ym = make_float2(e.x - q.x, q.y - e.y);
+}
+
+// Z[i] = ((X[i] + y) + i conj(W) (X[i] - y)) / 2, y = conj(X[h - i]), W = W_{2h}^i:
+// the reference's X[i] A'[i] + conj(X[h - i]) B'[i].
+FFT_DEV float2 c2r_split(float2 x, float2 xm, float2 w)
+{
+    const float2 y = cconj(xm);
+    const float2 sum = cadd(x, y), d = csub(x, y);
+    const float2 icw = make_float2(w.y, w.x);  // i * conj(w)
+    return cscale(cadd(sum, cmul(icw, d)), 0.5f);
+}
+
+// Both Z of the pair (i, h - i): z = (s + p) / 2 and zm = conj(s - p) / 2 with
+// s = x + conj(xm), p = i conj(w) (x - conj(xm)).
+FFT_DEV void c2r_split_pair(float2 x, float2 xm, float2 w, float2& z, float2& zm)
+{
+    const float2 s = make_float2(x.x + xm.x, x.y - xm.y);
+    const float2 d = make_float2(x.x - xm.x, x.y + xm.y);
+    const float2 p = make_float2(fmaf(w.y, d.x, -w.x * d.y), fmaf(w.y, d.y, w.x * d.x));
+    z = make_float2(0.5f * (s.x + p.x), 0.5f * (s.y + p.y));
+    zm = make_float2(0.5f * (s.x - p.x), 0.5f * (p.y - s.y));
+}
+
+// c2r (inMode 0) split of the first pass's raw bins in registers. v[q] is
+// X[j0 + q nb], v[R + q] is X[j1 + q nb] with (j0, j1) = (t, nb - t), or
+// (0, nb / 2) for thread 0; the mirror h - i of j0 + q nb is j1 + (R-1-q) nb,
+// of q nb (thread 0) (R - q) nb, and of bin 0 the Nyquist bin X[h] (raw[h]).
+// W_{2h}^(h-i) = -conj(W_{2h}^i): one table load serves each pair.
+template <int R>
+FFT_DEV void c2r_mirror_split(const FftArgs& a, float2* v, uint32_t t, uint32_t nb, const float2* raw)
+{
+    if (t != 0u) {
+        static_for<R>([&](auto q) FFT_INL {
+            constexpr int qq = decltype(q)::value;
+            const float2 w = __ldg(&a.twSplit[t + (uint32_t)qq * nb]);
+            c2r_split_pair(v[qq], v[2 * R - 1 - qq], w, v[qq], v[2 * R - 1 - qq]);
+        });
+        return;
+    }
+    const float2 xh = raw[a.N];
+    v[0] = c2r_split(v[0], xh, __ldg(&a.twSplit[0]));
+    static_for<R / 2>([&](auto q1) FFT_INL {
+        constexpr int q = decltype(q1)::value + 1;  // pairs (q, R - q), q = R/2 alone
+        const float2 w = __ldg(&a.twSplit[(uint32_t)q * nb]);
+        if constexpr (q != R - q) c2r_split_pair(v[q], v[R - q], w, v[q], v[R - q]);
+        else v[q] = c2r_split(v[q], v[q], w);
+    });
+    static_for<R / 2>([&](auto q1) FFT_INL {
+        constexpr int q = decltype(q1)::value;  // pairs (q, R-1-q) of butterfly nb / 2
+        const float2 w = __ldg(&a.twSplit[nb / 2u + (uint32_t)q * nb]);
+        c2r_split_pair(v[R + q], v[2 * R - 1 - q], w, v[R + q], v[2 * R - 1 - q]);
+    });
+}
+
+// r2c split of the last pass's outputs in registers (the pairing of
+// c2r_mirror_split), written as bins i and h - i of row (and, with
+// realMode, their conjugates at 2h - i).
+template <int R>
+FFT_DEV void r2c_mirror_store(const FftArgs& a, const float2* v, uint32_t t, uint32_t nb, float2* row)
+{
+    const uint32_t h = a.N;
+    const bool full = a.realMode != 0;
+    auto put = [&](uint32_t i, float2 y) FFT_INL {
+        row[i] = y;
+        if (full) row[2u * h - i] = cconj(y);
+    };
+    if (t != 0u) {
+        static_for<R>([&](auto q) FFT_INL {
+            constexpr int qq = decltype(q)::value;
+            const uint32_t i = t + (uint32_t)qq * nb;
+            float2 y, ym;
+            r2c_split_pair(v[qq], v[2 * R - 1 - qq], __ldg(&a.twSplit[i]), y, ym);
+            put(i, y);
+            put(h - i, ym);
+        });
+        return;
+    }
+    const float2 z0 = v[0];
+    row[0] = make_float2(z0.x + z0.y, 0.f);
+    row[h] = make_float2(z0.x - z0.y, 0.f);  // Nyquist bin
+    static_for<R / 2>([&](auto q1) FFT_INL {
+        constexpr int q = decltype(q1)::value + 1;
+        const uint32_t i = (uint32_t)q * nb;
+        const float2 w = __ldg(&a.twSplit[i]);
+        if constexpr (q != R - q) {
+            float2 y, ym;
+            r2c_split_pair(v[q], v[R - q], w, y, ym);
+            put(i, y);
+            put(h - i, ym);
+        } else {
+            put(i, r2c_split(v[q], v[q], w));
+        }
+    });
+    static_for<R / 2>([&](auto q1) FFT_INL {
+        constexpr int q = decltype(q1)::value;
+        const uint32_t i = nb / 2u + (uint32_t)q * nb;
+        float2 y, ym;
+        r2c_split_pair(v[R + q], v[2 * R - 1 - q], __ldg(&a.twSplit[i]), y, ym);
+        put(i, y);
+        put(h - i, ym);
+    });
+}
+
 FFT_DEV void r2c_epilogue(const FftArgs& a, const float2* sm, uint32_t t, float2* row, bool active)
 {
     if (!active) return;
@@ -259,11 +400,11 @@ FFT_DEV void r2c_epilogue(const FftArgs& a, const float2* sm, uint32_t t, float2
         // W_{2h}^(h-i) = -conj(W_{2h}^i): one table load serves the pair,
         // with the accuracy of the table's own entry (FP64 rounded to FP32)
         const float2 w = __ldg(&a.twSplit[i]);
-        const float2 yi = r2c_split(zi, zp, w);
+        float2 yi, yp;
+        r2c_split_pair(zi, zp, w, yi, yp);
         row[i] = yi;
         if (a.realMode) row[2 * h - i] = cconj(yi);
         if (ip != i) {
-            const float2 yp = r2c_split(zp, zi, make_float2(-w.x, w.y));
             row[ip] = yp;
             if (a.realMode) row[2 * h - ip] = cconj(yp);
         }

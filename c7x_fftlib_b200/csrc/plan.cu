@@ -433,7 +433,8 @@ ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err)
 
 namespace {
 
-// Tuned plans, per (device, length and choice).
+// Tuned plans and the real kinds' own schedules, per (device, length and
+// choice).
 std::map<std::pair<int, std::string>, ComplexPlan*> g_tuned_plans;
 
 std::string choice_key(uint32_t n, const BatchedChoice& c)
@@ -455,14 +456,55 @@ void free_plan(ComplexPlan* p)
 
 } // namespace
 
+namespace {
+
+const StaticEntry* static_of(const EnginePlan& e)
+{
+    for (const StaticEntry& st : static_schedules()) {
+        if (st.n != e.n || st.emax != e.emax || st.T != e.T || st.P != e.P) continue;
+        bool same = true;
+        for (int i = 0; i < e.P; ++i) same = same && st.R[i] == e.R[i];
+        if (same) return &st;
+    }
+    return nullptr;
+}
+
+// Without the autotuner, the real kinds take a fixed-size schedule of the
+// same length whose pipelined kernel runs their split in registers (the
+// first pass for c2r with inMode 0, the last for r2c) when the planner's
+// does not and one is registered (e.g. 8 x 16 x 16 beside 16 x 16 x 8 for
+// h = 2048).
+bool real_kind_schedule(const ComplexPlan* base, int kind, int mode, BatchedChoice* c)
+{
+    const bool wantFirst = kind == TUNE_C2R && mode == 0, wantLast = kind == TUNE_R2C;
+    if (!wantFirst && !wantLast) return false;
+    const StaticEntry* cur = static_of(base->eng);
+    if (cur && ((wantFirst && cur->mirrorFirst) || (wantLast && cur->mirrorLast))) return false;
+    for (const StaticEntry& st : static_schedules()) {
+        if (st.n != base->n || !((wantFirst && st.mirrorFirst) || (wantLast && st.mirrorLast))) continue;
+        EnginePlan e;
+        e.n = st.n;
+        e.emax = st.emax;
+        e.T = st.T;
+        e.P = st.P;
+        for (int i = 0; i < st.P; ++i) e.R[i] = st.R[i];
+        c->eng = e;
+        return true;
+    }
+    return false;
+}
+
+} // namespace
+
 ComplexPlan* get_batched_plan(uint32_t n, bool needSplit, int kind, int mode, uint32_t batch, cudaError_t* err)
 {
     ComplexPlan* base = get_complex_plan(n, needSplit, err);
-    if (!base || base->multiPass || !autotune_enabled()) return base;
+    if (!base || base->multiPass) return base;
     BatchedChoice c;
-    if (!tune_batched(base, kind, mode, batch, &c)) return base;
+    const bool tuned = autotune_enabled() && tune_batched(base, kind, mode, batch, &c);
+    if (!tuned && !real_kind_schedule(base, kind, mode, &c)) return base;
     std::lock_guard<std::mutex> lock(g_mu);
-    ComplexPlan*& slot = g_tuned_plans[{base->device, choice_key(n, c)}];
+    ComplexPlan*& slot = g_tuned_plans[{base->device, choice_key(n, c) + (tuned ? " tuned" : "")}];
     cudaStream_t s = cudaStreamPerThread;
     if (!slot) {
         ComplexPlan* p = new ComplexPlan();
@@ -473,12 +515,12 @@ ComplexPlan* get_batched_plan(uint32_t n, bool needSplit, int kind, int mode, ui
         p->gridCap = c.gridCap;
         p->tileM = c.tileM;
         p->noPipe = c.noPipe;
-        p->tuned = true;
+        p->tuned = tuned;
         *err = make_pass_table(&p->tw, p->eng, s);
         if (*err == cudaSuccess) *err = cudaStreamSynchronize(s);
         if (*err != cudaSuccess) {
             free_plan(p);
-            g_tuned_plans.erase({base->device, choice_key(n, c)});
+            g_tuned_plans.erase({base->device, choice_key(n, c) + (tuned ? " tuned" : "")});
             return nullptr;
         }
         slot = p;

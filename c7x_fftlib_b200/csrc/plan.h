@@ -122,7 +122,9 @@ ComplexPlan* get_complex_plan(uint32_t n, bool needSplit, cudaError_t* err);
 // Plan of a batched _init: get_complex_plan's, or with $FFTLIB_B200_AUTOTUNE
 // set and n a single-kernel length, a plan with the autotuner's choice for
 // (kind, mode, batch) (shared by every call shape that tunes to the same
-// choice; the planner's when timing fails).
+// choice; the planner's when timing fails). Untuned r2c / c2r calls take a
+// registered schedule of the same length whose pipelined kernel splits in
+// registers when the planner's does not.
 ComplexPlan* get_batched_plan(uint32_t n, bool needSplit, int kind, int mode, uint32_t batch, cudaError_t* err);
 // "tuned" / "planner" plus the schedule and launch choices of p.
 std::string describe_plan(const ComplexPlan* p);
