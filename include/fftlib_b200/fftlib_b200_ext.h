@@ -80,14 +80,16 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync(int16_t *pX
  *   such length; longer or other lengths return FFTLIB_ERR_INVALID_DIMENSION);
  *   stream: a cudaStream_t (NULL = legacy default stream). The call
  *   synchronizes `stream` and reads the device error word back before it
- *   returns, so the result is in pY on return.
+ *   returns, so the result is in pY on return; for the same reason it must
+ *   not be called while `stream` (or any stream) is being captured into a
+ *   graph.
  * - Every call looks up the scratch array's device address
  *   (cudaGetSymbolAddress). The first call in a process builds the host-side
  *   schedule tables and loads the library's device code on the current
  *   device; CUDA's lazy module loading (the default) loads each kernel's code
- *   on its first launch, so make one warm-up call per length at start-up,
- *   before any stream capture (or run with CUDA_MODULE_LOADING=EAGER), and
- *   later calls touch no allocator at all.
+ *   on its first launch, so make one warm-up call per length at start-up
+ *   (or run with CUDA_MODULE_LOADING=EAGER), and later calls touch no
+ *   allocator at all.
  * - Every call shares the one array and rebuilds its contents; calls that
  *   overlap on the GPU (other threads or streams) race on it. */
 FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc(FFTLIB_F32 *pX, FFTLIB_F32 *pY,
