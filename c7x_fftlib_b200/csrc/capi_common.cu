@@ -16,14 +16,20 @@ namespace {
 thread_local char t_error[512];
 constexpr size_t kChunkBytes = 32u << 20; // staged bytes per chunk (all host buffers)
 constexpr size_t kAlign = 256;
+// Staging slots, each with its own stream running copy-in, compute and
+// copy-out of one chunk: with three, the host-to-device copy of chunk k + 2
+// never waits for the device-to-host copy of chunk k (one slot would be the
+// copy-out's, one the compute's, one the copy-in's), so both copy directions
+// stream back to back.
+constexpr int kSlots = 3;
 
 size_t round_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 struct Staging {
     std::mutex mu;
-    void* buf[2] = {nullptr, nullptr};
-    size_t cap[2] = {0, 0};
-    cudaStream_t st[2] = {nullptr, nullptr};
+    void* buf[kSlots] = {};
+    size_t cap[kSlots] = {};
+    cudaStream_t st[kSlots] = {};
 };
 
 Staging* staging_for(int dev)
@@ -127,11 +133,13 @@ cudaError_t run_channels(std::vector<ChannelBuf>& bufs, uint32_t channels, const
     size_t slotBytes = 0;
     for (size_t i = 0; i < bufs.size(); ++i)
         if (!dev[i]) slotBytes += round_up(bufs[i].perChannel * chunk);
-    for (int s = 0; s < 2; ++s)
+    const uint32_t chunks = (channels + chunk - 1u) / chunk;
+    const int slots = (int)std::min<uint32_t>((uint32_t)kSlots, chunks);
+    for (int s = 0; s < slots; ++s)
         if ((e = ensure(*S, s, slotBytes)) != cudaSuccess) return e;
 
     for (uint32_t c0 = 0, it = 0; c0 < channels; c0 += chunk, ++it) {
-        const int slot = (int)(it & 1u);
+        const int slot = (int)(it % (uint32_t)slots);
         cudaStream_t st = S->st[slot];
         const uint32_t cc = std::min(chunk, channels - c0);
         char* base = (char*)S->buf[slot];
@@ -158,10 +166,13 @@ cudaError_t run_channels(std::vector<ChannelBuf>& bufs, uint32_t channels, const
             if (e != cudaSuccess) return e;
         }
     }
-    cudaError_t e0 = cudaStreamSynchronize(S->st[0]);
-    cudaError_t e1 = cudaStreamSynchronize(S->st[1]);
-    if (e0 == cudaSuccess && e1 == cudaSuccess && take_device_error()) return cudaErrorLaunchTimeout;
-    return e0 != cudaSuccess ? e0 : e1;
+    cudaError_t first = cudaSuccess;
+    for (int s = 0; s < slots; ++s) {
+        const cudaError_t es = cudaStreamSynchronize(S->st[s]);
+        if (first == cudaSuccess) first = es;
+    }
+    if (first == cudaSuccess && take_device_error()) return cudaErrorLaunchTimeout;
+    return first;
 }
 
 cudaError_t device_table(const void* p, size_t bytes, int slot, const void** out)
