@@ -53,6 +53,7 @@ struct FFTLIB_b200_mixed {
     uint32_t clsStage[kMixedClasses] = {};
     uint32_t groupStage = 0;            // largest stage of any group (per-size launches)
     uint32_t clsGrid[kMixedClasses] = {};
+    uint32_t perSizeGrid[kMixedClasses] = {};  // resident CTAs of each class at groupStage
     // fixed groups: the regular plan's fixed-size kernel on a grid share
     struct Fixed {
         uint32_t n, count;
@@ -383,10 +384,12 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
     for (int cls = 0; cls < kMixedClasses && err == cudaSuccess; ++cls) {
         if (h->clsTiles[cls]) err = class_grid(cls, h->clsStage[cls], h->device, &h->clsGrid[cls]);
     }
-    // per-size launches use the largest stage of any group with both classes
+    // per-size launches use the largest stage of any group with both classes,
+    // and every class that has a group (fixed groups included) on its full
+    // resident grid
     for (int cls = 0; cls < kMixedClasses && err == cudaSuccess; ++cls) {
-        uint32_t unused = 0;
-        if (h->clsTiles[cls]) err = class_grid(cls, h->groupStage, h->device, &unused);
+        const bool used = std::find(h->groupCls.begin(), h->groupCls.end(), cls) != h->groupCls.end();
+        if (used) err = class_grid(cls, h->groupStage, h->device, &h->perSizeGrid[cls]);
     }
     // Branches: the fixed groups are packed into kMaxBranches branches,
     // largest work first onto the least loaded; each class with tiles takes a
@@ -505,7 +508,7 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_execPerSize(FFTLIB_b200_mixedHandle h, const 
         const uint32_t b = h->groupTileBegin[g], e = h->groupTileEnd[g];
         const int cls = h->groupCls[g];
         cudaError_t err = launch_mixed(class_launch(cls, h->dGroups, h->dTilesByGroup + b, e - b, h->dOffsets, pX, pY,
-                                                    h->groupStage, h->clsGrid[cls]),
+                                                    h->groupStage, h->perSizeGrid[cls]),
                                        (cudaStream_t)stream);
         if (err != cudaSuccess) return cuda_fail(err, "mixed per-size launch");
     }
