@@ -30,6 +30,7 @@ struct PlanRecord {
     ComplexPlan* plan;   // FP32 kinds
     uint32_t i16Tg;      // int16: threads per transform (0: the launcher's default)
     uint32_t i16GridCap; //   and CTA cap (0: all resident)
+    uint32_t i16MinBlocks; // and register budget (CTAs per SM; 0: the default)
     uint32_t i16Tuned;   //   nonzero when the autotuner chose them
 };
 static_assert(sizeof(PlanRecord) <= 64, "plan record must fit the smallest pBlock");

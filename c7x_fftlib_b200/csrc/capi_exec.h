@@ -27,9 +27,10 @@ FFTLIB_STATUS exec_c2c(float* pX, float* pY, uint32_t n, uint32_t c, bool invers
 FFTLIB_STATUS exec_r2c(float* pX, float* pXFFT, float* pY, uint32_t n, uint32_t c, int outmode, ComplexPlan* plan);
 FFTLIB_STATUS exec_c2r(float* pX, float* pXFFT, float* pY, uint32_t n, uint32_t c, int inmode, ComplexPlan* plan);
 // int16 radix-4 transform with per-stage shifts (pW: the Q15 table of n).
-// tg, gridCap: the int16 launch shape (0, 0: the launcher's defaults).
+// tg, gridCap, minBlocks: the int16 launch shape (0, 0, 3: the launcher's
+// defaults).
 FFTLIB_STATUS exec_i16(int16_t* pX, const int16_t* pW, int16_t* pY, const uint32_t* pShift, uint32_t numShifts,
-                       uint32_t n, uint32_t c, uint32_t tg = 0, uint32_t gridCap = 0);
+                       uint32_t n, uint32_t c, uint32_t tg = 0, uint32_t gridCap = 0, uint32_t minBlocks = 3);
 
 // Builds (or finds) the FP32 plan of an _init and records it in pBlock;
 // real kinds plan the n/2-point complex transform with the split tables.

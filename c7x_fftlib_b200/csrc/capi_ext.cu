@@ -128,6 +128,7 @@ FFTLIB_STATUS FFTLIB_b200_describeBlock(const void* pBlock, char* buf, uint32_t 
         s = std::string(r.i16Tuned ? "tuned: " : "planner: ") + "int16 radix-4, " + std::to_string(tg) +
             " threads per transform, " + std::to_string(256u / tg) + " transforms per CTA";
         if (r.i16GridCap) s += ", " + std::to_string(r.i16GridCap) + " CTAs";
+        if (r.i16MinBlocks == 4u) s += ", 64 registers (4 CTAs per SM)";
     } else if (r.plan) {
         s = describe_plan(r.plan);
     } else {
@@ -199,7 +200,7 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync(int16_t* pX
     if (!pX || !pW || !pY || !pShift) return FFTLIB_ERR_NULL_POINTER;
     if (numShifts < i16_num_shifts(numPoints)) return FFTLIB_ERR_INVALID_DIMENSION;
     return launched(launch_fft_i16(pX, pY, pW, pShift, numPoints, numChannels, (cudaStream_t)stream, r.i16Tg,
-                                   r.i16GridCap),
+                                   r.i16GridCap, r.i16MinBlocks ? r.i16MinBlocks : 3u),
                     "fft1dBatched int16");
 }
 

@@ -207,7 +207,7 @@ FFTLIB_STATUS exec_c2r(float* pX, float* pXFFT, float* pY, uint32_t n, uint32_t 
 }
 
 FFTLIB_STATUS exec_i16(int16_t* pX, const int16_t* pW, int16_t* pY, const uint32_t* pShift, uint32_t numShifts,
-                       uint32_t n, uint32_t c, uint32_t tg, uint32_t gridCap)
+                       uint32_t n, uint32_t c, uint32_t tg, uint32_t gridCap, uint32_t minBlocks)
 {
     if (n == 0 || (n & (n - 1u)) || n > 16384u) {
         set_error("int16 numPoints %u must be a power of two <= 16384", n);
@@ -227,7 +227,7 @@ FFTLIB_STATUS exec_i16(int16_t* pX, const int16_t* pW, int16_t* pY, const uint32
     std::vector<ChannelBuf> bufs = {{pX, bytes, true, false}, {pY, bytes, false, true}};
     e = run_channels(bufs, c, [&](const std::vector<void*>& d, uint32_t, uint32_t cnt, cudaStream_t s) {
         return launch_fft_i16((const int16_t*)d[0], (int16_t*)d[1], (const int16_t*)dW, (const uint32_t*)dS, n, cnt, s,
-                              tg, gridCap);
+                              tg, gridCap, minBlocks);
     });
     if (e != cudaSuccess) return cuda_fail(e, "fft1dBatched int16");
     return FFTLIB_SUCCESS;
@@ -552,6 +552,7 @@ FFTLIB_STATUS FFTLIB_fft1dBatched_i16sc_c16sc_o16sc_init(int16_t* pX, FFTLIB_buf
         memcpy(&r, pBlock, sizeof(r));
         r.i16Tg = ch.tg;
         r.i16GridCap = ch.gridCap;
+        r.i16MinBlocks = ch.minBlocks;
         r.i16Tuned = 1u;
         memcpy(pBlock, &r, sizeof(r));
     }
@@ -570,7 +571,8 @@ FFTLIB_STATUS FFTLIB_fft1dBatched_i16sc_c16sc_o16sc_kernel(int16_t* pX, FFTLIB_b
     if (st != FFTLIB_SUCCESS) return st;
     if (!pX || !pW || !pY || !pShift || !bufParamsShift) return FFTLIB_ERR_NULL_POINTER;
     DeviceScope scope(r.device);
-    return exec_i16(pX, pW, pY, pShift, bufParamsShift->dim_x, numPoints, numChannels, r.i16Tg, r.i16GridCap);
+    return exec_i16(pX, pW, pY, pShift, bufParamsShift->dim_x, numPoints, numChannels, r.i16Tg, r.i16GridCap,
+                    r.i16MinBlocks ? r.i16MinBlocks : 3u);
 }
 
 FFTLIB_STATUS FFTLIB_fft1dBatched_i16sc_c16sc_o16sc_cn(int16_t* pX, FFTLIB_bufParams1D_t* bufParamsX,

@@ -164,7 +164,10 @@ __device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
 // time (its own padded shared-memory region) and the CTA walks the batch G
 // transforms at a step. The caller's twiddle table and the shift vector are
 // copied into shared memory once per CTA.
-__global__ void __launch_bounds__(256, 3) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
+// MINB: CTAs per SM the registers are budgeted for (3: 80 registers; 4: 64,
+// with a few spilled values), a launch-shape choice of the autotuner.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
                                                  const short2* __restrict__ w,
                                                  const uint32_t* __restrict__ shifts, uint32_t nsh, uint32_t n,
                                                  uint32_t logn, uint32_t batch, uint32_t tg, bool vec)
@@ -217,10 +220,11 @@ __global__ void __launch_bounds__(256, 3) k_fft_i16(const short2* __restrict__ x
             const ShiftRound srA(shiftA, m != 8u), srB(shiftB, m2 != 8u);
             const int2* tw2 = tw + 3u * (m / 4u);
             const uint32_t s16 = m / 16u;
+            const uint32_t ls16 = 31u - __clz(s16);  // m is a power of two: shifts, not divisions
             const uint32_t groups = n / 16u; // (block, k0) pairs
             if (active) {
                 for (uint32_t gi = t; gi < groups; gi += tg) {
-                    const uint32_t blk = gi / s16, k0 = gi - blk * s16;
+                    const uint32_t blk = gi >> ls16, k0 = gi & (s16 - 1u);
                     const uint32_t base = blk * m + k0;
                     C16 p[16];
 #pragma unroll
@@ -311,29 +315,35 @@ size_t i16_smem_bytes(uint32_t n, uint32_t tg)
 
 namespace {
 
-cudaError_t i16_configure(size_t smem)
+using I16Kernel = void (*)(const short2*, short2*, const short2*, const uint32_t*, uint32_t, uint32_t, uint32_t,
+                           uint32_t, uint32_t, bool);
+
+I16Kernel i16_kernel(uint32_t minBlocks) { return minBlocks == 4u ? &k_fft_i16<4> : &k_fft_i16<3>; }
+
+cudaError_t i16_configure(size_t smem, uint32_t minBlocks)
 {
     static std::mutex mu;
-    static size_t configured[64] = {};
+    static size_t configured[64][2] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (smem <= 48u * 1024u) return cudaSuccess;
+    const int k = minBlocks == 4u ? 1 : 0;
     std::lock_guard<std::mutex> lock(mu);
-    if (dev < 64 && configured[dev] >= smem) return cudaSuccess;
-    e = cudaFuncSetAttribute(k_fft_i16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess && dev < 64) configured[dev] = smem;
+    if (dev < 64 && configured[dev][k] >= smem) return cudaSuccess;
+    e = cudaFuncSetAttribute(i16_kernel(minBlocks), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && dev < 64) configured[dev][k] = smem;
     return e;
 }
 
 } // namespace
 
-int i16_resident(uint32_t n, uint32_t tg)
+int i16_resident(uint32_t n, uint32_t tg, uint32_t minBlocks)
 {
     const size_t smem = i16_smem_bytes(n, tg);
     int perSm = 0;
-    if (i16_configure(smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_fft_i16, 256, smem) != cudaSuccess) {
+    if (i16_configure(smem, minBlocks) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, i16_kernel(minBlocks), 256, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -341,9 +351,11 @@ int i16_resident(uint32_t n, uint32_t tg)
 }
 
 cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const uint32_t* shifts,
-                           uint32_t n, uint32_t batch, cudaStream_t s, uint32_t tg, uint32_t gridCap)
+                           uint32_t n, uint32_t batch, cudaStream_t s, uint32_t tg, uint32_t gridCap,
+                           uint32_t minBlocks)
 {
     if (batch == 0) return cudaSuccess;
+    const I16Kernel kern = i16_kernel(minBlocks);
     uint32_t logn = 0;
     while ((1u << logn) < n) ++logn;
     if (tg == 0) tg = i16_default_tg(n);
@@ -354,10 +366,10 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    e = i16_configure(smem);
+    e = i16_configure(smem, minBlocks);
     if (e != cudaSuccess) return e;
     int perSm = 0, sms = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_fft_i16, (int)threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, (int)threads, smem);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
@@ -365,8 +377,8 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
     uint32_t grid = (uint32_t)std::min<uint64_t>(steps, (uint64_t)std::max(1, perSm) * (uint64_t)sms);
     if (gridCap) grid = std::max(1u, std::min(grid, gridCap));
     const bool vec = (((uintptr_t)x & 15u) == 0) && (n % 4u) == 0;
-    k_fft_i16<<<grid, threads, smem, s>>>((const short2*)x, (short2*)y, (const short2*)w, shifts, i16_num_shifts(n),
-                                          n, logn, batch, tg, vec);
+    kern<<<grid, threads, smem, s>>>((const short2*)x, (short2*)y, (const short2*)w, shifts, i16_num_shifts(n), n,
+                                     logn, batch, tg, vec);
     return cudaGetLastError();
 }
 

@@ -10,23 +10,26 @@ namespace fftb200 {
 uint32_t i16_num_shifts(uint32_t n);
 
 // Launch shape of the int16 kernel: tg threads per transform (a power of
-// two up to 256; each CTA of 256 threads holds 256 / tg transforms) and at
-// most gridCap CTAs (0: all that are resident).
+// two up to 256; each CTA of 256 threads holds 256 / tg transforms), at
+// most gridCap CTAs (0: all that are resident), and the register budget
+// minBlocks (3: 80 registers per thread; 4: 64, four CTAs per SM; 0: 3).
 struct I16Choice {
     uint32_t tg;
     uint32_t gridCap;
+    uint32_t minBlocks;
 };
 // The launcher's default tg: 256 from n = 4096 up, else n / 16 (at least 1).
 uint32_t i16_default_tg(uint32_t n);
 // Dynamic shared memory of a CTA with that tg, and CTAs resident per SM.
 size_t i16_smem_bytes(uint32_t n, uint32_t tg);
-int i16_resident(uint32_t n, uint32_t tg);
+int i16_resident(uint32_t n, uint32_t tg, uint32_t minBlocks = 3);
 
 // x, y: batch x n interleaved int16 complex; w: the caller's Q15 radix-4
 // table (2n int16); shifts: i16_num_shifts(n) entries. All device pointers.
 // n must be a power of two, 1 <= n <= 16384. tg = 0: i16_default_tg(n).
 cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const uint32_t* shifts,
-                           uint32_t n, uint32_t batch, cudaStream_t s, uint32_t tg = 0, uint32_t gridCap = 0);
+                           uint32_t n, uint32_t batch, cudaStream_t s, uint32_t tg = 0, uint32_t gridCap = 0,
+                           uint32_t minBlocks = 3);
 
 // Autotuner of the int16 launch shape for (device, n, batch bucket): times
 // the candidate tg and CTA counts on synthetic data; cached like the FP32

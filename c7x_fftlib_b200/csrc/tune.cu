@@ -511,9 +511,11 @@ bool tune_i16(uint32_t n, uint32_t batch, I16Choice* out)
     const int sms = prop.multiProcessorCount;
     std::vector<I16Choice> cands;
     for (uint32_t tg : i16_tg_candidates(n)) {
-        const int resident = i16_resident(n, tg);
-        cands.push_back(I16Choice{tg, 0u});
-        for (int k = 1; k <= 2 && k < resident; ++k) cands.push_back(I16Choice{tg, (uint32_t)(k * sms)});
+        const int resident = i16_resident(n, tg, 3u);
+        cands.push_back(I16Choice{tg, 0u, 3u});
+        for (int k = 1; k <= 2 && k < resident; ++k) cands.push_back(I16Choice{tg, (uint32_t)(k * sms), 3u});
+        // the 64-register build, when shared memory lets a fourth CTA in
+        if (i16_resident(n, tg, 4u) > resident) cands.push_back(I16Choice{tg, 0u, 4u});
     }
     if (cands.empty()) return false;
     const std::string key = key_of(prop, n, batch, "c2c:i16");
@@ -522,9 +524,9 @@ bool tune_i16(uint32_t n, uint32_t batch, I16Choice* out)
     if (cache_get(key, &val)) {
         std::istringstream is(val);
         I16Choice c{};
-        if (is >> c.tg >> c.gridCap)
+        if (is >> c.tg >> c.gridCap >> c.minBlocks)
             for (const I16Choice& k : cands)
-                if (k.tg == c.tg && k.gridCap == c.gridCap) {
+                if (k.tg == c.tg && k.gridCap == c.gridCap && k.minBlocks == c.minBlocks) {
                     *out = k;
                     return true;
                 }
@@ -558,11 +560,12 @@ bool tune_i16(uint32_t n, uint32_t batch, I16Choice* out)
         const I16Choice c = cands[i];
         const float ms = time_runs(
             [&] {
-                return launch_fft_i16((const int16_t*)x, (int16_t*)y, w, sh, n, (uint32_t)tb, b.s, c.tg, c.gridCap);
+                return launch_fft_i16((const int16_t*)x, (int16_t*)y, w, sh, n, (uint32_t)tb, b.s, c.tg, c.gridCap,
+                                      c.minBlocks);
             },
             b.s, &ok);
         if (verbose)
-            fprintf(stderr, "fftlib_b200 tune %s: %u %u -> %s\n", key.c_str(), c.tg, c.gridCap,
+            fprintf(stderr, "fftlib_b200 tune %s: %u %u %u -> %s\n", key.c_str(), c.tg, c.gridCap, c.minBlocks,
                     ok ? (std::to_string(ms * 1e3f) + " us").c_str() : "failed");
         if (ok && (bestIdx < 0 || ms < best)) {
             best = ms;
@@ -571,7 +574,8 @@ bool tune_i16(uint32_t n, uint32_t batch, I16Choice* out)
     }
     if (bestIdx < 0) return false;
     *out = cands[(size_t)bestIdx];
-    cache_put(key, std::to_string(out->tg) + " " + std::to_string(out->gridCap));
+    cache_put(key, std::to_string(out->tg) + " " + std::to_string(out->gridCap) + " " +
+                       std::to_string(out->minBlocks));
     return true;
 }
 

@@ -185,3 +185,33 @@ def test_untuned_block_says_planner(torch, monkeypatch):
     x = torch.rand(2 * n * ch, device="cuda") * 2 - 1
     _, desc = c2c_init_run(torch, "c2c", x, n, ch)
     assert desc.startswith("planner: ") and "fixed-size pipelined kernel" in desc, desc
+
+
+@pytest.mark.parametrize("n,ch", [(1024, 4096), (256, 3000), (64, 2000)])
+def test_i16_64_register_build_bit_exact(torch, tuning, n, ch):
+    """A cache entry selects the int16 kernel built for 64 registers (four
+    CTAs per SM) when shared memory admits a fourth CTA; that build is
+    bit-exact too."""
+    nsh = 0
+    m = n
+    while m > 2:
+        nsh, m = nsh + 1, m // 4
+    sh = np.full(nsh, 2, np.uint32)
+    dev = torch.cuda.get_device_name(0).replace(" ", "_")
+    tgs = [t for t in (n // 16, n // 32, n // 64) if t >= 1]
+    tuning.write_text("".join(f"{dev}|{n}|{bucket(ch)}|c2c:i16 {tg} 0 4\n" for tg in tgs[::-1]))
+    x = O.int16_input(n, ch, 5 + n)
+    w = np.zeros(2 * n, np.int16)
+    F.lib().FFTLIB_b200_tw_gen_i16(F.ptr(w), n)
+    X, W = torch.from_numpy(x).cuda(), torch.from_numpy(w).cuda()
+    Y = torch.zeros(2 * n * ch, dtype=torch.int16, device="cuda")
+    S = torch.from_numpy(sh.view(np.int32)).cuda()
+    bX, bW, bS = F.bp(F.FFTLIB_INT16, 2 * n * ch), F.bp(F.FFTLIB_INT16, 2 * n), F.bp(F.FFTLIB_UINT32, nsh)
+    pb = F.pblock("i16")
+    args = (F.ptr(X), bX, F.ptr(W), bW, F.ptr(Y), bX, F.ptr(S), bS, n, ch)
+    F.check(F.fn(F.KERNELS["i16"] + "_init")(*args, pb))
+    desc = F.describe_block(pb)
+    F.check(F.fn(F.KERNELS["i16"] + "_kernel")(*args, pb))
+    np.testing.assert_array_equal(Y.cpu().numpy(), O.fft_c2c_i16(x, n, ch, sh))
+    if "64 registers" not in desc:
+        pytest.skip(f"no 64-register candidate for N={n} on this device: {desc}")
