@@ -132,3 +132,22 @@ def test_mixed_grouped_and_persistent_agree(torch, inverse):
         torch.cuda.synchronize()
         check_all(x, Y.cpu().numpy(), lengths, inverse)
         mb.close()
+
+
+@pytest.mark.parametrize("branches", ["1", "3", "8"])
+def test_mixed_chained_launches_on_branches(torch, monkeypatch, branches):
+    """The fixed-size groups' launches chained by programmatic dependent
+    launch, on one branch (the default) or spread over several, replayed
+    twice from the graph: every transform against FP64."""
+    monkeypatch.setenv("FFTLIB_B200_MIXED_BRANCHES", branches)
+    lengths = np.sort(fftcall.mixed_lengths(3000, seed=77))[::-1].copy()
+    total = int(lengths.sum())
+    x = O.uniform_c2c(total, 1, seed=78)
+    X = torch.from_numpy(x).cuda()
+    Y = torch.zeros_like(X)
+    mb = F.MixedBatch(lengths)
+    for _ in range(2):
+        mb.exec(X, Y)
+    torch.cuda.synchronize()
+    check_all(x, Y.cpu().numpy(), lengths, False)
+    mb.close()
