@@ -232,3 +232,24 @@ def test_lengths_up_to_4096_output_off_16_byte_boundary(torch):
         F.check(F.fn(base_name + "_kernel")(F.ptr(xo.data_ptr() + 8), bX, F.ptr(w), bW, F.ptr(yv), bX, n, ch, pb))
         overall, worst = O.gpu_check_c2c(x, yv, n, ch)
         assert overall <= REL_L2 and worst <= REL_L2, (n, "pX off 16 B", overall, worst)
+
+
+@pytest.mark.parametrize("kind", ["c2c", "ifft"])
+def test_host_buffers_through_the_chunk_pipeline(torch, kind):
+    """Host buffers spanning several 32 MiB staging chunks (three slots in
+    rotation, a short last chunk): the result equals the device-buffer
+    call's bit for bit."""
+    n, ch = 1024, 3 * 2048 + 5  # 32 MiB chunks of 2048 channels in + out
+    g = torch.Generator().manual_seed(99)
+    xh = (torch.rand(2 * n * ch, generator=g) * 2 - 1).pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    xd = xh.cuda()
+    yd = _c2c(torch, kind, xd, n, ch)
+    w = torch.zeros(2 * n)
+    bX, bW = F.bp(F.FFTLIB_FLOAT32, 2 * n * ch), F.bp(F.FFTLIB_FLOAT32, 2 * n)
+    pb = F.pblock(kind)
+    base = F.KERNELS[kind]
+    src = xh.clone()
+    F.check(F.fn(base + "_init")(F.ptr(src), bX, F.ptr(w), bW, F.ptr(yh), bX, n, ch, pb))
+    F.check(F.fn(base + "_kernel")(F.ptr(src), bX, F.ptr(w), bW, F.ptr(yh), bX, n, ch, pb))
+    assert torch.equal(yh, yd.cpu())
