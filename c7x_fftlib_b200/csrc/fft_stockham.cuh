@@ -151,9 +151,22 @@ FFT_DEV void r2c_split_pair(float2 z, float2 zm, float2 w, float2& y, float2& ym
 FFT_DEV float2 c2r_split(float2 x, float2 xm, float2 w);
 FFT_DEV void c2r_split_pair(float2 x, float2 xm, float2 w, float2& z, float2& zm);
 template <int R>
-FFT_DEV void c2r_mirror_split(const FftArgs& a, float2* v, uint32_t t, uint32_t nb, const float2* raw);
+FFT_DEV void c2r_mirror_split(const FftArgs& a, float2* v, uint32_t t, uint32_t nb, const float2* raw,
+                              const float2 (&w)[R + 1]);
 template <int R>
-FFT_DEV void r2c_mirror_store(const FftArgs& a, const float2* v, uint32_t t, uint32_t nb, float2* row);
+FFT_DEV void r2c_mirror_store(const FftArgs& a, const float2* v, uint32_t t, uint32_t nb, float2* row,
+                              const float2 (&w)[R + 1]);
+
+// Split-table index of slot q (0..R) of a mirrored pass: t + q nb for
+// thread t != 0 (slot R repeats slot 0); for thread 0, q nb (q <= R/2), then
+// nb/2 + (q - R/2 - 1) nb. The loads are issued before the pass's gather.
+template <int R>
+FFT_DEV uint32_t mirror_tw_index(uint32_t t, int q, uint32_t nb)
+{
+    const uint32_t q0 = (uint32_t)(q <= R / 2 ? q : q - R / 2 - 1);
+    const uint32_t t0 = q <= R / 2 ? 0u : nb / 2u;
+    return t != 0u ? t + (uint32_t)(q < R ? q : 0) * nb : t0 + q0 * nb;
+}
 
 template <int EMAX, int R, class Hook = NoHook, bool RAW_FIRST = false, int LIN = kPad16, int LOUT = kPad16,
           bool UNIT = false, int MIRROR = kMirrorNone>
@@ -166,6 +179,13 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
     static_assert(MIRROR == kMirrorNone || BMAX == 2, "the mirrored passes hold two butterflies per thread");
     const uint32_t nb = pi.stride; // butterflies in this pass: N / R
     auto bfly = [&](int i) FFT_INL { return MIRROR ? mirror_j(t, i, nb) : t + (uint32_t)i * T; };
+    // the mirrored split's table entries, in flight during the gather
+    [[maybe_unused]] float2 wsplit[MIRROR ? R + 1 : 1];
+    if constexpr (MIRROR != kMirrorNone) {
+        static_for<R + 1>([&](auto q) FFT_INL {
+            wsplit[q] = __ldg(&a.twSplit[mirror_tw_index<R>(t, decltype(q)::value, nb)]);
+        });
+    }
 
     // gather
     static_for<BMAX>([&](auto i) FFT_INL {
@@ -186,7 +206,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
             });
         }
     });
-    if constexpr (MIRROR == kMirrorC2R) c2r_mirror_split<R>(a, v, t, nb, raw);
+    if constexpr (MIRROR == kMirrorC2R) c2r_mirror_split<R>(a, v, t, nb, raw, wsplit);
     // one uniform branch around the input conjugation of the inverse
     if (first && (RAW_FIRST || raw) && a.conjIn) {
         static_for<BMAX * R>([&](auto e) FFT_INL { v[e] = cconj(v[e]); });
@@ -211,7 +231,7 @@ FFT_DEV void run_pass(const FftArgs& a, const PassInfo pi, const bool first, con
     });
 
     if constexpr (MIRROR == kMirrorR2C) {
-        if (active) r2c_mirror_store<R>(a, v, t, nb, rowOut);
+        if (active) r2c_mirror_store<R>(a, v, t, nb, rowOut, wsplit);
         return;
     }
 
@@ -310,28 +330,26 @@ FFT_DEV void c2r_split_pair(float2 x, float2 xm, float2 w, float2& z, float2& zm
 // of q nb (thread 0) (R - q) nb, and of bin 0 the Nyquist bin X[h] (raw[h]).
 // W_{2h}^(h-i) = -conj(W_{2h}^i): one table load serves each pair.
 template <int R>
-FFT_DEV void c2r_mirror_split(const FftArgs& a, float2* v, uint32_t t, uint32_t nb, const float2* raw)
+FFT_DEV void c2r_mirror_split(const FftArgs& a, float2* v, uint32_t t, uint32_t nb, const float2* raw,
+                              const float2 (&w)[R + 1])
 {
     if (t != 0u) {
         static_for<R>([&](auto q) FFT_INL {
             constexpr int qq = decltype(q)::value;
-            const float2 w = __ldg(&a.twSplit[t + (uint32_t)qq * nb]);
-            c2r_split_pair(v[qq], v[2 * R - 1 - qq], w, v[qq], v[2 * R - 1 - qq]);
+            c2r_split_pair(v[qq], v[2 * R - 1 - qq], w[qq], v[qq], v[2 * R - 1 - qq]);
         });
         return;
     }
     const float2 xh = raw[a.N];
-    v[0] = c2r_split(v[0], xh, __ldg(&a.twSplit[0]));
+    v[0] = c2r_split(v[0], xh, w[0]);
     static_for<R / 2>([&](auto q1) FFT_INL {
         constexpr int q = decltype(q1)::value + 1;  // pairs (q, R - q), q = R/2 alone
-        const float2 w = __ldg(&a.twSplit[(uint32_t)q * nb]);
-        if constexpr (q != R - q) c2r_split_pair(v[q], v[R - q], w, v[q], v[R - q]);
-        else v[q] = c2r_split(v[q], v[q], w);
+        if constexpr (q != R - q) c2r_split_pair(v[q], v[R - q], w[q], v[q], v[R - q]);
+        else v[q] = c2r_split(v[q], v[q], w[q]);
     });
     static_for<R / 2>([&](auto q1) FFT_INL {
         constexpr int q = decltype(q1)::value;  // pairs (q, R-1-q) of butterfly nb / 2
-        const float2 w = __ldg(&a.twSplit[nb / 2u + (uint32_t)q * nb]);
-        c2r_split_pair(v[R + q], v[2 * R - 1 - q], w, v[R + q], v[2 * R - 1 - q]);
+        c2r_split_pair(v[R + q], v[2 * R - 1 - q], w[R / 2 + 1 + q], v[R + q], v[2 * R - 1 - q]);
     });
 }
 
@@ -339,7 +357,8 @@ FFT_DEV void c2r_mirror_split(const FftArgs& a, float2* v, uint32_t t, uint32_t 
 // c2r_mirror_split), written as bins i and h - i of row (and, with
 // realMode, their conjugates at 2h - i).
 template <int R>
-FFT_DEV void r2c_mirror_store(const FftArgs& a, const float2* v, uint32_t t, uint32_t nb, float2* row)
+FFT_DEV void r2c_mirror_store(const FftArgs& a, const float2* v, uint32_t t, uint32_t nb, float2* row,
+                              const float2 (&w)[R + 1])
 {
     const uint32_t h = a.N;
     const bool full = a.realMode != 0;
@@ -352,7 +371,7 @@ FFT_DEV void r2c_mirror_store(const FftArgs& a, const float2* v, uint32_t t, uin
             constexpr int qq = decltype(q)::value;
             const uint32_t i = t + (uint32_t)qq * nb;
             float2 y, ym;
-            r2c_split_pair(v[qq], v[2 * R - 1 - qq], __ldg(&a.twSplit[i]), y, ym);
+            r2c_split_pair(v[qq], v[2 * R - 1 - qq], w[qq], y, ym);
             put(i, y);
             put(h - i, ym);
         });
@@ -364,21 +383,20 @@ FFT_DEV void r2c_mirror_store(const FftArgs& a, const float2* v, uint32_t t, uin
     static_for<R / 2>([&](auto q1) FFT_INL {
         constexpr int q = decltype(q1)::value + 1;
         const uint32_t i = (uint32_t)q * nb;
-        const float2 w = __ldg(&a.twSplit[i]);
         if constexpr (q != R - q) {
             float2 y, ym;
-            r2c_split_pair(v[q], v[R - q], w, y, ym);
+            r2c_split_pair(v[q], v[R - q], w[q], y, ym);
             put(i, y);
             put(h - i, ym);
         } else {
-            put(i, r2c_split(v[q], v[q], w));
+            put(i, r2c_split(v[q], v[q], w[q]));
         }
     });
     static_for<R / 2>([&](auto q1) FFT_INL {
         constexpr int q = decltype(q1)::value;
         const uint32_t i = nb / 2u + (uint32_t)q * nb;
         float2 y, ym;
-        r2c_split_pair(v[R + q], v[2 * R - 1 - q], __ldg(&a.twSplit[i]), y, ym);
+        r2c_split_pair(v[R + q], v[2 * R - 1 - q], w[R / 2 + 1 + q], y, ym);
         put(i, y);
         put(h - i, ym);
     });
