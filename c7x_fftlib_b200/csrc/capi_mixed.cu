@@ -436,7 +436,23 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
             f.grid = (uint32_t)std::max(1.0, std::round((double)sms * res * load[f.branch] / total));
             h->fixedPoints += (uint64_t)f.n * f.count;
         }
-        // launches of a branch in its order: largest first
+        // launches of a branch in its order: largest and smallest work in
+        // turn, so the launch that follows a large one (and starts while it
+        // drains) is a short one that fills its tail (20,000-transform set:
+        // 90 us against 92.5-93.5 us for ascending or descending length)
+        {
+            using Fx = FFTLIB_b200_mixed::Fixed;
+            std::stable_sort(h->fixed.begin(), h->fixed.end(), [](const Fx& a, const Fx& b) {
+                return (uint64_t)a.n * a.count > (uint64_t)b.n * b.count;
+            });
+            std::vector<Fx> o;
+            size_t lo = 0, hi = h->fixed.size();
+            while (lo < hi) {
+                o.push_back(h->fixed[lo++]);
+                if (lo < hi) o.push_back(h->fixed[--hi]);
+            }
+            h->fixed = o;
+        }
         std::stable_sort(h->fixed.begin(), h->fixed.end(), [](const FFTLIB_b200_mixed::Fixed& a,
                                                               const FFTLIB_b200_mixed::Fixed& b) {
             return a.branch < b.branch;
