@@ -20,6 +20,12 @@ int engine_max_threads(int emax);
 // the runtime-planned engine of width emax.
 cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s);
 
+// c2c rows of N <= kSmallFftMax contiguous values, one transform per thread
+// (fft_small.cu); launch_fft takes this path for every launch it fits.
+constexpr uint32_t kSmallFftMax = 32;
+bool small_fft_eligible(const FftArgs& a);
+cudaError_t launch_fft_small(const FftArgs& a, cudaStream_t s);
+
 // A compiled fixed-size schedule.
 struct StaticEntry {
     uint32_t n;

@@ -130,6 +130,7 @@ int static_pipelined_resident(uint32_t n, int emax, uint32_t T, int P, const int
 cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s)
 {
     if (a.batch == 0) return cudaSuccess;
+    if (small_fft_eligible(a)) return launch_fft_small(a, s);
     if (const StaticEntry* st = find_static(a, emax)) {
         // the pipelined kernel brings whole tiles in with bulk copies, so the
         // static kernel's staged I/O (for transforms of few threads) is moot
