@@ -20,9 +20,10 @@ int engine_max_threads(int emax);
 // the runtime-planned engine of width emax.
 cudaError_t launch_fft(const FftArgs& a, int emax, cudaStream_t s);
 
-// c2c rows of N <= kSmallFftMax contiguous values, one transform per thread
-// (fft_small.cu); launch_fft takes this path for every launch it fits.
-constexpr uint32_t kSmallFftMax = 32;
+// c2c rows of N contiguous values, one transform per thread (fft_small.cu),
+// for the lengths small_fft_length accepts; launch_fft takes this path for
+// every launch it fits.
+bool small_fft_length(uint32_t n);
 bool small_fft_eligible(const FftArgs& a);
 cudaError_t launch_fft_small(const FftArgs& a, cudaStream_t s);
 

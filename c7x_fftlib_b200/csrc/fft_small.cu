@@ -1,10 +1,11 @@
-// fft_small.cu -- FP32 c2c of lengths 2..32 with one transform per thread.
+// fft_small.cu -- FP32 c2c of lengths 2..32 and 45 with one transform per
+// thread.
 //
 // For these lengths every exchange-based schedule spends its time on
 // shared-memory traffic and barriers around a few butterflies (the
 // pipelined kernel's two passes ran N = 8 at 2.6 TB/s and N = 16 at
-// 3.3 TB/s). Here a CTA of 256 (128 above N = 16) threads takes as many
-// consecutive transforms (their values contiguous): the threads copy them into shared memory with
+// 3.3 TB/s). Here a CTA of 256 (128 above N = 16, 64 above 32) threads takes
+// as many consecutive transforms (their values contiguous): the threads copy them into shared memory with
 // coalesced 8- or 16-byte accesses (rows padded to an odd number of values,
 // so that one row per lane is conflict-free), each thread runs the
 // in-register DFT codelet dft<N> (natural order in and out) on its row, and
@@ -19,10 +20,10 @@ namespace fftb200 {
 
 namespace {
 
-// transforms (threads) per CTA: 256, or 128 above N = 16 (the padded rows
-// then stay within 48 KB of static shared memory)
+// transforms (threads) per CTA: 256, 128 above N = 16, 64 above N = 32 (the
+// padded rows stay within 48 KB of static shared memory)
 template <int N>
-constexpr int small_rows() { return N <= 16 ? 256 : 128; }
+constexpr int small_rows() { return N <= 16 ? 256 : (N <= 32 ? 128 : 64); }
 
 template <int N>
 __global__ void __launch_bounds__(small_rows<N>()) k_fft_small(const __grid_constant__ FftArgs a, bool vec)
@@ -93,11 +94,23 @@ cudaError_t launch_small_n(const FftArgs& a, cudaStream_t s)
 
 } // namespace
 
+bool small_fft_length(uint32_t n)
+{
+    switch (n) {
+    case 2: case 3: case 4: case 5: case 6: case 8: case 9: case 10: case 12: case 15: case 16:
+    case 18: case 20: case 24: case 25: case 27: case 30: case 32:
+    case 45:  // its two-pass schedule ran at 2.7 TB/s (here 4.7; 50, 60 and 75 measured
+              // slower here than their 3.5-3.8 TB/s two-pass schedules)
+        return true;
+    default:
+        return false;
+    }
+}
+
 bool small_fft_eligible(const FftArgs& a)
 {
-    return a.N >= 2u && a.N <= kSmallFftMax && a.ioMode == IO_C2C && !a.perCh && !a.batchMinor &&
-           a.inElem == 1 && a.outElem == 1 && a.inBatch == (int64_t)a.N && a.outBatch == (int64_t)a.N &&
-           is_235(a.N);
+    return small_fft_length(a.N) && a.ioMode == IO_C2C && !a.perCh && !a.batchMinor && a.inElem == 1 &&
+           a.outElem == 1 && a.inBatch == (int64_t)a.N && a.outBatch == (int64_t)a.N;
 }
 
 cudaError_t launch_fft_small(const FftArgs& a, cudaStream_t s)
@@ -122,6 +135,7 @@ cudaError_t launch_fft_small(const FftArgs& a, cudaStream_t s)
     case 27: return launch_small_n<27>(a, s);
     case 30: return launch_small_n<30>(a, s);
     case 32: return launch_small_n<32>(a, s);
+    case 45: return launch_small_n<45>(a, s);
     default: return cudaErrorInvalidValue;
     }
 }
