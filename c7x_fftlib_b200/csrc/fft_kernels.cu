@@ -66,6 +66,8 @@ void register_static_m(std::vector<StaticEntry>& out);
 void register_static_n(std::vector<StaticEntry>& out);
 void register_static_o(std::vector<StaticEntry>& out);
 void register_static_p(std::vector<StaticEntry>& out);
+void register_static_q(std::vector<StaticEntry>& out);
+void register_static_r(std::vector<StaticEntry>& out);
 
 const std::vector<StaticEntry>& static_schedules()
 {
@@ -87,6 +89,8 @@ const std::vector<StaticEntry>& static_schedules()
         register_static_n(t);
         register_static_o(t);
         register_static_p(t);
+        register_static_q(t);
+        register_static_r(t);
         return t;
     }();
     return table;

@@ -31,6 +31,9 @@ __global__ void __launch_bounds__(small_rows<N>()) k_fft_small(const __grid_cons
     constexpr int kSmallRows = small_rows<N>();
     constexpr int S = N | 1;  // padded row length
     __shared__ float2 rows[kSmallRows * S];
+    // a launch that follows with programmatic stream serialization may start
+    // now (a no-op otherwise)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const uint32_t tid = threadIdx.x;
     const uint64_t blocks = (a.batch + kSmallRows - 1u) / kSmallRows;
     for (uint64_t blk = blockIdx.x; blk < blocks; blk += gridDim.x) {
@@ -88,6 +91,18 @@ cudaError_t launch_small_n(const FftArgs& a, cudaStream_t s)
     const uint64_t blocks = (a.batch + kSmallRows - 1u) / kSmallRows;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(blocks, (uint64_t)std::max(sms, 1) * 8u);
     const bool vec = ((((uintptr_t)a.in) | ((uintptr_t)a.out)) & 15u) == 0;
+    if (a.overlapPrev) {  // see FftArgs::overlapPrev
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(grid);
+        lc.blockDim = dim3((unsigned)kSmallRows);
+        lc.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        return cudaLaunchKernelEx(&lc, k_fft_small<N>, a, vec);
+    }
     k_fft_small<N><<<grid, kSmallRows, 0, s>>>(a, vec);
     return cudaGetLastError();
 }

@@ -9,8 +9,6 @@ namespace fftb200 {
 
 void register_static_l(std::vector<StaticEntry>& out)
 {
-    out.push_back(static_entry<StaticSchedule<2430, 32, 135, 18, 15, 9>, 128, true>());
-    out.push_back(static_entry<StaticSchedule<2916, 32, 162, 18, 18, 9>, 128, true>());
     out.push_back(static_entry<StaticSchedule<3125, 32, 125, 25, 25, 5>, 128, true>());
     out.push_back(static_entry<StaticSchedule<3240, 32, 135, 27, 12, 10>, 128, true>());
     out.push_back(static_entry<StaticSchedule<3645, 32, 135, 27, 15, 9>, 128, true>());

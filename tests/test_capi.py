@@ -280,12 +280,13 @@ def test_planner_headline_schedule():
 def test_planner_prefers_the_measured_wide_schedules():
     """Lengths whose 32-wide fixed-size schedule (fewer passes, radices up to
     27 and 32) measured faster than the heuristic pick run that schedule."""
-    want = {250: "25x10", 576: "24x24", 864: "32x27", 2000: "25x10x8", 3645: "27x15x9", 4050: "27x15x10"}
+    want = {250: "25x10", 270: "27x10", 576: "24x24", 864: "32x27", 2000: "25x10x8", 2916: "27x12x9",
+            3000: "25x12x10", 3645: "27x15x9", 4050: "27x15x10"}
     for n, radices in want.items():
         d = F.describe_plan(n)
         assert d.startswith(f"N={n} E=32 ") and f"radices={radices} " in d, d
     # and the heuristic keeps the lengths where the 16-wide schedule won
-    for n in (1024, 2048, 3000, 3600):
+    for n in (1024, 2048, 1875, 3600):
         assert " E=16 " in F.describe_plan(n), F.describe_plan(n)
 
 
