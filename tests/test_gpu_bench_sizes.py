@@ -253,3 +253,42 @@ def test_host_buffers_through_the_chunk_pipeline(torch, kind):
     F.check(F.fn(base + "_init")(F.ptr(src), bX, F.ptr(w), bW, F.ptr(yh), bX, n, ch, pb))
     F.check(F.fn(base + "_kernel")(F.ptr(src), bX, F.ptr(w), bW, F.ptr(yh), bX, n, ch, pb))
     assert torch.equal(yh, yd.cpu())
+
+
+SMALL_LENGTHS = (2, 3, 4, 5, 6, 8, 9, 10, 12, 15, 16, 18, 20, 24, 25, 27, 30, 32, 45)
+
+
+@pytest.mark.parametrize("kind", ["c2c", "ifft"])
+@pytest.mark.parametrize("ch", [1, 63, 255, 257, 4097])
+def test_one_transform_per_thread_lengths(torch, kind, ch):
+    """The lengths run one transform per thread (2..32 and 45): batches below,
+    at and across a CTA's rows, every transform against the GPU FP64 oracle;
+    odd channel counts with odd lengths also leave the block's value count
+    odd (the 8-byte copy path)."""
+    g = torch.Generator(device="cuda").manual_seed(ch)
+    for n in SMALL_LENGTHS:
+        x = torch.rand(2 * n * ch, device="cuda", generator=g) * 2 - 1
+        y = _c2c(torch, kind, x, n, ch)
+        overall, worst = O.gpu_check_c2c(x, y, n, ch, inverse=(kind == "ifft"))
+        assert overall <= REL_L2 and worst <= REL_L2, (n, ch, overall, worst)
+
+
+def test_one_transform_per_thread_unaligned_buffers(torch):
+    """Input and output 8 bytes off a 16-byte boundary (the 8-byte copy path)
+    through the asynchronous entry, against the aligned result."""
+    st = torch.cuda.current_stream().cuda_stream
+    k = F.fn("FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync")
+    for n in SMALL_LENGTHS:
+        ch = 1000 + n
+        x = torch.rand(2 * n * ch + 2, device="cuda") * 2 - 1
+        y = torch.zeros(2 * n * ch + 2, device="cuda")
+        xv, yv = x[2:], y[2:]
+        pb = F.pblock("c2c")
+        bX, bW = F.bp(F.FFTLIB_FLOAT32, 2 * n * ch), F.bp(F.FFTLIB_FLOAT32, 2 * n)
+        w = torch.zeros(2 * n, device="cuda")
+        xa = xv.clone()
+        F.check(F.fn(F.KERNELS["c2c"] + "_init")(F.ptr(xa), bX, F.ptr(w), bW, F.ptr(yv), bX, n, ch, pb))
+        F.check(k(F.ptr(xv), F.ptr(yv), n, ch, pb, F.ptr(st)))
+        torch.cuda.synchronize()
+        overall, worst = O.gpu_check_c2c(xv, yv, n, ch)
+        assert overall <= REL_L2 and worst <= REL_L2, (n, overall, worst)
