@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (the north-star headline): FFTLIB_fft1dBatched_i32fc_c32fc_o32fc,
+Workload (the headline configuration): FFTLIB_fft1dBatched_i32fc_c32fc_o32fc,
 FP32 complex-to-complex forward FFT, N = 4096 points, 8192 channels per GPU,
 interleaved re/im, inputs iid U[-1, 1) from a fixed seed. A step is one
 batched transform of the whole batch. Metric: HBM throughput in GB/s of
