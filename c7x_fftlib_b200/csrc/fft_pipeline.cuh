@@ -152,8 +152,8 @@ FFT_DEV TileSpan tile_span(uint32_t tile, uint32_t m, uint32_t batch, uint64_t i
 // unpadded and back to back, at the start of the stage; the first pass of
 // transform m reads its input from there and (after the CTA-wide barrier
 // inside the pass, when every input has been read) writes its outputs in the
-// padded layout at m * SL, and so on; the stage is refilled once the first
-// pass has read it. IO (IO_C2C, IO_R2C_SPLIT or IO_C2R_SPLIT) is the one
+// padded layout at m * SL, and so on; a stage is refilled as soon as the
+// CTA has moved past the tile it held. IO (IO_C2C, IO_R2C_SPLIT or IO_C2R_SPLIT) is the one
 // transform kind the instantiation serves, so that none of them carries the
 // others' code (a.ioMode equals it).
 template <class S, int STAGES, int M, int IO>
@@ -215,19 +215,17 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
         }
         __syncthreads();
         if (s_fail) break;
+        // every thread is past the previous tile (its last pass, and the r2c
+        // epilogue, read that tile's stage before this barrier): refill that
+        // stage with the tile STAGES-1 iterations ahead right away
+        if (tid == 0 && it > 0) {
+            fence_proxy_async_smem();
+            const uint32_t next = tile + (uint32_t)(STAGES - 1) * G;
+            if (next < tiles) issue(next, (int)((it - 1) % STAGES));
+        }
 
         const uint32_t gidx = tile * (uint32_t)M + m;
         const bool active = gidx < a.batch;
-        // once every thread has read this tile's inputs (the barrier inside
-        // pass 0), the previous tile's stage is free: refill it with the
-        // tile STAGES-1 iterations ahead
-        auto refill = [&]() {
-            if (tid == 0 && it > 0) {
-                fence_proxy_async_smem();
-                const uint32_t next = tile + (uint32_t)(STAGES - 1) * G;
-                if (next < tiles) issue(next, (int)((it - 1) % STAGES));
-            }
-        };
         float2* rowOut = a.out + (size_t)gidx * (size_t)a.outBatch;
         // a schedule whose first (last) pass can run mirrored splits the
         // c2r input (r2c output) there, in registers
@@ -259,13 +257,11 @@ FFT_DEV void fft_pipeline(const FftArgs& a)
             const float2* raw = st + shift + m * (uint32_t)IC;
             if constexpr (P == 0) {
                 if constexpr (kC2RMirror)
-                    run_pass<S::EMAX, S::R[P], decltype(refill), false, kPad16, L0, true, kMirrorC2R>(
-                        a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut, raw,
-                        refill);
+                    run_pass<S::EMAX, S::R[P], NoHook, false, kPad16, L0, true, kMirrorC2R>(
+                        a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut, raw);
                 else
-                    run_pass<S::EMAX, S::R[P], decltype(refill), false, kPad16, L0, true>(
-                        a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut, raw,
-                        refill);
+                    run_pass<S::EMAX, S::R[P], NoHook, false, kPad16, L0, true>(
+                        a, pi, true, P + 1 == S::P, (uint32_t)S::T, v, st + m * SL, t, active, nullptr, rowOut, raw);
             } else if constexpr (P + 1 == S::P) {
                 if constexpr (kR2CMirror)
                     run_pass<S::EMAX, S::R[P], NoHook, false, P == 1 ? L0 : kPad16, kPad16, true, kMirrorR2C>(
