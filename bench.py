@@ -502,8 +502,8 @@ def secondary_configs(args):
     parity_check("mixed_20000 sampled rel-L2", mixed_rel <= REL_L2_BOUND, mixed_rel)
     mbytes = 16.0 * total
     res["mixed_20000"] = {"lengths": len(uniq), "total_points": total,
-                          "launch": "one graph: each length group's persistent fixed-size kernel on a grid "
-                                    "share, parallel branches",
+                          "launch": "one graph: the length groups' persistent fixed-size kernels chained "
+                                    "by programmatic dependent launch, largest and smallest groups in turn",
                           "persistent_graph_ms": round(ms_graph, 4),
                           "persistent_graph_GBps": round(mbytes / ms_graph / 1e6, 1),
                           "single_persistent_kernel_ms": round(ms_persistent, 4),
