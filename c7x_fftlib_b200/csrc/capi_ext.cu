@@ -96,8 +96,10 @@ FFTLIB_STATUS FFTLIB_b200_describePlan(uint32_t numPoints, char* buf, uint32_t l
     int G = 0;
     uint32_t R[kMaxGlobal];
     if (plan_engine(numPoints, &e)) {
-        s = describe(e) + (static_max_threads(numPoints, e.emax, e.T, e.P, e.R) ? " (fixed-size kernel)"
-                                                                              : " (runtime-radix engine)");
+        // (c2c of these lengths runs one transform per thread instead)
+        s = describe(e) + (small_fft_length(numPoints) ? " (fixed-size kernel; c2c: one transform per thread)"
+                           : static_max_threads(numPoints, e.emax, e.T, e.P, e.R) ? " (fixed-size kernel)"
+                                                                                : " (runtime-radix engine)");
     } else if (split_global(numPoints, &G, R)) {
         s = "global passes";
         for (int g = 0; g < G; ++g) {

@@ -546,6 +546,8 @@ std::string describe_plan(const ComplexPlan* p)
         return s;
     }
     const EnginePlan& e = p->eng;
+    if (small_fft_length(p->n)) return std::string(p->tuned ? "tuned: " : "planner: ") + "N=" + std::to_string(p->n) +
+                                      " (c2c: one transform per thread; real kinds: " + describe(e) + ")";
     const bool fixed = static_max_threads(p->n, e.emax, e.T, e.P, e.R) != 0;
     const bool pipe = fixed && !p->noPipe && static_pipelined_resident(p->n, e.emax, e.T, e.P, e.R) > 0;
     std::string s = std::string(p->tuned ? "tuned: " : "planner: ") + describe(e);

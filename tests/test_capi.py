@@ -293,9 +293,11 @@ def test_planner_prefers_the_measured_wide_schedules():
 def test_every_length_from_8_to_4096_has_a_fixed_size_kernel():
     """Every 2^a 3^b 5^c length in [8, 4096] runs a kernel compiled for its
     planned schedule (the runtime-radix engine serves the rest)."""
+    small = {8, 9, 10, 12, 15, 16, 18, 20, 24, 25, 27, 30, 32, 45}  # c2c: one transform per thread
     for n in _sizes_235(4096):
         if n >= 8:
-            assert F.describe_plan(n).endswith("(fixed-size kernel)"), (n, F.describe_plan(n))
+            want = "(fixed-size kernel; c2c: one transform per thread)" if n in small else "(fixed-size kernel)"
+            assert F.describe_plan(n).endswith(want), (n, F.describe_plan(n))
 
 
 def test_planner_rejects_other_primes():
