@@ -18,7 +18,7 @@ struct I16Choice {
     uint32_t gridCap;
     uint32_t minBlocks;
 };
-// The launcher's default tg: 256 from n = 4096 up, else n / 16 (at least 1).
+// The launcher's default tg: n / 32, within [1, 256].
 uint32_t i16_default_tg(uint32_t n);
 // Dynamic shared memory of a CTA with that tg, and CTAs resident per SM.
 size_t i16_smem_bytes(uint32_t n, uint32_t tg);

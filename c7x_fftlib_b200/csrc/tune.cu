@@ -357,17 +357,18 @@ float time_batched(const ComplexPlan* base, const BatchedChoice& c, int kind, in
 
 // ---- int16 -------------------------------------------------------------------
 
-// Threads per transform of the int16 kernel worth timing, the launcher's
-// default first; each leaves the CTA's shared memory (the Q15 table as
-// 32-bit pairs plus 256 / tg padded transforms) within 227 KB.
+// Threads per transform of the int16 kernel worth timing: the launcher's
+// default first, then twice and half as many, each a power of two up to 256
+// that leaves the CTA's shared memory (the Q15 table as 32-bit pairs plus
+// 256 / tg padded transforms) within 227 KB.
 std::vector<uint32_t> i16_tg_candidates(uint32_t n)
 {
     std::vector<uint32_t> out;
     const uint32_t def = i16_default_tg(n);
-    for (uint32_t tg = def; tg >= 1u && out.size() < 3; tg /= 2u) {
-        if (i16_smem_bytes(n, tg) <= 227u * 1024u) out.push_back(tg);
-        if (tg == 1u) break;
-    }
+    for (uint32_t tg : {def, 2u * def, def / 2u})
+        if (tg >= 1u && tg <= 256u && i16_smem_bytes(n, tg) <= 227u * 1024u &&
+            std::find(out.begin(), out.end(), tg) == out.end())
+            out.push_back(tg);
     return out;
 }
 
