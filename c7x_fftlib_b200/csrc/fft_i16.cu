@@ -27,12 +27,6 @@ namespace fftb200 {
 
 __device__ __forceinline__ int16_t wrap16(int v) { return (int16_t)(uint16_t)(unsigned)v; }
 
-// -im with the VCROT90H saturation of -(-32768) to 32767.
-__device__ __forceinline__ int16_t rot90_re(int16_t im)
-{
-    return im == (int16_t)-32768 ? (int16_t)32767 : (int16_t)(-(int)im);
-}
-
 // Right shift rounding by the last bit shifted out; the mask is formed as
 // the reference forms it on x86 (32-bit shift by shift-1 with the count
 // taken mod 32, narrowed to int16), which makes shift 0 a no-op.
@@ -105,54 +99,18 @@ struct C16 {
 __device__ __forceinline__ C16 ld(const short2* p) { short2 v = *p; return C16{v.x, v.y}; }
 __device__ __forceinline__ void st(short2* p, C16 c) { *p = make_short2(c.re, c.im); }
 
-// One 4-point butterfly on p[0..3] (stride q apart in the stage), outputs
-// written back as bins 0,2,1,3 (the reference's slot order), each followed
-// by the stage's shift sr (the identity for the 8-point stage).
-// tw: the three Q15 twiddles (x1, x2, x3) unless notw.
-// Sums and differences are formed in int32 and wrapped to int16 only where
-// the reference's value is used non-linearly: the j-rotation's saturation
-// test and the four outputs (wrapping is linear modulo 2^16, so delaying it
-// gives the same bits).
-__device__ __forceinline__ void bfly4(C16& p0, C16& p1, C16& p2, C16& p3, bool notw,
-                                      const int2* tw, uint32_t k, uint32_t q, const ShiftRound& sr)
-{
-    const int s1r = p0.re + p2.re, s1i = p0.im + p2.im;
-    const int s2r = p1.re + p3.re, s2i = p1.im + p3.im;
-    const int d1r = p0.re - p2.re, d1i = p0.im - p2.im;
-    const int d2r = p1.re - p3.re;
-    const int16_t d2i = wrap16(p1.im - p3.im);
-    const int jr = rot90_re(d2i), ji = d2r;
-    C16 x0{wrap16(s1r + s2r), wrap16(s1i + s2i)};
-    C16 x1{wrap16(d1r - jr), wrap16(d1i - ji)};
-    C16 x2{wrap16(s1r - s2r), wrap16(s1i - s2i)};
-    C16 x3{wrap16(d1r + jr), wrap16(d1i + ji)};
-    // x0's Q15 product with 32767+1 (the reference's 0x7FFF0000 >> 16 scale
-    // of x0 by 2^15) rounds back to x0 exactly: only the shift applies
-    x0 = C16{sr(x0.re), sr(x0.im)};
-    if (!notw) {
-        const int2 w1 = tw[k], w2 = tw[q + k], w3 = tw[2 * q + k];
-        const C16 a = x1, b = x2, c = x3;
-        x1 = C16{q15s_dot_sub(a.re, w1.x, a.im, w1.y, sr), q15s_dot_add(a.re, w1.y, a.im, w1.x, sr)};
-        x2 = C16{q15s_dot_sub(b.re, w2.x, b.im, w2.y, sr), q15s_dot_add(b.re, w2.y, b.im, w2.x, sr)};
-        x3 = C16{q15s_dot_sub(c.re, w3.x, c.im, w3.y, sr), q15s_dot_add(c.re, w3.y, c.im, w3.x, sr)};
-    } else {
-        x1 = C16{sr(x1.re), sr(x1.im)};
-        x2 = C16{sr(x2.re), sr(x2.im)};
-        x3 = C16{sr(x3.re), sr(x3.im)};
-    }
-    // slot order: bin0 -> 0, bin2 -> q, bin1 -> 2q, bin3 -> 3q
-    p0 = x0;
-    p1 = x2;
-    p2 = x1;
-    p3 = x3;
-}
-
-// The same butterfly on (re, im) pairs packed in 32 bits (re low), the sums
-// and differences in per-halfword SIMD: __vadd2 / __vsub2 wrap each 16-bit
-// half exactly as the int16 arithmetic does, and __vnegss2 saturates
-// -(-32768) to 32767 as the j-rotation does (only the imaginary half of its
-// result is used: j = (sat(-d2.im), d2.re)). The shift and the Q15 products
-// work on the unpacked halves.
+// One 4-point butterfly on p0..p3 (stride q apart in the stage), each an
+// (re, im) pair packed in 32 bits (re low); outputs written back as bins
+// 0, 2, 1, 3 (the reference's slot order), each followed by the stage's
+// shift sr (the identity for the 8-point stage); tw: the three Q15 twiddles
+// (of bins 1, 2, 3) unless notw. The sums and differences run in
+// per-halfword SIMD: __vadd2 / __vsub2 wrap each 16-bit half exactly as the
+// reference's int16 arithmetic does, and __vnegss2 saturates -(-32768) to
+// 32767 as its j-rotation does (only the imaginary half of that result is
+// used: j = (sat(-d2.im), d2.re)). Bin 0's Q15 product with 32767+1 (the
+// reference's 0x7FFF0000 >> 16 scale by 2^15) rounds back to itself exactly,
+// so only the shift applies to it; the shift and the Q15 products work on
+// the unpacked halves.
 __device__ __forceinline__ int lo16(uint32_t v) { return (int)(int16_t)(uint16_t)v; }
 __device__ __forceinline__ int hi16(uint32_t v) { return (int)v >> 16; }
 __device__ __forceinline__ uint32_t pack16(int re, int im)
@@ -179,15 +137,6 @@ __device__ __forceinline__ void bfly4_packed(uint32_t& p0, uint32_t& p1, uint32_
         p1 = pack16(sr((int16_t)lo16(x2)), sr((int16_t)hi16(x2)));
         p3 = pack16(sr((int16_t)lo16(x3)), sr((int16_t)hi16(x3)));
     }
-}
-
-// Stage with block size m (q = m/4) on the 4 points {k + b*m + i*q}; sr
-// is the identity for m = 8.
-__device__ __forceinline__ void stage_bfly(C16* pt, uint32_t m, uint32_t k, const int2* tw, const ShiftRound& sr)
-{
-    const uint32_t q = m / 4u;
-    const bool notw = (m == 4u) || (m == 8u && k == 0u);
-    bfly4(pt[0], pt[1], pt[2], pt[3], notw, tw, k, q, sr);
 }
 
 // Shared-memory index with one pad word per 16: the 16-point gathers of the
@@ -292,16 +241,18 @@ __global__ void __launch_bounds__(256, MINB) k_fft_i16(const short2* __restrict_
             shift = s_shift[stage];
             const uint32_t q = m / 4u;
             if (active) {
+                const ShiftRound sr(shift, m != 8u);
+                uint32_t* su = reinterpret_cast<uint32_t*>(sx);
                 for (uint32_t j = t; j < n / 4u; j += tg) {
-                    const uint32_t blk = j / q, k = j - blk * q;
+                    const uint32_t blk = j / q, k = j - blk * q;  // q is 1 or 2
                     const uint32_t base = blk * m + k;
-                    C16 q4[4] = {ld(sx + pad16(base)), ld(sx + pad16(base + q)), ld(sx + pad16(base + 2 * q)),
-                                 ld(sx + pad16(base + 3 * q))};
-                    stage_bfly(q4, m, k, tw, ShiftRound(shift, m != 8u));
-                    st(sx + pad16(base), q4[0]);
-                    st(sx + pad16(base + q), q4[1]);
-                    st(sx + pad16(base + 2 * q), q4[2]);
-                    st(sx + pad16(base + 3 * q), q4[3]);
+                    uint32_t u0 = su[pad16(base)], u1 = su[pad16(base + q)], u2 = su[pad16(base + 2 * q)],
+                             u3 = su[pad16(base + 3 * q)];
+                    bfly4_packed(u0, u1, u2, u3, (m == 4u) || (m == 8u && k == 0u), tw, k, q, sr);
+                    su[pad16(base)] = u0;
+                    su[pad16(base + q)] = u1;
+                    su[pad16(base + 2 * q)] = u2;
+                    su[pad16(base + 3 * q)] = u3;
                 }
             }
             __syncthreads();
