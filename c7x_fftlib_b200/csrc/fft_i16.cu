@@ -18,7 +18,9 @@
 // traffic and barriers.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <utility>
 #include <stdint.h>
 
 #include "fft_i16.h"
@@ -141,7 +143,52 @@ __device__ __forceinline__ void bfly4_packed(uint32_t& p0, uint32_t& p1, uint32_
 
 // Shared-memory index with one pad word per 16: the 16-point gathers of the
 // fused stages and the bit-reversed final gather hit distinct banks.
+// For an m-point block (m a multiple of 16) and k0 < s16 = m / 16,
+// pad16(blk*m + k0 + i*s16) = pad16(blk*m + k0) + pad16(i*s16): the points
+// of a fused group sit at fixed offsets from its padded base (for s16 >= 16
+// i*s16 is a multiple of 16; below, k0 + i*s16 crosses a multiple of 16
+// exactly where i*s16 does).
 __device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
+
+// Two radix-4 stages on one m-point block per 16-point group: block m with
+// shift shiftA, then the four m/4 sub-blocks with shiftB (m a power of two
+// >= 16; the 8-point special case where m or m/4 is 8).
+__device__ __forceinline__ void fused_pair(uint32_t* su, const int2* tw, uint32_t m, uint32_t n, uint32_t t,
+                                           uint32_t tg, uint32_t shiftA, uint32_t shiftB)
+{
+    const uint32_t m2 = m / 4u;
+    const ShiftRound srA(shiftA, m != 8u), srB(shiftB, m2 != 8u);
+    const int2* tw2 = tw + 3u * (m / 4u);
+    const uint32_t s16 = m / 16u;
+    const uint32_t ls16 = 31u - __clz(s16);  // m is a power of two: shifts, not divisions
+    const uint32_t groups = n / 16u;         // (block, k0) pairs
+    const uint32_t qA = m / 4u, qB = m2 / 4u;
+    for (uint32_t gi = t; gi < groups; gi += tg) {
+        const uint32_t blk = gi >> ls16, k0 = gi & (s16 - 1u);
+        const uint32_t pb = pad16(blk * m + k0);
+        uint32_t p[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) p[i] = su[pb + pad16((uint32_t)i * s16)];
+        // stage A (block m): butterflies k = k0 + i*s16, points i, i+4, i+8, i+12
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t kA = k0 + (uint32_t)i * s16;
+            const bool notwA = (m == 4u) || (m == 8u && kA == 0u);
+            bfly4_packed(p[i], p[i + 4], p[i + 8], p[i + 12], notwA, tw, kA, qA, srA);
+        }
+        // stage B (block m/4): sub-block s (points 4s..4s+3), butterfly k0
+        const bool notwB = (m2 == 4u) || (m2 == 8u && k0 == 0u);
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            bfly4_packed(p[4 * s], p[4 * s + 1], p[4 * s + 2], p[4 * s + 3], notwB, tw2, k0, qB, srB);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) su[pb + pad16((uint32_t)i * s16)] = p[i];
+    }
+}
+
+// Number of fused stage pairs of an n-point transform (m = n, n/16, ... >= 16).
+__host__ __device__ constexpr int i16_fused_pairs(uint32_t n) { return n >= 16u ? 1 + i16_fused_pairs(n / 16u) : 0; }
+__host__ __device__ constexpr uint32_t i16_log2(uint32_t n) { return n > 1u ? 1u + i16_log2(n / 2u) : 0u; }
 
 // Persistent CTAs of G groups; a group of tg threads owns one transform at a
 // time (its own padded shared-memory region) and the CTA walks the batch G
@@ -149,14 +196,21 @@ __device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
 // copied into shared memory once per CTA.
 // MINB: CTAs per SM the registers are budgeted for (3: 80 registers; 4: 64,
 // with a few spilled values), a launch-shape choice of the autotuner.
-template <int MINB>
+// NC: the transform length when fixed at compile time (every stage's block
+// size, stride and special case then fold into constants and the stage loop
+// unrolls), 0 for the kernel that takes it at run time.
+// vecIn / vecOut: 16-byte loads of x / stores of y (aligned buffers, n % 4 == 0).
+template <int MINB, uint32_t NC>
 __global__ void __launch_bounds__(256, MINB) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
                                                  const short2* __restrict__ w,
-                                                 const uint32_t* __restrict__ shifts, uint32_t nsh, uint32_t n,
-                                                 uint32_t logn, uint32_t batch, uint32_t tg, bool vec)
+                                                 const uint32_t* __restrict__ shifts, uint32_t nsh, uint32_t nArg,
+                                                 uint32_t lognArg, uint32_t batch, uint32_t tg, bool vecIn,
+                                                 bool vecOut)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t s_shift[8];
+    const uint32_t n = NC ? NC : nArg;
+    const uint32_t logn = NC ? i16_log2(NC) : lognArg;
     const uint32_t padn = n + (n >> 4);
     const uint32_t G = blockDim.x / tg;
     const uint32_t g = threadIdx.x / tg, t = threadIdx.x - g * tg;
@@ -165,6 +219,7 @@ __global__ void __launch_bounds__(256, MINB) k_fft_i16(const short2* __restrict_
     int2* stw = reinterpret_cast<int2*>(smem_raw);
     short2* smem = reinterpret_cast<short2*>(stw + n);
     short2* sx = smem + g * padn;
+    uint32_t* su = reinterpret_cast<uint32_t*>(sx);
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const short2 v = w[i];
         stw[i] = make_int2(v.x, v.y);
@@ -177,7 +232,7 @@ __global__ void __launch_bounds__(256, MINB) k_fft_i16(const short2* __restrict_
         const bool active = b < batch;
         if (active) {
             const short2* src = x + (size_t)b * n;
-            if (vec) {  // 16-byte loads: four points each
+            if (vecIn) {  // 16-byte loads: four points each
                 const int4* s4 = reinterpret_cast<const int4*>(src);
                 for (uint32_t i4 = t; i4 < n / 4u; i4 += tg) {
                     const int4 v = __ldg(s4 + i4);
@@ -196,45 +251,25 @@ __global__ void __launch_bounds__(256, MINB) k_fft_i16(const short2* __restrict_
         uint32_t m = n, stage = 0, shift = 0;
         const int2* tw = stw;
         // pairs of radix-4 stages fused in registers: 16 points per thread
-        while (m >= 16u) {
-            const uint32_t shiftA = s_shift[stage];
-            const uint32_t m2 = m / 4u;
-            const uint32_t shiftB = s_shift[stage + 1];
-            const ShiftRound srA(shiftA, m != 8u), srB(shiftB, m2 != 8u);
-            const int2* tw2 = tw + 3u * (m / 4u);
-            const uint32_t s16 = m / 16u;
-            const uint32_t ls16 = 31u - __clz(s16);  // m is a power of two: shifts, not divisions
-            const uint32_t groups = n / 16u; // (block, k0) pairs
-            if (active) {
-                for (uint32_t gi = t; gi < groups; gi += tg) {
-                    const uint32_t blk = gi >> ls16, k0 = gi & (s16 - 1u);
-                    const uint32_t base = blk * m + k0;
-                    uint32_t* su = reinterpret_cast<uint32_t*>(sx);
-                    uint32_t p[16];
+        if constexpr (NC != 0u) {
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) p[i] = su[pad16(base + (uint32_t)i * s16)];
-                    // stage A (block m): butterflies k = k0 + i*s16, points i, i+4, i+8, i+12
-                    const uint32_t qA = m / 4u, qB = m2 / 4u;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const uint32_t kA = k0 + (uint32_t)i * s16;
-                        const bool notwA = (m == 4u) || (m == 8u && kA == 0u);
-                        bfly4_packed(p[i], p[i + 4], p[i + 8], p[i + 12], notwA, tw, kA, qA, srA);
-                    }
-                    // stage B (block m/4): sub-block s (points 4s..4s+3), butterfly k0
-                    const bool notwB = (m2 == 4u) || (m2 == 8u && k0 == 0u);
-#pragma unroll
-                    for (int s = 0; s < 4; ++s)
-                        bfly4_packed(p[4 * s], p[4 * s + 1], p[4 * s + 2], p[4 * s + 3], notwB, tw2, k0, qB, srB);
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) su[pad16(base + (uint32_t)i * s16)] = p[i];
-                }
+            for (int pair = 0; pair < i16_fused_pairs(NC); ++pair) {
+                if (active) fused_pair(su, tw, m, n, t, tg, s_shift[stage], s_shift[stage + 1]);
+                __syncthreads();
+                shift = s_shift[stage + 1];
+                tw += 3u * (m / 4u) + 3u * (m / 16u);
+                m /= 16u;
+                stage += 2;
             }
-            __syncthreads();
-            shift = shiftB;
-            tw = tw2 + 3u * (m2 / 4u);
-            m = m2 / 4u;
-            stage += 2;
+        } else {
+            while (m >= 16u) {
+                if (active) fused_pair(su, tw, m, n, t, tg, s_shift[stage], s_shift[stage + 1]);
+                __syncthreads();
+                shift = s_shift[stage + 1];
+                tw += 3u * (m / 4u) + 3u * (m / 16u);
+                m /= 16u;
+                stage += 2;
+            }
         }
         // one remaining radix-4 stage (m == 4 or 8)
         if (m > 2u) {
@@ -242,7 +277,6 @@ __global__ void __launch_bounds__(256, MINB) k_fft_i16(const short2* __restrict_
             const uint32_t q = m / 4u;
             if (active) {
                 const ShiftRound sr(shift, m != 8u);
-                uint32_t* su = reinterpret_cast<uint32_t*>(sx);
                 for (uint32_t j = t; j < n / 4u; j += tg) {
                     const uint32_t blk = j / q, k = j - blk * q;  // q is 1 or 2
                     const uint32_t base = blk * m + k;
@@ -274,9 +308,21 @@ __global__ void __launch_bounds__(256, MINB) k_fft_i16(const short2* __restrict_
         // bit-reversed gather into natural order
         if (active) {
             short2* dst = y + (size_t)b * n;
-            for (uint32_t k = t; k < n; k += tg) {
-                const uint32_t r = logn ? (__brev(k) >> (32u - logn)) : 0u;
-                dst[k] = sx[pad16(r)];
+            if (vecOut && n >= 64u) {
+                // outputs 4j..4j+3 come from r(4j) + {0, n/2, n/4, 3n/4} (the
+                // reversed low bits are disjoint from r(4j)'s), each a multiple
+                // of 16, so their padded indices are pad16(r(4j)) + pad16(offset)
+                const uint32_t o1 = pad16(n / 2u), o2 = pad16(n / 4u), o3 = pad16(3u * (n / 4u));
+                int4* d4 = reinterpret_cast<int4*>(dst);
+                for (uint32_t j = t; j < n / 4u; j += tg) {
+                    const uint32_t r = pad16(__brev(4u * j) >> (32u - logn));
+                    d4[j] = make_int4((int)su[r], (int)su[r + o1], (int)su[r + o2], (int)su[r + o3]);
+                }
+            } else {
+                for (uint32_t k = t; k < n; k += tg) {
+                    const uint32_t r = logn ? (__brev(k) >> (32u - logn)) : 0u;
+                    dst[k] = sx[pad16(r)];
+                }
             }
         }
         __syncthreads();  // the region is reloaded next iteration
@@ -290,10 +336,16 @@ uint32_t i16_num_shifts(uint32_t n)
     return s;
 }
 
-// n / 32 (8 transforms per CTA at N = 1024): timed faster than n / 16 at
-// N = 256, 1024 and 4096 (27.8 / 30.8 / 74.1 us against 28.8 / 32.9 / 77.2 us
-// on 16,384 / 4,096 / 2,048 transforms)
-uint32_t i16_default_tg(uint32_t n) { return std::max(1u, std::min(256u, n / 32u)); }
+// The fixed-length kernels (56 registers, four CTAs per SM): n / 16, timed
+// faster than n / 32 at N = 256 and 4096 (20.6 / 53.3 us against 21.5 /
+// 55.6 us on 16,384 / 4,096 transforms) and level at 1024 (26.7 us). The
+// run-time-length kernel (80 registers, three CTAs): n / 32, timed faster
+// than n / 16 at N = 256, 1024 and 4096 (27.8 / 30.8 / 74.1 us against
+// 28.8 / 32.9 / 77.2 us on 16,384 / 4,096 / 2,048 transforms).
+uint32_t i16_default_tg(uint32_t n)
+{
+    return std::max(1u, std::min(256u, i16_fixed_length(n) ? n / 16u : n / 32u));
+}
 
 size_t i16_smem_bytes(uint32_t n, uint32_t tg)
 {
@@ -304,34 +356,56 @@ size_t i16_smem_bytes(uint32_t n, uint32_t tg)
 namespace {
 
 using I16Kernel = void (*)(const short2*, short2*, const short2*, const uint32_t*, uint32_t, uint32_t, uint32_t,
-                           uint32_t, uint32_t, bool);
+                           uint32_t, uint32_t, bool, bool);
 
-I16Kernel i16_kernel(uint32_t minBlocks) { return minBlocks == 4u ? &k_fft_i16<4> : &k_fft_i16<3>; }
+// the lengths with a compile-time kernel; others take the run-time one
+template <int MINB>
+I16Kernel i16_kernel_for(uint32_t n)
+{
+    switch (n) {
+    case 64u: return &k_fft_i16<MINB, 64u>;
+    case 128u: return &k_fft_i16<MINB, 128u>;
+    case 256u: return &k_fft_i16<MINB, 256u>;
+    case 512u: return &k_fft_i16<MINB, 512u>;
+    case 1024u: return &k_fft_i16<MINB, 1024u>;
+    case 2048u: return &k_fft_i16<MINB, 2048u>;
+    case 4096u: return &k_fft_i16<MINB, 4096u>;
+    default: return &k_fft_i16<MINB, 0u>;
+    }
+}
 
-cudaError_t i16_configure(size_t smem, uint32_t minBlocks)
+I16Kernel i16_kernel(uint32_t n, uint32_t minBlocks)
+{
+    return minBlocks == 4u ? i16_kernel_for<4>(n) : i16_kernel_for<3>(n);
+}
+
+cudaError_t i16_configure(I16Kernel kern, size_t smem)
 {
     static std::mutex mu;
-    static size_t configured[64][2] = {};
+    static std::map<std::pair<int, I16Kernel>, size_t> configured;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (smem <= 48u * 1024u) return cudaSuccess;
-    const int k = minBlocks == 4u ? 1 : 0;
     std::lock_guard<std::mutex> lock(mu);
-    if (dev < 64 && configured[dev][k] >= smem) return cudaSuccess;
-    e = cudaFuncSetAttribute(i16_kernel(minBlocks), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess && dev < 64) configured[dev][k] = smem;
+    size_t& done = configured[std::make_pair(dev, kern)];
+    if (done >= smem) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) done = smem;
     return e;
 }
 
 } // namespace
 
+bool i16_fixed_length(uint32_t n) { return i16_kernel_for<3>(n) != &k_fft_i16<3, 0u>; }
+
 int i16_resident(uint32_t n, uint32_t tg, uint32_t minBlocks)
 {
     const size_t smem = i16_smem_bytes(n, tg);
+    const I16Kernel kern = i16_kernel(n, minBlocks);
     int perSm = 0;
-    if (i16_configure(smem, minBlocks) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, i16_kernel(minBlocks), 256, smem) != cudaSuccess) {
+    if (i16_configure(kern, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, 256, smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -343,7 +417,7 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
                            uint32_t minBlocks)
 {
     if (batch == 0) return cudaSuccess;
-    const I16Kernel kern = i16_kernel(minBlocks);
+    const I16Kernel kern = i16_kernel(n, minBlocks);
     uint32_t logn = 0;
     while ((1u << logn) < n) ++logn;
     if (tg == 0) tg = i16_default_tg(n);
@@ -354,7 +428,7 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    e = i16_configure(smem, minBlocks);
+    e = i16_configure(kern, smem);
     if (e != cudaSuccess) return e;
     int perSm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, (int)threads, smem);
@@ -364,9 +438,10 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
     const uint64_t steps = (batch + G - 1u) / G;
     uint32_t grid = (uint32_t)std::min<uint64_t>(steps, (uint64_t)std::max(1, perSm) * (uint64_t)sms);
     if (gridCap) grid = std::max(1u, std::min(grid, gridCap));
-    const bool vec = (((uintptr_t)x & 15u) == 0) && (n % 4u) == 0;
+    const bool vecIn = (((uintptr_t)x & 15u) == 0) && (n % 4u) == 0;
+    const bool vecOut = (((uintptr_t)y & 15u) == 0) && (n % 4u) == 0;
     kern<<<grid, threads, smem, s>>>((const short2*)x, (short2*)y, (const short2*)w, shifts, i16_num_shifts(n), n,
-                                     logn, batch, tg, vec);
+                                     logn, batch, tg, vecIn, vecOut);
     return cudaGetLastError();
 }
 

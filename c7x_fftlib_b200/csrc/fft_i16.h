@@ -18,11 +18,14 @@ struct I16Choice {
     uint32_t gridCap;
     uint32_t minBlocks;
 };
-// The launcher's default tg: n / 32, within [1, 256].
+// The launcher's default tg: n / 16 for the fixed-length kernels, n / 32 for the
+// run-time-length one, within [1, 256].
 uint32_t i16_default_tg(uint32_t n);
 // Dynamic shared memory of a CTA with that tg, and CTAs resident per SM.
 size_t i16_smem_bytes(uint32_t n, uint32_t tg);
 int i16_resident(uint32_t n, uint32_t tg, uint32_t minBlocks = 3);
+// n has a kernel built for that length (64...4096), its stage constants folded
+bool i16_fixed_length(uint32_t n);
 
 // x, y: batch x n interleaved int16 complex; w: the caller's Q15 radix-4
 // table (2n int16); shifts: i16_num_shifts(n) entries. All device pointers.
