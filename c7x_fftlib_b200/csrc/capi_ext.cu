@@ -128,8 +128,8 @@ FFTLIB_STATUS FFTLIB_b200_describeBlock(const void* pBlock, char* buf, uint32_t 
     if (r.kind == REC_I16 || r.kind == REC_1D_I16) {
         const uint32_t tg = r.i16Tg ? r.i16Tg : i16_default_tg(r.numPoints);
         s = std::string(r.i16Tuned ? "tuned: " : "planner: ") + "int16 radix-4 (" +
-            (i16_fixed_length(r.numPoints) ? "fixed-length" : "run-time-length") + " kernel), " + std::to_string(tg) +
-            " threads per transform, " + std::to_string(256u / tg) + " transforms per CTA";
+            (i16_fixed_length(r.numPoints, tg) ? "fixed-length" : "run-time-length") + " kernel), " + std::to_string(tg) +
+            " threads per transform, " + std::to_string(i16_block_threads(tg) / tg) + " transforms per CTA";
         if (r.i16GridCap) s += ", " + std::to_string(r.i16GridCap) + " CTAs";
         if (r.i16MinBlocks == 4u) s += ", 64 registers (4 CTAs per SM)";
     } else if (r.plan) {

@@ -200,8 +200,10 @@ __host__ __device__ constexpr uint32_t i16_log2(uint32_t n) { return n > 1u ? 1u
 // size, stride and special case then fold into constants and the stage loop
 // unrolls), 0 for the kernel that takes it at run time.
 // vecIn / vecOut: 16-byte loads of x / stores of y (aligned buffers, n % 4 == 0).
-template <int MINB, uint32_t NC>
-__global__ void __launch_bounds__(256, MINB) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
+// MAXT: the largest block: 256 (groups of up to 256 threads), or 1024 for the
+// longest lengths, where one transform per CTA takes up to 1024 threads.
+template <int MINB, uint32_t NC, int MAXT = 256>
+__global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
                                                  const short2* __restrict__ w,
                                                  const uint32_t* __restrict__ shifts, uint32_t nsh, uint32_t nArg,
                                                  uint32_t lognArg, uint32_t batch, uint32_t tg, bool vecIn,
@@ -342,14 +344,21 @@ uint32_t i16_num_shifts(uint32_t n)
 // run-time-length kernel (80 registers, three CTAs): n / 32, timed faster
 // than n / 16 at N = 256, 1024 and 4096 (27.8 / 30.8 / 74.1 us against
 // 28.8 / 32.9 / 77.2 us on 16,384 / 4,096 / 2,048 transforms).
+// N = 8192 and 16384: n / 16 threads (512 / 1024) on one transform per CTA;
+// with 256 threads per transform one CTA per SM (shared memory) leaves 8
+// warps to the SM.
 uint32_t i16_default_tg(uint32_t n)
 {
-    return std::max(1u, std::min(256u, i16_fixed_length(n) ? n / 16u : n / 32u));
+    return std::max(1u, std::min(i16_max_tg(n), i16_fixed_length(n, n / 16u) ? n / 16u : n / 32u));
 }
+
+uint32_t i16_max_tg(uint32_t n) { return (n == 8192u || n == 16384u) ? 1024u : 256u; }
+
+uint32_t i16_block_threads(uint32_t tg) { return std::max(256u, tg); }
 
 size_t i16_smem_bytes(uint32_t n, uint32_t tg)
 {
-    const uint32_t G = 256u / tg;
+    const uint32_t G = i16_block_threads(tg) / tg;
     return (size_t)n * sizeof(int2) + (size_t)G * (n + (n >> 4)) * sizeof(short2);
 }
 
@@ -374,8 +383,15 @@ I16Kernel i16_kernel_for(uint32_t n)
     }
 }
 
-I16Kernel i16_kernel(uint32_t n, uint32_t minBlocks)
+// tg > 256: the 1024-thread kernels of the longest lengths (one transform per
+// CTA); nullptr for other lengths
+I16Kernel i16_kernel(uint32_t n, uint32_t minBlocks, uint32_t tg)
 {
+    if (tg > 256u) {
+        if (n == 8192u) return &k_fft_i16<1, 8192u, 1024>;
+        if (n == 16384u) return &k_fft_i16<1, 16384u, 1024>;
+        return nullptr;
+    }
     return minBlocks == 4u ? i16_kernel_for<4>(n) : i16_kernel_for<3>(n);
 }
 
@@ -397,15 +413,20 @@ cudaError_t i16_configure(I16Kernel kern, size_t smem)
 
 } // namespace
 
-bool i16_fixed_length(uint32_t n) { return i16_kernel_for<3>(n) != &k_fft_i16<3, 0u>; }
+bool i16_fixed_length(uint32_t n, uint32_t tg)
+{
+    const I16Kernel k = i16_kernel(n, 3u, tg);
+    return k != nullptr && k != &k_fft_i16<3, 0u>;
+}
 
 int i16_resident(uint32_t n, uint32_t tg, uint32_t minBlocks)
 {
     const size_t smem = i16_smem_bytes(n, tg);
-    const I16Kernel kern = i16_kernel(n, minBlocks);
+    const I16Kernel kern = i16_kernel(n, minBlocks, tg);
     int perSm = 0;
-    if (i16_configure(kern, smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, 256, smem) != cudaSuccess) {
+    if (!kern || i16_configure(kern, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, (int)i16_block_threads(tg), smem) !=
+            cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
@@ -417,13 +438,14 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
                            uint32_t minBlocks)
 {
     if (batch == 0) return cudaSuccess;
-    const I16Kernel kern = i16_kernel(n, minBlocks);
     uint32_t logn = 0;
     while ((1u << logn) < n) ++logn;
     if (tg == 0) tg = i16_default_tg(n);
-    if (tg > 256u || (tg & (tg - 1u))) return cudaErrorInvalidValue;
-    const uint32_t G = 256u / tg;
-    const uint32_t threads = tg * G;
+    if (tg > i16_max_tg(n) || (tg & (tg - 1u))) return cudaErrorInvalidValue;
+    const I16Kernel kern = i16_kernel(n, minBlocks, tg);
+    if (!kern) return cudaErrorInvalidValue;
+    const uint32_t threads = i16_block_threads(tg);
+    const uint32_t G = threads / tg;
     const size_t smem = i16_smem_bytes(n, tg);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

@@ -19,13 +19,18 @@ struct I16Choice {
     uint32_t minBlocks;
 };
 // The launcher's default tg: n / 16 for the fixed-length kernels, n / 32 for the
-// run-time-length one, within [1, 256].
+// run-time-length one, within [1, i16_max_tg(n)].
 uint32_t i16_default_tg(uint32_t n);
+// The largest tg: 1024 for n = 8192 and 16384 (one transform per CTA of tg
+// threads), else 256. A CTA has i16_block_threads(tg) threads: max(256, tg).
+uint32_t i16_max_tg(uint32_t n);
+uint32_t i16_block_threads(uint32_t tg);
 // Dynamic shared memory of a CTA with that tg, and CTAs resident per SM.
 size_t i16_smem_bytes(uint32_t n, uint32_t tg);
 int i16_resident(uint32_t n, uint32_t tg, uint32_t minBlocks = 3);
-// n has a kernel built for that length (64...4096), its stage constants folded
-bool i16_fixed_length(uint32_t n);
+// n with tg threads per transform takes a kernel built for that length (64...4096;
+// 8192 and 16384 with tg > 256), its stage constants folded
+bool i16_fixed_length(uint32_t n, uint32_t tg);
 
 // x, y: batch x n interleaved int16 complex; w: the caller's Q15 radix-4
 // table (2n int16); shifts: i16_num_shifts(n) entries. All device pointers.
