@@ -202,11 +202,14 @@ __host__ __device__ constexpr uint32_t i16_log2(uint32_t n) { return n > 1u ? 1u
 // vecIn / vecOut: 16-byte loads of x / stores of y (aligned buffers, n % 4 == 0).
 // MAXT: the largest block: 256 (groups of up to 256 threads), or 1024 for the
 // longest lengths, where one transform per CTA takes up to 1024 threads.
-template <int MINB, uint32_t NC, int MAXT = 256>
+// TG: the threads per transform when fixed at compile time (the default
+// launch of a fixed length: every loop's trip count becomes a constant), 0
+// when taken from tgArg.
+template <int MINB, uint32_t NC, int MAXT = 256, uint32_t TG = 0>
 __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
                                                  const short2* __restrict__ w,
                                                  const uint32_t* __restrict__ shifts, uint32_t nsh, uint32_t nArg,
-                                                 uint32_t lognArg, uint32_t batch, uint32_t tg, bool vecIn,
+                                                 uint32_t lognArg, uint32_t batch, uint32_t tgArg, bool vecIn,
                                                  bool vecOut)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -214,7 +217,9 @@ __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict
     const uint32_t n = NC ? NC : nArg;
     const uint32_t logn = NC ? i16_log2(NC) : lognArg;
     const uint32_t padn = n + (n >> 4);
-    const uint32_t G = blockDim.x / tg;
+    const uint32_t tg = TG ? TG : tgArg;
+    const uint32_t nthreads = TG ? (TG > 256u ? TG : 256u) : blockDim.x;
+    const uint32_t G = nthreads / tg;
     const uint32_t g = threadIdx.x / tg, t = threadIdx.x - g * tg;
     // the caller's Q15 table as 32-bit pairs (one load per twiddle, no
     // extraction), then the transforms' padded regions
@@ -222,7 +227,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict
     short2* smem = reinterpret_cast<short2*>(stw + n);
     short2* sx = smem + g * padn;
     uint32_t* su = reinterpret_cast<uint32_t*>(sx);
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    for (uint32_t i = threadIdx.x; i < n; i += nthreads) {
         const short2 v = w[i];
         stw[i] = make_int2(v.x, v.y);
     }
@@ -367,32 +372,35 @@ namespace {
 using I16Kernel = void (*)(const short2*, short2*, const short2*, const uint32_t*, uint32_t, uint32_t, uint32_t,
                            uint32_t, uint32_t, bool, bool);
 
-// the lengths with a compile-time kernel; others take the run-time one
-template <int MINB>
-I16Kernel i16_kernel_for(uint32_t n)
+// a length with a compile-time kernel: the default launch (n / 16 threads per
+// transform) has its thread count built in too
+template <uint32_t NC>
+I16Kernel fixed_kernel(uint32_t minBlocks, uint32_t tg)
 {
-    switch (n) {
-    case 64u: return &k_fft_i16<MINB, 64u>;
-    case 128u: return &k_fft_i16<MINB, 128u>;
-    case 256u: return &k_fft_i16<MINB, 256u>;
-    case 512u: return &k_fft_i16<MINB, 512u>;
-    case 1024u: return &k_fft_i16<MINB, 1024u>;
-    case 2048u: return &k_fft_i16<MINB, 2048u>;
-    case 4096u: return &k_fft_i16<MINB, 4096u>;
-    default: return &k_fft_i16<MINB, 0u>;
-    }
+    if (minBlocks == 4u) return &k_fft_i16<4, NC>;
+    return tg == NC / 16u ? &k_fft_i16<3, NC, 256, NC / 16u> : &k_fft_i16<3, NC>;
 }
 
 // tg > 256: the 1024-thread kernels of the longest lengths (one transform per
-// CTA); nullptr for other lengths
+// CTA); nullptr for other lengths. Lengths without a compile-time kernel take
+// the run-time one.
 I16Kernel i16_kernel(uint32_t n, uint32_t minBlocks, uint32_t tg)
 {
     if (tg > 256u) {
-        if (n == 8192u) return &k_fft_i16<1, 8192u, 1024>;
-        if (n == 16384u) return &k_fft_i16<1, 16384u, 1024>;
+        if (n == 8192u) return tg == 512u ? &k_fft_i16<1, 8192u, 1024, 512u> : &k_fft_i16<1, 8192u, 1024>;
+        if (n == 16384u) return tg == 1024u ? &k_fft_i16<1, 16384u, 1024, 1024u> : &k_fft_i16<1, 16384u, 1024>;
         return nullptr;
     }
-    return minBlocks == 4u ? i16_kernel_for<4>(n) : i16_kernel_for<3>(n);
+    switch (n) {
+    case 64u: return fixed_kernel<64u>(minBlocks, tg);
+    case 128u: return fixed_kernel<128u>(minBlocks, tg);
+    case 256u: return fixed_kernel<256u>(minBlocks, tg);
+    case 512u: return fixed_kernel<512u>(minBlocks, tg);
+    case 1024u: return fixed_kernel<1024u>(minBlocks, tg);
+    case 2048u: return fixed_kernel<2048u>(minBlocks, tg);
+    case 4096u: return fixed_kernel<4096u>(minBlocks, tg);
+    default: return minBlocks == 4u ? &k_fft_i16<4, 0u> : &k_fft_i16<3, 0u>;
+    }
 }
 
 cudaError_t i16_configure(I16Kernel kern, size_t smem)
