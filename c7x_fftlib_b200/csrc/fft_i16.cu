@@ -186,8 +186,6 @@ __device__ __forceinline__ void fused_pair(uint32_t* su, const int2* tw, uint32_
     }
 }
 
-// Number of fused stage pairs of an n-point transform (m = n, n/16, ... >= 16).
-__host__ __device__ constexpr int i16_fused_pairs(uint32_t n) { return n >= 16u ? 1 + i16_fused_pairs(n / 16u) : 0; }
 __host__ __device__ constexpr uint32_t i16_log2(uint32_t n) { return n > 1u ? 1u + i16_log2(n / 2u) : 0u; }
 
 // Persistent CTAs of G groups; a group of tg threads owns one transform at a
@@ -257,35 +255,19 @@ __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict
 
         uint32_t m = n, stage = 0, shift = 0;
         const int2* tw = stw;
-        // pairs of radix-4 stages fused in registers: 16 points per thread
-        if constexpr (NC != 0u) {
-#pragma unroll
-            for (int pair = 0; pair < i16_fused_pairs(NC); ++pair) {
-                if (active) fused_pair(su, tw, m, n, t, tg, s_shift[stage], s_shift[stage + 1]);
-                __syncthreads();
-                shift = s_shift[stage + 1];
-                tw += 3u * (m / 4u) + 3u * (m / 16u);
-                m /= 16u;
-                stage += 2;
-            }
-        } else {
-            while (m >= 16u) {
-                if (active) fused_pair(su, tw, m, n, t, tg, s_shift[stage], s_shift[stage + 1]);
-                __syncthreads();
-                shift = s_shift[stage + 1];
-                tw += 3u * (m / 4u) + 3u * (m / 16u);
-                m /= 16u;
-                stage += 2;
-            }
-        }
-        // one remaining radix-4 stage (m == 4 or 8)
-        if (m > 2u) {
-            shift = s_shift[stage];
-            const uint32_t q = m / 4u;
+        // An odd number of radix-4 stages (logn / 2 of them, the 8-point stage
+        // included) leaves one stage outside the fused pairs; it runs first, at
+        // m = n, where its butterflies read consecutive points (conflict-free)
+        // — run last, at m = 4 or 8, its four loads per thread collide in banks.
+        // The stages run in the same order either way, each butterfly the same.
+        const uint32_t nst = logn / 2u;
+        if (nst & 1u) {
+            shift = s_shift[0];
+            const uint32_t q = m / 4u, lq = logn - 2u;  // q = n / 4: blk = 0, k = j
             if (active) {
                 const ShiftRound sr(shift, m != 8u);
                 for (uint32_t j = t; j < n / 4u; j += tg) {
-                    const uint32_t blk = j / q, k = j - blk * q;  // q is 1 or 2
+                    const uint32_t blk = j >> lq, k = j & (q - 1u);
                     const uint32_t base = blk * m + k;
                     uint32_t u0 = su[pad16(base)], u1 = su[pad16(base + q)], u2 = su[pad16(base + 2 * q)],
                              u3 = su[pad16(base + 3 * q)];
@@ -297,7 +279,30 @@ __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict
                 }
             }
             __syncthreads();
+            tw += 3u * q;
             m = q;
+            stage = 1;
+        }
+        // pairs of radix-4 stages fused in registers: 16 points per thread
+        if constexpr (NC != 0u) {
+#pragma unroll
+            for (uint32_t pair = 0; pair < i16_log2(NC) / 4u; ++pair) {
+                if (active) fused_pair(su, tw, m, n, t, tg, s_shift[stage], s_shift[stage + 1]);
+                __syncthreads();
+                shift = s_shift[stage + 1];
+                tw += 3u * (m / 4u) + 3u * (m / 16u);
+                m /= 16u;
+                stage += 2;
+            }
+        } else {
+            for (uint32_t pair = 0; pair < nst / 2u; ++pair) {
+                if (active) fused_pair(su, tw, m, n, t, tg, s_shift[stage], s_shift[stage + 1]);
+                __syncthreads();
+                shift = s_shift[stage + 1];
+                tw += 3u * (m / 4u) + 3u * (m / 16u);
+                m /= 16u;
+                stage += 2;
+            }
         }
         // trailing radix-2 shares the shift of the 8-point stage
         if (m == 2u) {
