@@ -150,11 +150,25 @@ __device__ __forceinline__ void bfly4_packed(uint32_t& p0, uint32_t& p1, uint32_
 // exactly where i*s16 does).
 __device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
 
+// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned),
+// completed by cp_async_wait_all in the issuing thread.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // Two radix-4 stages on one m-point block per 16-point group: block m with
 // shift shiftA, then the four m/4 sub-blocks with shiftB (m a power of two
-// >= 16; the 8-point special case where m or m/4 is 8).
+// >= 16; the 8-point special case where m or m/4 is 8). FLAT: the points are
+// read from flat (unpadded) src instead of su, for the first stage (m = n,
+// where a warp's 16-point groups are consecutive columns, conflict-free).
+template <bool FLAT = false>
 __device__ __forceinline__ void fused_pair(uint32_t* su, const int2* tw, uint32_t m, uint32_t n, uint32_t t,
-                                           uint32_t tg, uint32_t shiftA, uint32_t shiftB)
+                                           uint32_t tg, uint32_t shiftA, uint32_t shiftB,
+                                           const uint32_t* src = nullptr)
 {
     const uint32_t m2 = m / 4u;
     const ShiftRound srA(shiftA, m != 8u), srB(shiftB, m2 != 8u);
@@ -168,7 +182,8 @@ __device__ __forceinline__ void fused_pair(uint32_t* su, const int2* tw, uint32_
         const uint32_t pb = pad16(blk * m + k0);
         uint32_t p[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) p[i] = su[pb + pad16((uint32_t)i * s16)];
+        for (int i = 0; i < 16; ++i)
+            p[i] = FLAT ? src[blk * m + k0 + (uint32_t)i * s16] : su[pb + pad16((uint32_t)i * s16)];
         // stage A (block m): butterflies k = k0 + i*s16, points i, i+4, i+8, i+12
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -203,13 +218,17 @@ __host__ __device__ constexpr uint32_t i16_log2(uint32_t n) { return n > 1u ? 1u
 // TG: the threads per transform when fixed at compile time (the default
 // launch of a fixed length: every loop's trip count becomes a constant), 0
 // when taken from tgArg.
-template <int MINB, uint32_t NC, int MAXT = 256, uint32_t TG = 0>
+// PF: the next transform's input is copied (cp.async, 16 bytes) into a flat
+// shared-memory buffer of the group while the current one is transformed;
+// the first stage reads it from there. Needs vecIn and n >= 64.
+template <int MINB, uint32_t NC, int MAXT = 256, uint32_t TG = 0, bool PF = false>
 __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict__ x, short2* __restrict__ y,
                                                  const short2* __restrict__ w,
                                                  const uint32_t* __restrict__ shifts, uint32_t nsh, uint32_t nArg,
                                                  uint32_t lognArg, uint32_t batch, uint32_t tgArg, bool vecIn,
                                                  bool vecOut)
 {
+    static_assert(!PF || NC >= 64u, "the prefetching build needs a fixed length of at least 64");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t s_shift[8];
     const uint32_t n = NC ? NC : nArg;
@@ -225,17 +244,30 @@ __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict
     short2* smem = reinterpret_cast<short2*>(stw + n);
     short2* sx = smem + g * padn;
     uint32_t* su = reinterpret_cast<uint32_t*>(sx);
+    // PF: the flat input buffers follow the G padded regions (16-byte aligned:
+    // padn * 4 bytes is a multiple of 16 for n >= 64)
+    uint32_t* inb = reinterpret_cast<uint32_t*>(smem + G * padn) + g * n;
+    const auto prefetch = [&](uint32_t bb) {
+        const int4* s4 = reinterpret_cast<const int4*>(x + (size_t)bb * n);
+        for (uint32_t i4 = t; i4 < n / 4u; i4 += tg) cp_async16(inb + 4u * i4, s4 + i4);
+    };
     for (uint32_t i = threadIdx.x; i < n; i += nthreads) {
         const short2 v = w[i];
         stw[i] = make_int2(v.x, v.y);
     }
     if (threadIdx.x < nsh && threadIdx.x < 8u) s_shift[threadIdx.x] = shifts[threadIdx.x];
+    if constexpr (PF) {
+        if (blockIdx.x * G + g < batch) prefetch(blockIdx.x * G + g);
+        cp_async_commit();
+    }
     __syncthreads();
 
     for (uint32_t b0 = blockIdx.x * G; b0 < batch; b0 += gridDim.x * G) {
         const uint32_t b = b0 + g;
         const bool active = b < batch;
-        if (active) {
+        if constexpr (PF) {
+            cp_async_wait_all();  // this thread's copies of transform b
+        } else if (active) {
             const short2* src = x + (size_t)b * n;
             if (vecIn) {  // 16-byte loads: four points each
                 const int4* s4 = reinterpret_cast<const int4*>(src);
@@ -269,8 +301,13 @@ __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict
                 for (uint32_t j = t; j < n / 4u; j += tg) {
                     const uint32_t blk = j >> lq, k = j & (q - 1u);
                     const uint32_t base = blk * m + k;
-                    uint32_t u0 = su[pad16(base)], u1 = su[pad16(base + q)], u2 = su[pad16(base + 2 * q)],
-                             u3 = su[pad16(base + 3 * q)];
+                    uint32_t u0, u1, u2, u3;
+                    if (PF) {
+                        u0 = inb[base], u1 = inb[base + q], u2 = inb[base + 2 * q], u3 = inb[base + 3 * q];
+                    } else {
+                        u0 = su[pad16(base)], u1 = su[pad16(base + q)], u2 = su[pad16(base + 2 * q)],
+                        u3 = su[pad16(base + 3 * q)];
+                    }
                     bfly4_packed(u0, u1, u2, u3, (m == 4u) || (m == 8u && k == 0u), tw, k, q, sr);
                     su[pad16(base)] = u0;
                     su[pad16(base + q)] = u1;
@@ -279,6 +316,10 @@ __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict
                 }
             }
             __syncthreads();
+            if constexpr (PF) {  // the input buffer is free: fetch the group's next transform
+                if (b + gridDim.x * G < batch) prefetch(b + gridDim.x * G);
+                cp_async_commit();
+            }
             tw += 3u * q;
             m = q;
             stage = 1;
@@ -287,8 +328,18 @@ __global__ void __launch_bounds__(MAXT, MINB) k_fft_i16(const short2* __restrict
         if constexpr (NC != 0u) {
 #pragma unroll
             for (uint32_t pair = 0; pair < i16_log2(NC) / 4u; ++pair) {
-                if (active) fused_pair(su, tw, m, n, t, tg, s_shift[stage], s_shift[stage + 1]);
+                const bool first = PF && pair == 0u && !(nst & 1u);
+                if (active) {
+                    if (first)
+                        fused_pair<true>(su, tw, m, n, t, tg, s_shift[stage], s_shift[stage + 1], inb);
+                    else
+                        fused_pair(su, tw, m, n, t, tg, s_shift[stage], s_shift[stage + 1]);
+                }
                 __syncthreads();
+                if (first) {
+                    if (b + gridDim.x * G < batch) prefetch(b + gridDim.x * G);
+                    cp_async_commit();
+                }
                 shift = s_shift[stage + 1];
                 tw += 3u * (m / 4u) + 3u * (m / 16u);
                 m /= 16u;
@@ -366,10 +417,16 @@ uint32_t i16_max_tg(uint32_t n) { return (n == 8192u || n == 16384u) ? 1024u : 2
 
 uint32_t i16_block_threads(uint32_t tg) { return std::max(256u, tg); }
 
-size_t i16_smem_bytes(uint32_t n, uint32_t tg)
+bool i16_prefetch(uint32_t n, uint32_t tg, uint32_t minBlocks)
+{
+    return minBlocks != 4u && n >= 64u && n <= 2048u && (n & (n - 1u)) == 0 && tg == n / 16u;
+}
+
+size_t i16_smem_bytes(uint32_t n, uint32_t tg, bool prefetch)
 {
     const uint32_t G = i16_block_threads(tg) / tg;
-    return (size_t)n * sizeof(int2) + (size_t)G * (n + (n >> 4)) * sizeof(short2);
+    return (size_t)n * sizeof(int2) + (size_t)G * (n + (n >> 4)) * sizeof(short2) +
+           (prefetch ? (size_t)G * n * sizeof(short2) : 0u);
 }
 
 namespace {
@@ -380,30 +437,35 @@ using I16Kernel = void (*)(const short2*, short2*, const short2*, const uint32_t
 // a length with a compile-time kernel: the default launch (n / 16 threads per
 // transform) has its thread count built in too
 template <uint32_t NC>
-I16Kernel fixed_kernel(uint32_t minBlocks, uint32_t tg)
+I16Kernel fixed_kernel(uint32_t minBlocks, uint32_t tg, bool prefetch)
 {
     if (minBlocks == 4u) return &k_fft_i16<4, NC>;
-    return tg == NC / 16u ? &k_fft_i16<3, NC, 256, NC / 16u> : &k_fft_i16<3, NC>;
+    if (tg != NC / 16u) return &k_fft_i16<3, NC>;
+    if constexpr (NC <= 2048u) {
+        if (prefetch) return &k_fft_i16<3, NC, 256, NC / 16u, true>;
+    }
+    return &k_fft_i16<3, NC, 256, NC / 16u>;
 }
 
 // tg > 256: the 1024-thread kernels of the longest lengths (one transform per
 // CTA); nullptr for other lengths. Lengths without a compile-time kernel take
-// the run-time one.
-I16Kernel i16_kernel(uint32_t n, uint32_t minBlocks, uint32_t tg)
+// the run-time one. prefetch: the cp.async build where i16_prefetch allows it.
+I16Kernel i16_kernel(uint32_t n, uint32_t minBlocks, uint32_t tg, bool prefetch)
 {
+    prefetch = prefetch && i16_prefetch(n, tg, minBlocks);
     if (tg > 256u) {
         if (n == 8192u) return tg == 512u ? &k_fft_i16<1, 8192u, 1024, 512u> : &k_fft_i16<1, 8192u, 1024>;
         if (n == 16384u) return tg == 1024u ? &k_fft_i16<1, 16384u, 1024, 1024u> : &k_fft_i16<1, 16384u, 1024>;
         return nullptr;
     }
     switch (n) {
-    case 64u: return fixed_kernel<64u>(minBlocks, tg);
-    case 128u: return fixed_kernel<128u>(minBlocks, tg);
-    case 256u: return fixed_kernel<256u>(minBlocks, tg);
-    case 512u: return fixed_kernel<512u>(minBlocks, tg);
-    case 1024u: return fixed_kernel<1024u>(minBlocks, tg);
-    case 2048u: return fixed_kernel<2048u>(minBlocks, tg);
-    case 4096u: return fixed_kernel<4096u>(minBlocks, tg);
+    case 64u: return fixed_kernel<64u>(minBlocks, tg, prefetch);
+    case 128u: return fixed_kernel<128u>(minBlocks, tg, prefetch);
+    case 256u: return fixed_kernel<256u>(minBlocks, tg, prefetch);
+    case 512u: return fixed_kernel<512u>(minBlocks, tg, prefetch);
+    case 1024u: return fixed_kernel<1024u>(minBlocks, tg, prefetch);
+    case 2048u: return fixed_kernel<2048u>(minBlocks, tg, prefetch);
+    case 4096u: return fixed_kernel<4096u>(minBlocks, tg, prefetch);
     default: return minBlocks == 4u ? &k_fft_i16<4, 0u> : &k_fft_i16<3, 0u>;
     }
 }
@@ -428,14 +490,16 @@ cudaError_t i16_configure(I16Kernel kern, size_t smem)
 
 bool i16_fixed_length(uint32_t n, uint32_t tg)
 {
-    const I16Kernel k = i16_kernel(n, 3u, tg);
+    const I16Kernel k = i16_kernel(n, 3u, tg, false);
     return k != nullptr && k != &k_fft_i16<3, 0u>;
 }
 
 int i16_resident(uint32_t n, uint32_t tg, uint32_t minBlocks)
 {
-    const size_t smem = i16_smem_bytes(n, tg);
-    const I16Kernel kern = i16_kernel(n, minBlocks, tg);
+    // as launched on aligned buffers
+    const bool pf = i16_prefetch(n, tg, minBlocks);
+    const size_t smem = i16_smem_bytes(n, tg, pf);
+    const I16Kernel kern = i16_kernel(n, minBlocks, tg, pf);
     int perSm = 0;
     if (!kern || i16_configure(kern, smem) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, (int)i16_block_threads(tg), smem) !=
@@ -455,11 +519,14 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
     while ((1u << logn) < n) ++logn;
     if (tg == 0) tg = i16_default_tg(n);
     if (tg > i16_max_tg(n) || (tg & (tg - 1u))) return cudaErrorInvalidValue;
-    const I16Kernel kern = i16_kernel(n, minBlocks, tg);
+    const bool vecIn = (((uintptr_t)x & 15u) == 0) && (n % 4u) == 0;
+    const bool vecOut = (((uintptr_t)y & 15u) == 0) && (n % 4u) == 0;
+    const bool pf = vecIn && i16_prefetch(n, tg, minBlocks);
+    const I16Kernel kern = i16_kernel(n, minBlocks, tg, pf);
     if (!kern) return cudaErrorInvalidValue;
     const uint32_t threads = i16_block_threads(tg);
     const uint32_t G = threads / tg;
-    const size_t smem = i16_smem_bytes(n, tg);
+    const size_t smem = i16_smem_bytes(n, tg, pf);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -473,8 +540,6 @@ cudaError_t launch_fft_i16(const int16_t* x, int16_t* y, const int16_t* w, const
     const uint64_t steps = (batch + G - 1u) / G;
     uint32_t grid = (uint32_t)std::min<uint64_t>(steps, (uint64_t)std::max(1, perSm) * (uint64_t)sms);
     if (gridCap) grid = std::max(1u, std::min(grid, gridCap));
-    const bool vecIn = (((uintptr_t)x & 15u) == 0) && (n % 4u) == 0;
-    const bool vecOut = (((uintptr_t)y & 15u) == 0) && (n % 4u) == 0;
     kern<<<grid, threads, smem, s>>>((const short2*)x, (short2*)y, (const short2*)w, shifts, i16_num_shifts(n), n,
                                      logn, batch, tg, vecIn, vecOut);
     return cudaGetLastError();

@@ -25,8 +25,12 @@ uint32_t i16_default_tg(uint32_t n);
 // threads), else 256. A CTA has i16_block_threads(tg) threads: max(256, tg).
 uint32_t i16_max_tg(uint32_t n);
 uint32_t i16_block_threads(uint32_t tg);
+// The default launch of lengths 64...2048 on 16-byte aligned input copies the
+// next transform's input into shared memory while the current one is
+// transformed (an extra flat buffer per transform).
+bool i16_prefetch(uint32_t n, uint32_t tg, uint32_t minBlocks);
 // Dynamic shared memory of a CTA with that tg, and CTAs resident per SM.
-size_t i16_smem_bytes(uint32_t n, uint32_t tg);
+size_t i16_smem_bytes(uint32_t n, uint32_t tg, bool prefetch = false);
 int i16_resident(uint32_t n, uint32_t tg, uint32_t minBlocks = 3);
 // n with tg threads per transform takes a kernel built for that length (64...4096;
 // 8192 and 16384 with tg > 256), its stage constants folded

@@ -366,7 +366,7 @@ std::vector<uint32_t> i16_tg_candidates(uint32_t n)
     std::vector<uint32_t> out;
     const uint32_t def = i16_default_tg(n);
     for (uint32_t tg : {def, 2u * def, def / 2u})
-        if (tg >= 1u && tg <= i16_max_tg(n) && i16_smem_bytes(n, tg) <= 227u * 1024u &&
+        if (tg >= 1u && tg <= i16_max_tg(n) && i16_smem_bytes(n, tg, i16_prefetch(n, tg, 3u)) <= 227u * 1024u &&
             std::find(out.begin(), out.end(), tg) == out.end())
             out.push_back(tg);
     return out;
