@@ -56,6 +56,7 @@ __device__ __forceinline__ int16_t shift_round(int16_t v, uint32_t shift)
 struct ShiftRound {
     int s, add;
     int k2, sh, lo, hi;  // the product path: K / 2, 14 + s (at most 31), f(-32768), f(32767)
+    int k2u;             // (K - C) / 2 for a sum offset by C = 2^31 - 2^16 (q15u)
     __device__ __forceinline__ explicit ShiftRound(uint32_t shift, bool apply = true)
     {
         if (!apply) shift = 0;
@@ -63,6 +64,7 @@ struct ShiftRound {
         const uint32_t rb = (shift - 1u) & 31u;
         add = rb < 16u ? (int)(1u << rb) : 0;  // the mask narrowed to int16 is non-zero
         k2 = 0x2000 + add * 16384;
+        k2u = k2 - 0x3FFF8000;
         sh = min(14 + s, 31);
         lo = (-32768 + add) >> s;
         hi = (32767 + add) >> s;
@@ -72,6 +74,13 @@ struct ShiftRound {
     __device__ __forceinline__ int16_t operator()(int16_t v) const { return (int16_t)(((int)v + add) >> s); }
     // the Q15 rounding clamp((x + 0x4000) >> 15) followed by the shift
     __device__ __forceinline__ int16_t q15(int x) const { return (int16_t)max(lo, min(hi, ((x >> 1) + k2) >> sh)); }
+    // the same for u = x + C as an unsigned word (x in [-C, 2^31]):
+    // floor(x / 2) + K / 2 = (u >> 1) + (K - C) / 2, which stays within int32
+    // (add <= 2^15)
+    __device__ __forceinline__ int16_t q15u(uint32_t u) const
+    {
+        return (int16_t)max(lo, min(hi, ((int)(u >> 1) + k2u) >> sh));
+    }
 };
 
 // Q15 product with the reference's rounding and saturation: x = a*b +/- c*d
@@ -80,9 +89,11 @@ struct ShiftRound {
 // [-32768, 32767] ((2u) >> 16 == u >> 15 with floor semantics, and the clamp
 // bounds map onto each other). Products of int16 values lie in
 // [-(2^30 - 2^15), 2^30], and 2^30 only for (-32768)^2, so a difference
-// always fits in int32 and a sum does too except for 2^31 exactly (all four
-// factors -32768), which wraps to INT_MIN and saturates to 32767. Elsewhere
-// |x| <= 2^31 - 2^15, so x + 0x4000 cannot overflow.
+// always fits in int32 and a sum lies in [-(2^31 - 2^16), 2^31]: offset by
+// C = 2^31 - 2^16 it is exact as an unsigned word (the one sum beyond int32,
+// 2^31 with all four factors -32768, then rounds and saturates to 32767 like
+// every other sum). Elsewhere |x| <= 2^31 - 2^15, so x + 0x4000 cannot
+// overflow.
 // The products are then rounded and shifted in one step (ShiftRound::q15).
 __device__ __forceinline__ int16_t q15s_dot_sub(int a, int b, int c, int d, const ShiftRound& sr)
 {
@@ -90,8 +101,7 @@ __device__ __forceinline__ int16_t q15s_dot_sub(int a, int b, int c, int d, cons
 }
 __device__ __forceinline__ int16_t q15s_dot_add(int a, int b, int c, int d, const ShiftRound& sr)
 {
-    const int x = (int)((unsigned)(a * b) + (unsigned)(c * d));
-    return x == (int)0x80000000 ? (int16_t)sr.hi : sr.q15(x);  // 2^31 saturates to 32767, then shifted
+    return sr.q15u((uint32_t)(a * b) + (uint32_t)(c * d) + 0x7FFF0000u);
 }
 
 struct C16 {
