@@ -51,12 +51,14 @@ __device__ __forceinline__ int16_t shift_round(int16_t v, uint32_t shift)
 // clamp(f(u), f(-32768), f(32767)), and nested floor divisions compose:
 // f(floor((x + 2^14) / 2^15)) = floor((x + K) / 2^(15+s)), K = 2^14 + add 2^15.
 // K is even, so that is floor((floor(x / 2) + K / 2) / 2^(14+s)), which stays
-// in 32 bits (|x| <= 2^31 - 2^15 outside the one saturating sum); for
-// 14 + s >= 31 every such quotient is 0 or -1 and a shift by 31 gives it.
+// in 32 bits for a difference of products (|x| <= 2^31 - 2^15; a sum is
+// offset first, cmul_q15); for 14 + s >= 31 every such quotient is 0 or -1
+// and a shift by 31 gives it.
 struct ShiftRound {
     int s, add;
     int k2, sh, lo, hi;  // the product path: K / 2, 14 + s (at most 31), f(-32768), f(32767)
-    int k2u;             // (K - C) / 2 for a sum offset by C = 2^31 - 2^16 (q15u)
+    int k2u;             // (K - C) / 2 for a sum offset by C = 2^31 - 2^16 (cmul_q15)
+    uint32_t lo2, hi2;   // f(-32768), f(32767) in both halfwords
     __device__ __forceinline__ explicit ShiftRound(uint32_t shift, bool apply = true)
     {
         if (!apply) shift = 0;
@@ -68,41 +70,13 @@ struct ShiftRound {
         sh = min(14 + s, 31);
         lo = (-32768 + add) >> s;
         hi = (32767 + add) >> s;
+        lo2 = ((uint32_t)lo & 0xFFFFu) * 0x10001u;
+        hi2 = ((uint32_t)hi & 0xFFFFu) * 0x10001u;
     }
     // the result always fits in int16 (for s = 0 nothing is added), so no
     // wrap is needed
     __device__ __forceinline__ int16_t operator()(int16_t v) const { return (int16_t)(((int)v + add) >> s); }
-    // the Q15 rounding clamp((x + 0x4000) >> 15) followed by the shift
-    __device__ __forceinline__ int16_t q15(int x) const { return (int16_t)max(lo, min(hi, ((x >> 1) + k2) >> sh)); }
-    // the same for u = x + C as an unsigned word (x in [-C, 2^31]):
-    // floor(x / 2) + K / 2 = (u >> 1) + (K - C) / 2, which stays within int32
-    // (add <= 2^15)
-    __device__ __forceinline__ int16_t q15u(uint32_t u) const
-    {
-        return (int16_t)max(lo, min(hi, ((int)(u >> 1) + k2u) >> sh));
-    }
 };
-
-// Q15 product with the reference's rounding and saturation: x = a*b +/- c*d
-// formed exactly, then ((x + 0x4000) << 1) clamped to [-2^31, 0x7FFF0000]
-// and shifted right by 16, which equals clamp((x + 0x4000) >> 15) to
-// [-32768, 32767] ((2u) >> 16 == u >> 15 with floor semantics, and the clamp
-// bounds map onto each other). Products of int16 values lie in
-// [-(2^30 - 2^15), 2^30], and 2^30 only for (-32768)^2, so a difference
-// always fits in int32 and a sum lies in [-(2^31 - 2^16), 2^31]: offset by
-// C = 2^31 - 2^16 it is exact as an unsigned word (the one sum beyond int32,
-// 2^31 with all four factors -32768, then rounds and saturates to 32767 like
-// every other sum). Elsewhere |x| <= 2^31 - 2^15, so x + 0x4000 cannot
-// overflow.
-// The products are then rounded and shifted in one step (ShiftRound::q15).
-__device__ __forceinline__ int16_t q15s_dot_sub(int a, int b, int c, int d, const ShiftRound& sr)
-{
-    return sr.q15(a * b - c * d);
-}
-__device__ __forceinline__ int16_t q15s_dot_add(int a, int b, int c, int d, const ShiftRound& sr)
-{
-    return sr.q15u((uint32_t)(a * b) + (uint32_t)(c * d) + 0x7FFF0000u);
-}
 
 struct C16 {
     int16_t re, im;
@@ -110,6 +84,47 @@ struct C16 {
 
 __device__ __forceinline__ C16 ld(const short2* p) { short2 v = *p; return C16{v.x, v.y}; }
 __device__ __forceinline__ void st(short2* p, C16 c) { *p = make_short2(c.re, c.im); }
+
+// (re, im) halves of a packed pair (re low) and the packing
+__device__ __forceinline__ int lo16(uint32_t v) { return (int)(int16_t)(uint16_t)v; }
+__device__ __forceinline__ int hi16(uint32_t v) { return (int)v >> 16; }
+__device__ __forceinline__ uint32_t pack16(int re, int im)
+{
+    return (uint32_t)(uint16_t)re | ((uint32_t)im << 16);
+}
+
+// Two 32-bit values packed as int16 halves (re low, im high) with signed
+// saturation (cvt.pack.sat: its first source goes to the upper half).
+__device__ __forceinline__ uint32_t pack_sat16(int re, int im)
+{
+    uint32_t d;
+    asm("cvt.pack.sat.s16.s32 %0, %1, %2;" : "=r"(d) : "r"(im), "r"(re));
+    return d;
+}
+
+// Q15 complex product with the reference's rounding and saturation, then the
+// stage shift: for each component x = a*b +/- c*d formed exactly,
+// ((x + 0x4000) << 1) clamped to [-2^31, 0x7FFF0000] and shifted right by 16
+// equals clamp((x + 0x4000) >> 15) to [-32768, 32767] ((2u) >> 16 == u >> 15
+// with floor semantics, and the clamp bounds map onto each other); that and
+// the shift are one step (ShiftRound). Products of int16 values lie in
+// [-(2^30 - 2^15), 2^30], and 2^30 only for (-32768)^2, so the difference
+// (re = x.re*w.x - x.im*w.y) always fits in int32 (|x| <= 2^31 - 2^15, so
+// halving and adding K/2 cannot overflow), and the sum (im = x.re*w.y +
+// x.im*w.x) lies in [-(2^31 - 2^16), 2^31]: offset by C = 2^31 - 2^16 it is
+// exact as an unsigned word u, and floor(x / 2) + K / 2 = (u >> 1) + (K - C) / 2
+// stays within int32 (add <= 2^15); the one sum beyond int32, 2^31 with all
+// four factors -32768, then rounds and saturates to 32767 like every other
+// sum. Both components are clamped to [f(-32768), f(32767)] at once on the
+// packed pair: saturating to int16 first changes nothing, since those bounds
+// lie within int16.
+__device__ __forceinline__ uint32_t cmul_q15(uint32_t xv, int2 w, const ShiftRound& sr)
+{
+    const int re = lo16(xv), im = hi16(xv);
+    const int vr = (((re * w.x - im * w.y) >> 1) + sr.k2) >> sr.sh;
+    const int vi = ((int)(((uint32_t)(re * w.y) + (uint32_t)(im * w.x) + 0x7FFF0000u) >> 1) + sr.k2u) >> sr.sh;
+    return __vmaxs2(__vmins2(pack_sat16(vr, vi), sr.hi2), sr.lo2);
+}
 
 // One 4-point butterfly on p0..p3 (stride q apart in the stage), each an
 // (re, im) pair packed in 32 bits (re low); outputs written back as bins
@@ -122,13 +137,7 @@ __device__ __forceinline__ void st(short2* p, C16 c) { *p = make_short2(c.re, c.
 // used: j = (sat(-d2.im), d2.re)). Bin 0's Q15 product with 32767+1 (the
 // reference's 0x7FFF0000 >> 16 scale by 2^15) rounds back to itself exactly,
 // so only the shift applies to it; the shift and the Q15 products work on
-// the unpacked halves.
-__device__ __forceinline__ int lo16(uint32_t v) { return (int)(int16_t)(uint16_t)v; }
-__device__ __forceinline__ int hi16(uint32_t v) { return (int)v >> 16; }
-__device__ __forceinline__ uint32_t pack16(int re, int im)
-{
-    return (uint32_t)(uint16_t)re | ((uint32_t)im << 16);
-}
+// the unpacked halves (cmul_q15).
 
 __device__ __forceinline__ void bfly4_packed(uint32_t& p0, uint32_t& p1, uint32_t& p2, uint32_t& p3, bool notw,
                                              const int2* tw, uint32_t k, uint32_t q, const ShiftRound& sr)
@@ -141,9 +150,9 @@ __device__ __forceinline__ void bfly4_packed(uint32_t& p0, uint32_t& p1, uint32_
     p0 = pack16(sr((int16_t)lo16(x0)), sr((int16_t)hi16(x0)));
     if (!notw) {
         const int2 w1 = tw[k], w2 = tw[q + k], w3 = tw[2 * q + k];
-        p2 = pack16(q15s_dot_sub(lo16(x1), w1.x, hi16(x1), w1.y, sr), q15s_dot_add(lo16(x1), w1.y, hi16(x1), w1.x, sr));
-        p1 = pack16(q15s_dot_sub(lo16(x2), w2.x, hi16(x2), w2.y, sr), q15s_dot_add(lo16(x2), w2.y, hi16(x2), w2.x, sr));
-        p3 = pack16(q15s_dot_sub(lo16(x3), w3.x, hi16(x3), w3.y, sr), q15s_dot_add(lo16(x3), w3.y, hi16(x3), w3.x, sr));
+        p2 = cmul_q15(x1, w1, sr);
+        p1 = cmul_q15(x2, w2, sr);
+        p3 = cmul_q15(x3, w3, sr);
     } else {
         p2 = pack16(sr((int16_t)lo16(x1)), sr((int16_t)hi16(x1)));
         p1 = pack16(sr((int16_t)lo16(x2)), sr((int16_t)hi16(x2)));

@@ -191,9 +191,10 @@ def test_untuned_block_says_planner(torch, monkeypatch):
 def test_i16_64_register_build_bit_exact(torch, tuning, n, ch):
     """A cache entry selects the int16 kernel built for 64 registers (four
     CTAs per SM) when shared memory admits a fourth CTA; that build is
-    bit-exact too. Lengths 64...4096 have a fixed-length kernel whose
-    registers already admit four CTAs: there the entry is no candidate, the
-    length is timed afresh and the result is still bit-exact."""
+    bit-exact too. Lengths 64...4096 have fixed-length kernels: whether their
+    64-register build admits more CTAs than the default one depends on both
+    builds' register counts, so there the entry may be a candidate or be
+    timed afresh; either way the result is bit-exact."""
     nsh = 0
     m = n
     while m > 2:
@@ -217,5 +218,3 @@ def test_i16_64_register_build_bit_exact(torch, tuning, n, ch):
     np.testing.assert_array_equal(Y.cpu().numpy(), O.fft_c2c_i16(x, n, ch, sh))
     if n < 64:
         assert "64 registers" in desc, desc
-    else:
-        assert "64 registers" not in desc, desc
