@@ -85,3 +85,17 @@ def test_i16_host_buffers(gpu):
     sh = np.array([1, 1, 1, 1], np.uint32)
     x = O.int16_input(n, ch, 3)
     np.testing.assert_array_equal(fftcall.i16(x, n, ch, sh), fftcall.i16(x, n, ch, sh, on_device=False))
+
+
+@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024, 2048, 4096, 8192, 16384])
+def test_i16_every_cta_walks_several_transforms(gpu, n):
+    """Batches large enough that every persistent CTA takes three or more
+    steps, so each group's input copied ahead (while the previous transform
+    is computed) is the one transformed next; the last step is partial, and
+    full-range inputs with mixed shifts. Bit-exact with the oracle."""
+    per_step = 148 * (4 * max(1, 4096 // n) if n <= 4096 else 2)  # CTAs per GPU x transforms per CTA
+    ch = 3 * per_step + 5
+    rng = np.random.default_rng(7 * n)
+    sh = rng.integers(0, 3, nshifts(n)).astype(np.uint32)
+    x = O.int16_input(n, ch, 11 * n, -32768, 32767)
+    np.testing.assert_array_equal(fftcall.i16(x, n, ch, sh), O.fft_c2c_i16(x, n, ch, sh))
