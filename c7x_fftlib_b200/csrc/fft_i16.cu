@@ -418,7 +418,7 @@ uint32_t i16_num_shifts(uint32_t n)
     return s;
 }
 
-// The fixed-length kernels (56 registers, four CTAs per SM): n / 16, timed
+// The fixed-length kernels (at most 64 registers, four CTAs per SM): n / 16, timed
 // faster than n / 32 at N = 256 and 4096 (20.6 / 53.3 us against 21.5 /
 // 55.6 us on 16,384 / 4,096 transforms) and level at 1024 (26.7 us). The
 // run-time-length kernel (80 registers, three CTAs): n / 32, timed faster

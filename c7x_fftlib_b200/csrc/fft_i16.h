@@ -10,9 +10,10 @@ namespace fftb200 {
 uint32_t i16_num_shifts(uint32_t n);
 
 // Launch shape of the int16 kernel: tg threads per transform (a power of
-// two up to 256; each CTA of 256 threads holds 256 / tg transforms), at
-// most gridCap CTAs (0: all that are resident), and the register budget
-// minBlocks (3: 80 registers per thread; 4: 64, four CTAs per SM; 0: 3).
+// two up to i16_max_tg(n); a CTA of max(256, tg) threads holds
+// max(256, tg) / tg transforms), at most gridCap CTAs (0: all that are
+// resident), and the register budget minBlocks (3: at most 80 registers per
+// thread; 4: at most 64, four CTAs per SM; 0: 3).
 struct I16Choice {
     uint32_t tg;
     uint32_t gridCap;
