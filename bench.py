@@ -802,7 +802,7 @@ def run_case(args):
         k = F.fn("FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelAsync")
 
         def launch():
-            k(F.ptr(x), F.ptr(y), n, batch, pb, sp)
+            return k(F.ptr(x), F.ptr(y), n, batch, pb, sp)
     elif kind in ("r2c", "c2r"):
         nb = 4 * n + 8 * (n // 2 + 1)
         nbytes = float(nb) * batch
@@ -811,13 +811,14 @@ def run_case(args):
         b = F.bp(F.FFTLIB_FLOAT32, n * batch)
         pb = F.pblock(kind)
         src, dst = (xr, yc) if kind == "r2c" else (yc, xr)
+        wk = torch.empty(n * batch, device="cuda")  # pXFFT: the global-pass lengths' work buffer
         F.check(F.fn(F.KERNELS[kind] + "_init")(F.ptr(src), b, F.ptr(src), b, None, b, F.ptr(src), b, F.ptr(dst), b,
                                                 n, batch, 0, pb))
         k = F.fn("FFTLIB_b200_fft1dBatched_i32f_c32fc_o32fc_kernelAsync" if kind == "r2c"
                  else "FFTLIB_b200_ifft1dBatched_i32fc_c32fc_o32f_kernelAsync")
 
         def launch():
-            k(F.ptr(src), None, F.ptr(dst), n, batch, 0, pb, sp)
+            return k(F.ptr(src), F.ptr(wk), F.ptr(dst), n, batch, 0, pb, sp)
     elif kind == "i16":
         nbytes = 8.0 * n * batch
         x = torch.randint(-2048, 2048, (2 * n * batch,), device="cuda", dtype=torch.int16, generator=g)
@@ -834,7 +835,7 @@ def run_case(args):
         k = F.fn("FFTLIB_b200_fft1dBatched_i16sc_c16sc_o16sc_kernelAsync")
 
         def launch():
-            k(F.ptr(x), F.ptr(wd), F.ptr(y), F.ptr(sh), ns, n, batch, pb, sp)
+            return k(F.ptr(x), F.ptr(wd), F.ptr(y), F.ptr(sh), ns, n, batch, pb, sp)
     elif kind in ("int16", "int32"):  # the coordinator's integer path, interleaved
         bits = int(kind[3:])
         dt = F.FFTLIB_INT16 if bits == 16 else F.FFTLIB_INT32
@@ -871,7 +872,9 @@ def run_case(args):
     else:
         raise SystemExit(f"unknown case kind {kind}")
     for _ in range(args.warmup):
-        launch()
+        st = launch()
+        if isinstance(st, int):  # the C-ABI calls return their status
+            F.check(st, args.case)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
