@@ -43,6 +43,30 @@ __global__ void k_r2c_post(const float2* __restrict__ z, float2* __restrict__ y,
 }
 
 // z[i] = 0.5 [(X[i] + b) + i conj(W) (X[i] - b)], b = conj(X[h-i]) or X[i+h].
+FFT_DEV float2 c2r_pre_point(float2 xi, float2 bb, float2 w)
+{
+    const float2 s = cadd(xi, bb), d = csub(xi, bb);
+    return cscale(cadd(s, cmul(make_float2(w.y, w.x), d)), 0.5f);
+}
+
+// inMode 0 (h + 1 bins per row): one thread per pair (i, h-i), i in
+// [0, h/2], so each bin is read once (X[i] and X[h-i] serve both outputs).
+__global__ void k_c2r_pre_pairs(const float2* __restrict__ x, float2* __restrict__ z, const float2* __restrict__ wsp,
+                                uint32_t h, uint32_t batch)
+{
+    const uint32_t pairs = h / 2u + 1u;
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)pairs * batch) return;
+    const uint32_t b = (uint32_t)(g / pairs), i = (uint32_t)(g - (uint64_t)b * pairs);
+    const float2* row = x + (size_t)b * (h + 1u);
+    float2* zr = z + (size_t)b * h;
+    const uint32_t ip = h - i;
+    const float2 xi = row[i], xp = row[ip];
+    zr[i] = c2r_pre_point(xi, cconj(xp), wsp[i]);
+    if (i != 0u && ip != i) zr[ip] = c2r_pre_point(xp, cconj(xi), wsp[ip]);
+}
+
+// inMode 1 (2h bins per row): one thread per output point.
 __global__ void k_c2r_pre(const float2* __restrict__ x, float2* __restrict__ z, const float2* __restrict__ wsp,
                           uint32_t h, uint32_t batch, int inmode)
 {
@@ -52,9 +76,7 @@ __global__ void k_c2r_pre(const float2* __restrict__ x, float2* __restrict__ z, 
     const float2* row = x + (size_t)b * (inmode ? 2u * h : h + 1u);
     const float2 xi = row[i];
     const float2 bb = inmode ? row[i + h] : cconj(row[h - i]);
-    const float2 w = wsp[i];
-    const float2 s = cadd(xi, bb), d = csub(xi, bb);
-    z[(size_t)b * h + i] = cscale(cadd(s, cmul(make_float2(w.y, w.x), d)), 0.5f);
+    z[(size_t)b * h + i] = c2r_pre_point(xi, bb, wsp[i]);
 }
 
 cudaError_t launch_r2c_post(const float2* z, float2* y, const float2* wsp, uint32_t h, uint32_t batch,
@@ -69,6 +91,12 @@ cudaError_t launch_r2c_post(const float2* z, float2* y, const float2* wsp, uint3
 cudaError_t launch_c2r_pre(const float2* x, float2* z, const float2* wsp, uint32_t h, uint32_t batch,
                            int inmode, cudaStream_t s)
 {
+    if (!inmode) {
+        const uint64_t pairs = (uint64_t)(h / 2u + 1u) * batch;
+        if (pairs == 0 || h == 0) return cudaSuccess;
+        k_c2r_pre_pairs<<<(unsigned)((pairs + 255) / 256), 256, 0, s>>>(x, z, wsp, h, batch);
+        return cudaGetLastError();
+    }
     const uint64_t total = (uint64_t)h * batch;
     if (total == 0) return cudaSuccess;
     k_c2r_pre<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(x, z, wsp, h, batch, inmode);

@@ -144,7 +144,7 @@ def test_c2c_headline_size_properties(gpu):
 
 
 @pytest.mark.parametrize("n", [2, 4, 6, 10, 12, 18, 30, 50, 64, 128, 250, 256, 480, 960, 1024, 2304, 4096, 5760, 8192,
-                               12800, 16000, 26244, 62500])
+                               12800, 16000, 26244, 62500, 118098])
 @pytest.mark.parametrize("mode", [0, 1])
 def test_r2c_c2r_vs_fp64(gpu, n, mode):
     ch = 3 if n <= 8192 else 2
