@@ -207,6 +207,10 @@ cudaError_t device_table(const void* p, size_t bytes, int slot, const void** out
         t.cap[slot] = bytes;
     }
     e = cudaMemcpy(t.ptr[slot], p, bytes, cudaMemcpyHostToDevice);
+    // a copy from pageable memory may return before its DMA lands, and the
+    // kernel that reads the table may run on a stream that does not wait for
+    // the legacy stream
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
     *out = t.ptr[slot];
     return e;
 }

@@ -166,9 +166,14 @@ float time_mixed_group(const EnginePlan& e, float2* x, float2* y, uint32_t batch
     if (err == cudaSuccess) err = cudaMalloc(&dg, sizeof(g));
     if (err == cudaSuccess) err = cudaMalloc(&dt, tiles.size() * sizeof(MixedTile));
     if (err == cudaSuccess) err = cudaMalloc(&doff, offs.size() * sizeof(uint64_t));
-    if (err == cudaSuccess) err = cudaMemcpy(dg, &g, sizeof(g), cudaMemcpyHostToDevice);
-    if (err == cudaSuccess) err = cudaMemcpy(dt, tiles.data(), tiles.size() * sizeof(MixedTile), cudaMemcpyHostToDevice);
-    if (err == cudaSuccess) err = cudaMemcpy(doff, offs.data(), offs.size() * sizeof(uint64_t), cudaMemcpyHostToDevice);
+    // the descriptors go up on the timing stream itself: a synchronous copy
+    // from pageable memory may return before its DMA lands, and this
+    // non-blocking stream would not wait for it
+    if (err == cudaSuccess) err = cudaMemcpyAsync(dg, &g, sizeof(g), cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(dt, tiles.data(), tiles.size() * sizeof(MixedTile), cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(doff, offs.data(), offs.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, s);
     int dev = 0;
     uint32_t grid = 1;
     if (err == cudaSuccess) err = cudaGetDevice(&dev);
@@ -381,6 +386,9 @@ FFTLIB_STATUS FFTLIB_b200_fftMixed_create(const uint32_t* numPoints, uint32_t co
     upload((void**)&h->dTiles, lpt.data(), lpt.size() * sizeof(MixedTile));
     upload((void**)&h->dTilesByGroup, tiles.data(), tiles.size() * sizeof(MixedTile));
     upload((void**)&h->dOffsets, offsByGroup.data(), offsByGroup.size() * sizeof(uint64_t));
+    // a copy from pageable memory may return before its DMA lands; the graph
+    // replays on streams that do not wait for the legacy stream
+    if (err == cudaSuccess) err = cudaDeviceSynchronize();
     for (int cls = 0; cls < kMixedClasses && err == cudaSuccess; ++cls) {
         if (h->clsTiles[cls]) err = class_grid(cls, h->clsStage[cls], h->device, &h->clsGrid[cls]);
     }
