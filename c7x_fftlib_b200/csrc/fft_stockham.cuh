@@ -457,6 +457,13 @@ FFT_DEV int64_t row_out(const FftArgs& a, uint32_t b)
 // back. Columns (inElem != 1, a full tile of M transforms inside one
 // channel, and inside one twNs block when the input twiddle is on):
 // element i of the tile's transforms is a run of M adjacent values.
+// U: column loads in flight per thread before their shared-memory stores.
+// 4 by default; 8 for the 1024-point pass kernel, whose large column tiles
+// hold few CTAs per SM anyway (4 transforms of 2^20 points as 1024 x 1024
+// passes: 83 -> 75 us),
+// while at 256 points the extra registers cost a CTA per SM (2^24: 0.308 ->
+// 0.339 ms with 8).
+template <int U = 4>
 FFT_DEV void stage_in(const FftArgs& a, float2* smem, uint32_t b0)
 {
     const uint32_t inCount = a.inCount, slen = a.slen;
@@ -464,8 +471,6 @@ FFT_DEV void stage_in(const FftArgs& a, float2* smem, uint32_t b0)
     const uint32_t total = nm * inCount;
     const float2* src = a.in + row_in(a, b0);
     if (a.inElem != 1) {
-        // U loads in flight per thread before their shared-memory stores
-        constexpr int U = 4;
         const uint32_t j0 = a.twLo ? (b0 % a.perCh) % a.twNs : 0u;
         const uint32_t step = blockDim.x;
         for (uint32_t e0 = threadIdx.x; e0 < total; e0 += U * step) {
@@ -607,7 +612,7 @@ FFT_DEV void fft_tile_static(const FftArgs& a, float2* smem, uint32_t b0)
     uint32_t m0, t;
     lane_of(a, (uint32_t)S::T, &m0, &t);
     if (a.staged) {
-        stage_in(a, smem, b0);
+        stage_in<S::N == 1024 ? 8 : 4>(a, smem, b0);
         __syncthreads();
     }
     const uint32_t groups = tile_groups(a), mc = tile_group(a);
