@@ -113,7 +113,8 @@ FFTLIB_STATUS FFTLIB_b200_fft1dBatched_i32fc_c32fc_o32fc_kernelNoAlloc(FFTLIB_F3
  * non-zero; results cached in $FFTLIB_B200_TUNE_CACHE, default
  * $HOME/.cache/fftlib_b200_tune.txt). exec() enqueues the transform on `stream`
  * (device buffers) and returns; execPerSize() runs the persistent kernel once
- * per distinct length, for comparison. */
+ * per distinct length, for comparison. create() synchronizes the device
+ * (its descriptor uploads must land before any graph replay). */
 typedef struct FFTLIB_b200_mixed *FFTLIB_b200_mixedHandle;
 #define FFTLIB_B200_MIXED_INVERSE  1u
 #define FFTLIB_B200_MIXED_AUTOTUNE 2u
